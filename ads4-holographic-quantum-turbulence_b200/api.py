@@ -1,0 +1,287 @@
+"""Host-side interface of the B200 RK4 step, mirroring the reference workflow.
+
+The reference drives its step from MATLAB scripts operating on the workspace
+arrays ``Z1`` (complex Psi), ``Z2`` (A_t), ``Z3`` (A_x), ``Z4`` (A_y) and
+``rhoi`` (``scripts/simulation/tevol_driven_cluster.m:117-187``).
+:class:`Simulation` owns one C-ABI context (``include/hqt.h``) and exposes
+the loop body, the right-hand side ``F1..F4``, the filter ``ff``, the
+boundary order parameter, the winding and ``countN`` on the same arrays.
+
+Host arrays are NumPy arrays indexed ``[x, y, z]`` like the MATLAB arrays
+(any memory order; they are passed in column-major order).  Device arrays
+are CUDA tensors in the same column-major layout, i.e. torch tensors of shape
+``(nz, ny, nx)`` (``(ny, nx)`` for 2-D fields), contiguous.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import HQT_FP64, HQT_MIXED, HQTError, NonfiniteEvolution, check
+
+__all__ = ["Simulation", "StepInfo", "HQTError", "NonfiniteEvolution"]
+
+
+@dataclass
+class StepInfo:
+    steps_done: int
+    nonfinite_step: int
+    last_winding: int
+    records: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Simulation:
+    """A context for one grid and parameter set on one GPU.
+
+    Parameters follow ``tevol_driven_cluster.m``: ``nx, ny`` periodic grid,
+    ``nz`` Chebyshev points, box lengths ``Lx, Ly`` (``L0, L``), chemical
+    potential ``mu``, drive ``vy`` (boundary value ``A_y = -vy``), time step
+    ``dt`` (``h``), ``remove_winding`` (driven script) and ``apply_filter``.
+    """
+
+    def __init__(self, nx: int, ny: int | None = None, nz: int = 21,
+                 Lx: float | None = None, Ly: float | None = None,
+                 mu: float = 6.0, vy: float = 0.0, dt: float = 0.02,
+                 remove_winding: bool = True, precision: str = "fp64",
+                 diag_every: int = 0, apply_filter: bool = True,
+                 device: int = 0):
+        ny = nx if ny is None else ny
+        Lx = (nx - 1) / 2 if Lx is None else Lx
+        Ly = Lx if Ly is None else Ly
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.device = int(device)
+        prec = {"fp64": HQT_FP64, "mixed": HQT_MIXED}[precision]
+        self.params = _lib.hqt_params(self.nx, self.ny, self.nz, float(Lx),
+                                      float(Ly), float(mu), float(vy),
+                                      float(dt), int(bool(remove_winding)),
+                                      prec, int(diag_every),
+                                      int(bool(apply_filter)))
+        self._lib = _lib.load()
+        ctx = ctypes.c_void_p()
+        code = self._lib.hqt_create(ctypes.byref(self.params), self.device,
+                                    ctypes.byref(ctx))
+        check(code, None)
+        self._ctx = ctx
+        self._stream = None
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.hqt_destroy(self._ctx)
+            self._ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    # -- helpers ----------------------------------------------------------
+    def _check(self, code: int) -> None:
+        check(code, self._ctx)
+
+    def _sync_stream(self) -> None:
+        """Order the library after torch's work.  On a torch side stream the
+        library launches on that stream; on the legacy default stream (which
+        cannot be graph-captured) it keeps its own stream and the device is
+        synchronised first."""
+        import torch
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        if s != self._stream:
+            self._check(self._lib.hqt_set_stream(self._ctx, ctypes.c_void_p(s or None)))
+            self._stream = s
+        if not s:
+            torch.cuda.synchronize(self.device)
+
+    def _host3(self, a, dtype) -> np.ndarray:
+        a = np.asarray(a)
+        if a.shape != self.shape:
+            raise ValueError(f"expected shape {self.shape}, got {a.shape}")
+        return np.asfortranarray(a, dtype=dtype)
+
+    def _dev(self, t, shape, dtype):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda):
+            raise TypeError("expected a CUDA tensor")
+        if tuple(t.shape) != shape or t.dtype != dtype or not t.is_contiguous():
+            raise ValueError(f"expected contiguous {dtype} of shape {shape}")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def _dev3(self, t, complex_=False):
+        import torch
+        return self._dev(t, (self.nz, self.ny, self.nx),
+                         torch.complex128 if complex_ else torch.float64)
+
+    def _dev2(self, t, complex_=False):
+        import torch
+        return self._dev(t, (self.ny, self.nx),
+                         torch.complex128 if complex_ else torch.float64)
+
+    def _diag(self, records: int):
+        buf = np.zeros((max(records, 0), 4), dtype=np.int32)
+        d = _lib.hqt_diag()
+        d.capacity = int(records)
+        d.records = (buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+                     if records > 0 else None)
+        return d, buf
+
+    @staticmethod
+    def _info(d, buf) -> StepInfo:
+        return StepInfo(int(d.steps_done), int(d.nonfinite_step),
+                        int(d.last_winding), buf[:d.n_records].copy())
+
+    # -- the loop body ----------------------------------------------------
+    def step(self, Z1, Z2, Z3, Z4, rhoi, nsteps: int = 1, records: int = 0,
+             inplace: bool = False):
+        """Advance host arrays ``nsteps`` RK4 steps (loop body
+        ``tevol_driven_cluster.m:120-142``).  Returns the new
+        ``(Z1, Z2, Z3, Z4, rhoi)`` as column-major arrays and a
+        :class:`StepInfo`; raises :class:`NonfiniteEvolution` on NaN/Inf.
+        With ``inplace=True`` column-major arrays of the right dtype (for
+        example pinned buffers) are updated in place instead of copied."""
+        z1 = self._host3(Z1, np.complex128)
+        z2 = self._host3(Z2, np.float64)
+        z3 = self._host3(Z3, np.float64)
+        z4 = self._host3(Z4, np.float64)
+        rh = self._host3(rhoi, np.float64)
+        if not inplace and (z1 is Z1 or z2 is Z2 or z3 is Z3 or z4 is Z4 or rh is rhoi):
+            z1, z2, z3, z4, rh = (z1.copy(order="F"), z2.copy(order="F"),
+                                  z3.copy(order="F"), z4.copy(order="F"),
+                                  rh.copy(order="F"))
+        d, buf = self._diag(records)
+        code = self._lib.hqt_step(
+            self._ctx, z1.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            _dptr(z2), _dptr(z3), _dptr(z4), _dptr(rh), int(nsteps),
+            ctypes.byref(d))
+        info = self._info(d, buf)
+        if code == _lib.HQT_ENONFINITE:
+            err = NonfiniteEvolution(code, self._lib.hqt_last_error(self._ctx).decode())
+            err.state = (z1, z2, z3, z4, rh)
+            err.info = info
+            raise err
+        self._check(code)
+        return (z1, z2, z3, z4, rh), info
+
+    def step_device(self, Z1, Z2, Z3, Z4, rhoi, nsteps: int = 1,
+                    records: int = 0) -> StepInfo:
+        """Advance CUDA tensors in place (shape ``(nz, ny, nx)``)."""
+        ptrs = [self._dev3(Z1, True), self._dev3(Z2), self._dev3(Z3),
+                self._dev3(Z4), self._dev3(rhoi)]
+        self._sync_stream()
+        d, buf = self._diag(records)
+        code = self._lib.hqt_step_device(self._ctx, *ptrs, int(nsteps),
+                                         ctypes.byref(d))
+        info = self._info(d, buf)
+        self._check(code)
+        return info
+
+    # -- instrumentation --------------------------------------------------
+    def profile(self, enable: bool) -> None:
+        """Reset the launch counters; with ``enable`` every launch is timed
+        with CUDA events (outside the step graph)."""
+        self._check(self._lib.hqt_profile(self._ctx, int(bool(enable))))
+
+    def profile_report(self) -> dict:
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.hqt_profile_report(self._ctx, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    # -- individual operators ---------------------------------------------
+    def rhs_device(self, Z1, Z2, Z3, Z4):
+        """``F1, F3, F4`` and ``F2`` at the boundary slice
+        (``tevol_driven_cluster.m:72-76``), without the factor ``h``."""
+        import torch
+        dev = Z1.device
+        F1 = torch.empty_like(Z1)
+        F3 = torch.empty((self.nz, self.ny, self.nx), dtype=torch.float64, device=dev)
+        F4 = torch.empty_like(F3)
+        F2b = torch.empty((self.ny, self.nx), dtype=torch.float64, device=dev)
+        ptrs = [self._dev3(Z1, True), self._dev3(Z2), self._dev3(Z3),
+                self._dev3(Z4), self._dev3(F1, True), self._dev3(F3),
+                self._dev3(F4), self._dev2(F2b)]
+        self._sync_stream()
+        self._check(self._lib.hqt_rhs_device(self._ctx, *ptrs))
+        return F1, F2b, F3, F4
+
+    def filter_device(self, x, out=None):
+        """``ff(x, fxyz)`` (``src/numerics/ff.m``) of real fields, a tensor of
+        shape ``(nf, nz, ny, nx)`` or ``(nz, ny, nx)``."""
+        import torch
+        if x.dtype != torch.float64 or not x.is_cuda or not x.is_contiguous():
+            raise ValueError("expected a contiguous float64 CUDA tensor")
+        nf = 1 if x.dim() == 3 else x.shape[0]
+        if tuple(x.shape[-3:]) != (self.nz, self.ny, self.nx):
+            raise ValueError("bad field shape")
+        out = torch.empty_like(x) if out is None else out
+        self._sync_stream()
+        self._check(self._lib.hqt_filter_device(
+            self._ctx, ctypes.c_void_p(x.data_ptr()),
+            ctypes.c_void_p(out.data_ptr()), nf))
+        return out
+
+    def order_parameter_device(self, Z1):
+        """``O = func_Lz(Z1)(:,:,nz)`` as a ``(ny, nx)`` complex tensor."""
+        import torch
+        O = torch.empty((self.ny, self.nx), dtype=torch.complex128, device=Z1.device)
+        p = [self._dev3(Z1, True), self._dev2(O, True)]
+        self._sync_stream()
+        self._check(self._lib.hqt_boundary_order_parameter_device(self._ctx, *p))
+        return O
+
+    def winding_device(self, O) -> int:
+        w = ctypes.c_int32()
+        p = self._dev2(O, True)
+        self._sync_stream()
+        self._check(self._lib.hqt_winding_device(self._ctx, p, ctypes.byref(w)))
+        return int(w.value)
+
+    def count_vortices(self, O) -> tuple[int, int, int]:
+        """``countN`` of a host ``(nx, ny)`` complex field."""
+        O = np.asarray(O)
+        if O.shape != (self.nx, self.ny):
+            raise ValueError("expected shape (nx, ny)")
+        o = np.asfortranarray(O, dtype=np.complex128)
+        n, p, m = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._lib.hqt_count_vortices(
+            self._ctx, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            ctypes.byref(n), ctypes.byref(p), ctypes.byref(m)))
+        return int(n.value), int(p.value), int(m.value)
+
+    def count_vortices_device(self, O) -> tuple[int, int, int]:
+        n, p, m = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        ptr = self._dev2(O, True)
+        self._sync_stream()
+        self._check(self._lib.hqt_count_vortices_device(
+            self._ctx, ptr, ctypes.byref(n), ctypes.byref(p), ctypes.byref(m)))
+        return int(n.value), int(p.value), int(m.value)
+
+
+def to_device(a: np.ndarray, device: int = 0):
+    """A host ``[x, y, z]`` array as a column-major CUDA tensor
+    (shape ``(nz, ny, nx)``)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(np.asarray(a).T))
+    return t.to(f"cuda:{device}")
+
+
+def from_device(t) -> np.ndarray:
+    """Inverse of :func:`to_device`: a host ``[x, y, z]`` array."""
+    return t.detach().cpu().numpy().T

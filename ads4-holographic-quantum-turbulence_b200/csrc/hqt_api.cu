@@ -1,0 +1,1013 @@
+// hqt_api.cu -- context, step orchestration and the C ABI of include/hqt.h.
+//
+// One RK4 step of scripts/simulation/tevol_driven_cluster.m:120-142 is the
+// launch sequence below (FP64 drop-in):
+//   x/y first derivatives of A_t (step-constant, A_t is frozen during the
+//   four stages, :120-123)
+//   4 x [x pass, y pass, z stage]                         (:120-124,128)
+//   x/y divergence of the combined A, z constraint kernel (:129-133)
+//   winding reduction                                     (:136-139)
+//   filter: x forward, y weight, x inverse + NaN guard    (:142, :182-185)
+// The sequence is captured once as a CUDA graph and replayed per step.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "hqt.h"
+#include "hqt_diag.cuh"
+#include "hqt_launch.h"
+#include "hqt_ops_host.h"
+
+namespace hqt {
+
+static constexpr int kThreadsFFT = 128;
+static constexpr int kThreadsZ = 64;
+static constexpr size_t kSmemBudget = 72 * 1024;
+static constexpr int kPartials = 296;
+
+#define HQT_NZP_VAL(N) N,
+static const int kNZP[] = {HQT_NZP_LIST(HQT_NZP_VAL)};
+#undef HQT_NZP_VAL
+
+}  // namespace hqt
+
+using namespace hqt;
+
+struct hqt_ctx {
+    hqt_params p{};
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int nx = 0, ny = 0, nz = 0, NZP = 0;
+    long long plane = 0, vol = 0;
+    FFTPlan planx{}, plany{};
+    double2 *rootsx = nullptr, *rootsy = nullptr;
+    double *mx = nullptr, *my = nullptr;
+    // operators (host copies, nz x nz row-major)
+    std::vector<double> Lz, Lz1, zz;
+    // state
+    double2 *psi = nullptr;
+    double *at = nullptr, *ax = nullptr, *ay = nullptr, *rho = nullptr;
+    // stage input and accumulators
+    double2 *ypsi = nullptr, *kpsi = nullptr;
+    double *yax = nullptr, *yay = nullptr, *kax = nullptr, *kay = nullptr, *krho = nullptr;
+    // derivatives
+    double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr;
+    double *dxxay = nullptr, *divA = nullptr, *dxB = nullptr, *dyB = nullptr;
+    double *dxat = nullptr, *dyat = nullptr, *dat = nullptr, *dxax = nullptr;
+    double2 *O = nullptr;
+    double *partial = nullptr;
+    int *d_int = nullptr;  // scratch ints (winding, counts)
+    DevStatus *st = nullptr;
+    // launch geometry
+    int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
+    // state arrays the step acts on (internal buffers, or the caller's
+    // device arrays for hqt_step_device)
+    double2 *cpsi = nullptr;
+    double *cat = nullptr, *cax = nullptr, *cay = nullptr;
+    // CUDA graph of one step, captured for the state pointers above
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+    // profiling: CUDA events around every launch (graphs are bypassed)
+    bool prof_on = false;
+    bool capturing = false;
+    struct ProfEv {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfEv> prof_ev;
+    std::vector<long long> prof_count;
+    std::vector<double> prof_ms;
+    long long launches = 0;
+    std::vector<void *> allocs;
+    std::string err;
+};
+
+static thread_local std::string g_create_err;
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int fail(hqt_ctx *c, int code, const std::string &msg) {
+    if (c)
+        c->err = msg;
+    else
+        g_create_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(c, HQT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// kernel kinds reported by hqt_profile_report
+enum Kind {
+    K_X_RHS, K_Y_RHS, K_ZSTAGE, K_X_D1, K_Y_D1, K_ZCONS, K_ZMISC, K_WIND, K_FILT_X_FWD,
+    K_FILT_Y, K_FILT_X_INV, K_PHASE, K_STEP_END, K_COUNT, K_RHO, K_NKINDS
+};
+const char *const kKindName[K_NKINDS] = {
+    "x_rhs", "y_rhs", "zstage", "x_d1", "y_d1", "zcons", "zcol_misc", "winding",
+    "filter_x_fwd", "filter_y", "filter_x_inv", "phase_multiply", "step_end",
+    "count_vortices", "rho_gather_scatter"};
+
+struct Prof {
+    hqt_ctx *c;
+    int kind;
+    cudaEvent_t a = nullptr;
+    Prof(hqt_ctx *c_, int k, int nlaunch = 1) : c(c_), kind(k) {
+        c->launches += nlaunch;
+        if (c->prof_on && !c->capturing) {
+            cudaEventCreate(&a);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~Prof() {
+        if (a) {
+            cudaEvent_t b;
+            cudaEventCreate(&b);
+            cudaEventRecord(b, c->stream);
+            c->prof_ev.push_back({kind, a, b});
+        }
+    }
+};
+
+template <typename P> int dalloc(hqt_ctx *c, P **ptr, size_t bytes) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(c, HQT_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemset(q, 0, bytes);
+    c->allocs.push_back(q);
+    *ptr = reinterpret_cast<P *>(q);
+    return HQT_OK;
+}
+
+size_t smem_x(int n, int nbuf, int NB) { return sizeof(double2) * (size_t)n * (1 + (size_t)nbuf * NB); }
+
+int pick_lines(int n, int nbuf, int cap) {
+    int NB = (int)((kSmemBudget / sizeof(double2) / (size_t)n - 1) / nbuf);
+    if (NB < 1) NB = 1;
+    if (NB > cap) NB = cap;
+    return NB;
+}
+
+ZHost zhost(const hqt_ctx *c) { return ZHost{c->nz, c->Lz.data(), c->Lz1.data(), c->zz.data()}; }
+
+size_t smem_z(int NZP) { return sizeof(double) * 4 * (size_t)NZP * kThreadsZ; }
+
+// ---------------------------------------------------------------- launches
+int launch_x_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double *ay) {
+    XRhsArgs<double> a{};
+    a.plan = c->planx;
+    a.roots = c->rootsx;
+    a.NB = c->NBx_rhs;
+    a.nlines = c->ny * c->nz;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    a.s1 = two_pi / c->p.Lx / c->nx;
+    a.s2 = -(two_pi / c->p.Lx) * (two_pi / c->p.Lx) / c->nx;
+    a.psi = psi;
+    a.ax = ax;
+    a.ay = ay;
+    a.dxpsi = c->dxpsi;
+    a.dxxpsi = c->dxxpsi;
+    a.E = c->E;
+    a.dxxay = c->dxxay;
+    const int grid = (a.nlines + a.NB - 1) / a.NB;
+    Prof pr(c, K_X_RHS);
+    CK(launch_x_rhs(a, grid, smem_x(c->nx, 3, a.NB), c->stream));
+    return HQT_OK;
+}
+
+int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double *ay) {
+    YRhsArgs<double> a{};
+    a.plan = c->plany;
+    a.roots = c->rootsy;
+    a.TX = c->TXy_rhs;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    a.s1 = two_pi / c->p.Ly / c->ny;
+    a.s2 = -(two_pi / c->p.Ly) * (two_pi / c->p.Ly) / c->ny;
+    a.psi = psi;
+    a.ax = ax;
+    a.ay = ay;
+    a.E = c->E;
+    a.dxxpsi = c->dxxpsi;
+    a.dxxay = c->dxxay;
+    a.dypsi = c->dypsi;
+    a.lap = c->dxxpsi;
+    a.divA = c->divA;
+    a.dxB = c->dxB;
+    a.dyB = c->dyB;
+    dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
+    Prof pr(c, K_Y_RHS);
+    CK(launch_y_rhs(a, grid, smem_x(c->ny, 4, a.TX), c->stream));
+    return HQT_OK;
+}
+
+int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out) {
+    XD1Args<double> a{};
+    a.plan = c->planx;
+    a.roots = c->rootsx;
+    a.NB = c->NBx_2;
+    a.nlines = c->ny * c->nz;
+    a.s1 = 2.0 * 3.14159265358979323846 / c->p.Lx / c->nx;
+    a.in = in;
+    a.out = out;
+    const int grid = (a.nlines + a.NB - 1) / a.NB;
+    Prof pr(c, K_X_D1);
+    CK(launch_x_d1(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+    return HQT_OK;
+}
+
+int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<double> out) {
+    YD1Args<double> a{};
+    a.plan = c->plany;
+    a.roots = c->rootsy;
+    a.TX = c->TXy_2;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.s1 = 2.0 * 3.14159265358979323846 / c->p.Ly / c->ny;
+    a.in = in;
+    a.add_re = add_re;
+    a.out = out;
+    dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
+    Prof pr(c, K_Y_D1);
+    CK(launch_y_d1(a, grid, smem_x(c->ny, 2, a.TX), c->stream));
+    return HQT_OK;
+}
+
+// Filter nf (<= 3) complex fields in place through the x-spectra buffers.
+int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<double> *out,
+                  bool phase, bool check) {
+    double2 *spec[3] = {c->dxpsi, c->dypsi, c->E};
+    {
+        XFiltFwdArgs<double> a{};
+        a.plan = c->planx;
+        a.roots = c->rootsx;
+        a.NB = c->NBx_2;
+        a.nlines = c->ny * c->nz;
+        a.ny = c->ny;
+        a.nf = nf;
+        for (int f = 0; f < nf; ++f) {
+            a.in[f] = in[f];
+            a.spec[f] = spec[f];
+        }
+        a.st = phase ? c->st : nullptr;
+        const int grid = (a.nlines + a.NB - 1) / a.NB;
+        Prof pr(c, K_FILT_X_FWD);
+        CK(launch_x_filt_fwd(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+    }
+    {
+        YFiltArgs<double> a{};
+        a.plan = c->plany;
+        a.roots = c->rootsy;
+        a.TX = c->TXy_filt;
+        a.nx = c->nx;
+        a.ny = c->ny;
+        a.nf = nf;
+        for (int f = 0; f < nf; ++f) a.spec[f] = spec[f];
+        a.mx = c->mx;
+        a.my = c->my;
+        a.scale = 1.0 / ((double)c->nx * (double)c->ny);
+        dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
+        Prof pr(c, K_FILT_Y);
+        CK(launch_y_filt(a, grid, smem_x(c->ny, 2, a.TX * 3), c->stream));
+    }
+    {
+        XFiltInvArgs<double> a{};
+        a.plan = c->planx;
+        a.roots = c->rootsx;
+        a.NB = c->NBx_2;
+        a.nlines = c->ny * c->nz;
+        a.nf = nf;
+        for (int f = 0; f < nf; ++f) {
+            a.spec[f] = spec[f];
+            a.out[f] = out[f];
+        }
+        a.st = check ? c->st : nullptr;
+        const int grid = (a.nlines + a.NB - 1) / a.NB;
+        Prof pr(c, K_FILT_X_INV);
+        CK(launch_x_filt_inv(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+    }
+    return HQT_OK;
+}
+
+template <int MODE> int launch_zstage(hqt_ctx *c, const ZStageArgs<double, double> &a) {
+    const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
+    const ZHost h = zhost(c);
+    Prof pr(c, K_ZSTAGE);
+    switch (c->NZP) {
+#define HQT_Z(N)                                                                      \
+    case N:                                                                           \
+        CK(z_stage<N>(MODE, a, h, grid, kThreadsZ, smem_z(N), c->stream));            \
+        return HQT_OK;
+        HQT_NZP_LIST(HQT_Z)
+#undef HQT_Z
+    }
+    return fail(c, HQT_EUNSUPPORTED, "unsupported nz");
+}
+
+int launch_zcons(hqt_ctx *c) {
+    ZConsArgs<double> a{};
+    a.nz = c->nz;
+    a.plane = c->plane;
+    a.mu = c->p.mu;
+    a.vy = c->p.vy;
+    a.psi = c->cpsi;
+    a.ax = c->cax;
+    a.ay = c->cay;
+    a.at = c->cat;
+    a.dat = c->dat;
+    a.divA = c->divA;
+    a.rho = c->rho;
+    a.O = c->O;
+    const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
+    Prof pr(c, K_ZCONS);
+    switch (c->NZP) {
+#define HQT_Z(N)                                              \
+    case N:                                                   \
+        CK(z_cons<N>(a, zhost(c), grid, kThreadsZ, c->stream)); \
+        return HQT_OK;
+        HQT_NZP_LIST(HQT_Z)
+#undef HQT_Z
+    }
+    return fail(c, HQT_EUNSUPPORTED, "unsupported nz");
+}
+
+int launch_zcol_misc(hqt_ctx *c, const double *at, double *dat, const double2 *psi, double2 *O) {
+    ZColArgs<double> a{};
+    a.nz = c->nz;
+    a.plane = c->plane;
+    a.at = at;
+    a.dat = dat;
+    a.psi = psi;
+    a.O = O;
+    const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
+    Prof pr(c, K_ZMISC);
+    switch (c->NZP) {
+#define HQT_Z(N)                                              \
+    case N:                                                   \
+        CK(z_misc<N>(a, zhost(c), grid, kThreadsZ, c->stream)); \
+        return HQT_OK;
+        HQT_NZP_LIST(HQT_Z)
+#undef HQT_Z
+    }
+    return fail(c, HQT_EUNSUPPORTED, "unsupported nz");
+}
+
+int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
+    Prof pr(c, K_WIND, 2);
+    k_wind_partial<<<kPartials, kRedThreads, 0, c->stream>>>(O, c->nx, c->ny, c->partial);
+    CK(cudaGetLastError());
+    k_wind_final<<<1, kRedThreads, 0, c->stream>>>(c->partial, kPartials, c->ny, c->st, out);
+    CK(cudaGetLastError());
+    return HQT_OK;
+}
+
+#define RC(call)                         \
+    do {                                 \
+        int r_ = (call);                 \
+        if (r_ != HQT_OK) return r_;     \
+    } while (0)
+
+// ---------------------------------------------------------------- one step
+int enqueue_step(hqt_ctx *c) {
+    double2 *psi = c->cpsi;
+    double *at = c->cat, *ax = c->cax, *ay = c->cay;
+    // A_t is frozen during the four stages: its horizontal derivatives once
+    RC(launch_x_d1(c, FieldIn<double>{nullptr, at, nullptr},
+                   FieldOut<double>{nullptr, c->dxat, nullptr}));
+    RC(launch_y_d1(c, FieldIn<double>{nullptr, at, nullptr}, nullptr,
+                   FieldOut<double>{nullptr, c->dyat, nullptr}));
+    for (int s = 1; s <= 4; ++s) {
+        const double2 *ypsi = (s == 1) ? psi : c->ypsi;
+        const double *yax = (s == 1) ? ax : c->yax;
+        const double *yay = (s == 1) ? ay : c->yay;
+        RC(launch_x_rhs(c, ypsi, yax, yay));
+        RC(launch_y_rhs(c, ypsi, yax, yay));
+        ZStageArgs<double, double> a{};
+        a.nz = c->nz;
+        a.plane = c->plane;
+        a.h = c->p.dt;
+        a.ypsi = ypsi;
+        a.yax = yax;
+        a.yay = yay;
+        a.at = at;
+        a.dat = c->dat;
+        a.dxat = c->dxat;
+        a.dyat = c->dyat;
+        a.dxpsi = c->dxpsi;
+        a.dypsi = c->dypsi;
+        a.lap = c->dxxpsi;
+        a.divA = c->divA;
+        a.dxB = c->dxB;
+        a.dyB = c->dyB;
+        a.zpsi = psi;
+        a.zax = ax;
+        a.zay = ay;
+        a.zrho = c->rho;
+        a.kpsi = c->kpsi;
+        a.kax = c->kax;
+        a.kay = c->kay;
+        a.krho = c->krho;
+        a.npsi = c->ypsi;
+        a.nax = c->yax;
+        a.nay = c->yay;
+        a.wpsi = psi;
+        a.wax = ax;
+        a.way = ay;
+        a.wrho = c->rho;
+        switch (s) {
+            case 1: RC(launch_zstage<1>(c, a)); break;
+            case 2: RC(launch_zstage<2>(c, a)); break;
+            case 3: RC(launch_zstage<3>(c, a)); break;
+            default: RC(launch_zstage<4>(c, a)); break;
+        }
+    }
+    // constraint: div A of the combined fields, then A_t, BCs, O
+    RC(launch_x_d1(c, FieldIn<double>{nullptr, ax, nullptr},
+                   FieldOut<double>{nullptr, c->dxax, nullptr}));
+    RC(launch_y_d1(c, FieldIn<double>{nullptr, ay, nullptr}, c->dxax,
+                   FieldOut<double>{nullptr, c->divA, nullptr}));
+    RC(launch_zcons(c));
+    if (c->p.remove_winding) RC(launch_winding(c, c->O, nullptr));
+    if (c->p.apply_filter) {
+        FieldIn<double> in[3] = {{psi, nullptr, nullptr}, {nullptr, at, c->dat}, {nullptr, ax, ay}};
+        FieldOut<double> out[3] = {{psi, nullptr, nullptr}, {nullptr, at, c->dat}, {nullptr, ax, ay}};
+        RC(launch_filter(c, 3, in, out, c->p.remove_winding != 0, true));
+    } else if (c->p.remove_winding) {
+        Prof pr(c, K_PHASE);
+        k_phase_multiply<<<592, 256, 0, c->stream>>>(psi, c->nx, c->ny, c->vol, c->st);
+        CK(cudaGetLastError());
+    }
+    {
+        Prof pr(c, K_STEP_END);
+        k_step_end<<<1, 32, 0, c->stream>>>(c->st);
+        CK(cudaGetLastError());
+    }
+    return HQT_OK;
+}
+
+void drop_graph(hqt_ctx *c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+}
+
+int build_graph(hqt_ctx *c) {
+    const void *key[4] = {c->cpsi, c->cat, c->cax, c->cay};
+    if (c->gexec && std::memcmp(key, c->graph_key, sizeof(key)) == 0) return HQT_OK;
+    drop_graph(c);
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->capturing = true;
+    const long long l0 = c->launches;
+    const int r = enqueue_step(c);
+    c->launches = l0;
+    c->capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r != HQT_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(c, HQT_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    std::memcpy(c->graph_key, key, sizeof(key));
+    return HQT_OK;
+}
+
+// kernels one captured step launches (counted by a dry count of enqueue_step)
+long long launches_per_step(hqt_ctx *c) {
+    long long n = 2 + 4 * 3 + 2 + 1 + 1;
+    if (c->p.remove_winding) n += 2;
+    if (c->p.apply_filter)
+        n += 3;
+    else if (c->p.remove_winding)
+        n += 1;
+    return n;
+}
+
+int count_vortices_dev(hqt_ctx *c, const double2 *O, int32_t *n, int32_t *np, int32_t *nm) {
+    CK(cudaMemsetAsync(c->d_int, 0, 4 * sizeof(int), c->stream));
+    {
+        Prof pr(c, K_COUNT);
+        k_count_vortices<<<kPartials, kRedThreads, 0, c->stream>>>(O, c->nx, c->ny, c->d_int);
+        CK(cudaGetLastError());
+    }
+    int h[4];
+    CK(cudaMemcpyAsync(h, c->d_int, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (n) *n = h[0];
+    if (np) *np = h[1];
+    if (nm) *nm = h[2];
+    return HQT_OK;
+}
+
+// Advance the current state nsteps steps.
+int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
+    DevStatus h0{};
+    CK(cudaMemcpyAsync(&h0, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const long long step0 = h0.step;
+    h0.first_bad_step = LLONG_MAX;
+    h0.winding = 0;
+    CK(cudaMemcpyAsync(c->st, &h0, sizeof(DevStatus), cudaMemcpyHostToDevice, c->stream));
+    // d_z A_t of the incoming potential
+    RC(launch_zcol_misc(c, c->cat, c->dat, nullptr, nullptr));
+    if (!c->prof_on) RC(build_graph(c));
+    if (diag) {
+        diag->n_records = 0;
+        diag->nonfinite_step = -1;
+        diag->steps_done = 0;
+    }
+    int64_t done = 0;
+    bool bad = false;
+    const int every = c->p.diag_every;
+    for (int64_t s = 0; s < nsteps; ++s) {
+        if (c->prof_on) {
+            RC(enqueue_step(c));
+        } else {
+            CK(cudaGraphLaunch(c->gexec, c->stream));
+            c->launches += launches_per_step(c);
+        }
+        ++done;
+        const long long gstep = step0 + done;
+        if (every > 0 && gstep % every == 0 && diag && diag->records &&
+            diag->n_records < diag->capacity) {
+            RC(launch_zcol_misc(c, nullptr, nullptr, c->cpsi, c->O));
+            int32_t n = 0, np = 0, nm = 0;
+            RC(count_vortices_dev(c, c->O, &n, &np, &nm));
+            int32_t *r = diag->records + 4 * diag->n_records;
+            r[0] = (int32_t)gstep;
+            r[1] = n;
+            r[2] = np;
+            r[3] = nm;
+            diag->n_records++;
+        }
+        if ((done % 64) == 0 || done == nsteps) {
+            DevStatus h{};
+            CK(cudaMemcpyAsync(&h, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            if (h.first_bad_step != LLONG_MAX) {
+                bad = true;
+                if (diag) diag->nonfinite_step = h.first_bad_step - step0;
+                break;
+            }
+        }
+    }
+    DevStatus h{};
+    CK(cudaMemcpyAsync(&h, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (diag) {
+        diag->steps_done = done;
+        diag->last_winding = h.winding;
+    }
+    if (bad) return fail(c, HQT_ENONFINITE, "non-finite value in the evolved fields");
+    return HQT_OK;
+}
+
+void use_internal_state(hqt_ctx *c) {
+    c->cpsi = c->psi;
+    c->cat = c->at;
+    c->cax = c->ax;
+    c->cay = c->ay;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int hqt_abi_version(void) { return HQT_ABI_VERSION; }
+
+const char *hqt_last_error(const hqt_ctx *ctx) {
+    if (ctx) return ctx->err.c_str();
+    return g_create_err.c_str();
+}
+
+
+int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
+    hqt_ctx *c = nullptr;
+    if (!params || !out) return fail(nullptr, HQT_EINVAL, "null argument");
+    *out = nullptr;
+    const hqt_params &p = *params;
+    if (p.nx < 4 || p.ny < 4) return fail(nullptr, HQT_EINVAL, "nx, ny must be >= 4");
+    if (p.nz < 3 || p.nz > 40) return fail(nullptr, HQT_EUNSUPPORTED, "nz must be in [3, 40]");
+    if (!(p.Lx > 0) || !(p.Ly > 0) || !std::isfinite(p.Lx) || !std::isfinite(p.Ly))
+        return fail(nullptr, HQT_EINVAL, "box lengths must be positive");
+    if (!std::isfinite(p.dt) || !std::isfinite(p.mu) || !std::isfinite(p.vy))
+        return fail(nullptr, HQT_EINVAL, "dt, mu, vy must be finite");
+    if (p.precision != HQT_FP64 && p.precision != HQT_MIXED)
+        return fail(nullptr, HQT_EINVAL, "precision must be HQT_FP64 or HQT_MIXED");
+    if (p.precision == HQT_MIXED)
+        return fail(nullptr, HQT_EUNSUPPORTED, "mixed precision is not built in this library");
+    if ((long long)p.nx * p.ny * p.nz > (1LL << 31))
+        return fail(nullptr, HQT_EUNSUPPORTED, "grid too large");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(nullptr, HQT_ECUDA, "no such CUDA device");
+    DeviceGuard guard(device);
+
+    c = new hqt_ctx();
+    c->p = p;
+    c->device = device;
+    c->nx = p.nx;
+    c->ny = p.ny;
+    c->nz = p.nz;
+    c->plane = (long long)p.nx * p.ny;
+    c->vol = c->plane * p.nz;
+    c->NZP = 0;
+    for (int v : kNZP)
+        if (v >= p.nz) {
+            c->NZP = v;
+            break;
+        }
+    auto bail = [&](int code) {
+        g_create_err = c->err;
+        hqt_destroy(c);
+        return code;
+    };
+    if (!c->NZP) {
+        c->err = "nz too large";
+        return bail(HQT_EUNSUPPORTED);
+    }
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        c->err = "cudaStreamCreate failed";
+        return bail(HQT_ECUDA);
+    }
+    c->stream = c->own_stream;
+
+    // radial operators: Lz = 2*chebdif(nz,1), Lz1 = inv(Lz(1:nz-1,1:nz-1))
+    {
+        std::vector<double> x, D;
+        chebdif_host(p.nz, x, D);
+        const int nz = p.nz;
+        c->Lz.resize((size_t)nz * nz);
+        for (size_t i = 0; i < c->Lz.size(); ++i) c->Lz[i] = 2.0 * D[i];
+        c->zz.resize(nz);
+        for (int i = 0; i < nz; ++i) c->zz[i] = (x[i] - 1.0) * 1.0 / 2.0 + 1.0;
+        std::vector<double> A((size_t)(nz - 1) * (nz - 1));
+        for (int i = 0; i < nz - 1; ++i)
+            for (int j = 0; j < nz - 1; ++j) A[(size_t)i * (nz - 1) + j] = c->Lz[(size_t)i * nz + j];
+        if (!invert_host(nz - 1, A, c->Lz1)) {
+            c->err = "Lz(1:nz-1,1:nz-1) is singular";
+            return bail(HQT_EINVAL);
+        }
+    }
+    // Fourier plans, roots, filter masks
+    c->planx = make_plan(p.nx);
+    c->plany = make_plan(p.ny);
+    if (c->planx.npass > kMaxPass || c->plany.npass > kMaxPass) {
+        c->err = "line length has too many factors";
+        return bail(HQT_EUNSUPPORTED);
+    }
+    int rc = HQT_OK;
+    auto A = [&](auto **ptr, size_t bytes) {
+        if (rc == HQT_OK) rc = dalloc(c, ptr, bytes);
+    };
+    A(&c->rootsx, sizeof(double2) * p.nx);
+    A(&c->rootsy, sizeof(double2) * p.ny);
+    A(&c->mx, sizeof(double) * p.nx);
+    A(&c->my, sizeof(double) * p.ny);
+    const size_t V = (size_t)c->vol, P2 = (size_t)c->plane;
+    A(&c->psi, sizeof(double2) * V);
+    A(&c->at, sizeof(double) * V);
+    A(&c->ax, sizeof(double) * V);
+    A(&c->ay, sizeof(double) * V);
+    A(&c->rho, sizeof(double) * P2);
+    A(&c->ypsi, sizeof(double2) * V);
+    A(&c->yax, sizeof(double) * V);
+    A(&c->yay, sizeof(double) * V);
+    A(&c->kpsi, sizeof(double2) * V);
+    A(&c->kax, sizeof(double) * V);
+    A(&c->kay, sizeof(double) * V);
+    A(&c->krho, sizeof(double) * P2);
+    A(&c->dxpsi, sizeof(double2) * V);
+    A(&c->dxxpsi, sizeof(double2) * V);
+    A(&c->E, sizeof(double2) * V);
+    A(&c->dypsi, sizeof(double2) * V);
+    A(&c->dxxay, sizeof(double) * V);
+    A(&c->divA, sizeof(double) * V);
+    A(&c->dxB, sizeof(double) * V);
+    A(&c->dyB, sizeof(double) * V);
+    A(&c->dxat, sizeof(double) * V);
+    A(&c->dyat, sizeof(double) * V);
+    A(&c->dat, sizeof(double) * V);
+    A(&c->dxax, sizeof(double) * V);
+    A(&c->O, sizeof(double2) * P2);
+    A(&c->partial, sizeof(double) * kPartials);
+    A(&c->d_int, sizeof(int) * 8);
+    A(&c->st, sizeof(DevStatus));
+    if (rc != HQT_OK) return bail(rc);
+    {
+        std::vector<double2> rx = make_roots(p.nx), ry = make_roots(p.ny);
+        std::vector<double> hmx(p.nx, 1.0), hmy(p.ny, 1.0);
+        int lo, hi;
+        filter_band(p.nx, lo, hi);
+        for (int i = lo - 1; i <= hi - 1; ++i)
+            if (i >= 0 && i < p.nx) hmx[i] = 0.0;
+        filter_band(p.ny, lo, hi);
+        for (int i = lo - 1; i <= hi - 1; ++i)
+            if (i >= 0 && i < p.ny) hmy[i] = 0.0;
+        DevStatus s0{};
+        s0.first_bad_step = LLONG_MAX;
+        if (cudaMemcpy(c->rootsx, rx.data(), sizeof(double2) * p.nx, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->rootsy, ry.data(), sizeof(double2) * p.ny, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->mx, hmx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->my, hmy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->st, &s0, sizeof(s0), cudaMemcpyHostToDevice)) {
+            c->err = "operator upload failed";
+            return bail(HQT_ECUDA);
+        }
+    }
+    // launch geometry and shared-memory opt-in
+    c->NBx_rhs = pick_lines(p.nx, 3, 32);
+    c->NBx_2 = pick_lines(p.nx, 2, 32);
+    c->TXy_rhs = pick_lines(p.ny, 4, 16);
+    c->TXy_2 = pick_lines(p.ny, 2, 16);
+    c->TXy_filt = pick_lines(p.ny, 6, 16);
+    {
+        const size_t lim = 227 * 1024 - 1024;
+        const size_t need = std::max({smem_x(p.nx, 3, c->NBx_rhs), smem_x(p.ny, 4, c->TXy_rhs),
+                                      smem_x(p.nx, 2, c->NBx_2), smem_x(p.ny, 2, c->TXy_2),
+                                      smem_x(p.ny, 2, 3 * c->TXy_filt)});
+        if (need > lim) {
+            c->err = "line length too large for the shared-memory line transforms";
+            return bail(HQT_EUNSUPPORTED);
+        }
+    }
+    {
+        const int maxs = 227 * 1024;
+        std::vector<double> tc, ts;
+        make_radix_tables(tc, ts);
+        cudaError_t e = fft_init(tc.data(), ts.data(), (int)tc.size(), maxs);
+#define HQT_Z(N) \
+    if (e == cudaSuccess) e = z_init<N>(maxs);
+        HQT_NZP_LIST(HQT_Z)
+#undef HQT_Z
+        if (e != cudaSuccess) {
+            c->err = std::string("kernel set-up: ") + cudaGetErrorString(e);
+            return bail(HQT_ECUDA);
+        }
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        c->err = "initialisation failed";
+        return bail(HQT_ECUDA);
+    }
+    use_internal_state(c);
+    c->prof_count.assign(K_NKINDS, 0);
+    c->prof_ms.assign(K_NKINDS, 0.0);
+    *out = c;
+    return HQT_OK;
+}
+
+void hqt_destroy(hqt_ctx *c) {
+    if (!c) return;
+    DeviceGuard guard(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    for (auto &e : c->prof_ev) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    for (void *q : c->allocs) cudaFree(q);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+int hqt_set_stream(hqt_ctx *c, void *s) {
+    if (!c) return HQT_EINVAL;
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    c->stream = s ? reinterpret_cast<cudaStream_t>(s) : c->own_stream;
+    return HQT_OK;
+}
+
+int hqt_step(hqt_ctx *c, double *Z1, double *Z2, double *Z3, double *Z4, double *rhoi,
+             int64_t nsteps, hqt_diag *diag) {
+    if (!c) return HQT_EINVAL;
+    if (!Z1 || !Z2 || !Z3 || !Z4 || !rhoi || nsteps < 0) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    const size_t V = (size_t)c->vol;
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice, d2h = cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(c->psi, Z1, sizeof(double2) * V, h2d, c->stream));
+    CK(cudaMemcpyAsync(c->at, Z2, sizeof(double) * V, h2d, c->stream));
+    CK(cudaMemcpyAsync(c->ax, Z3, sizeof(double) * V, h2d, c->stream));
+    CK(cudaMemcpyAsync(c->ay, Z4, sizeof(double) * V, h2d, c->stream));
+    // rhoi is replicated along z: its boundary slice carries the data
+    CK(cudaMemcpyAsync(c->rho, rhoi + (size_t)(c->nz - 1) * c->plane,
+                       sizeof(double) * c->plane, h2d, c->stream));
+    use_internal_state(c);
+    const int r = run_steps(c, nsteps, diag);
+    CK(cudaMemcpyAsync(Z1, c->psi, sizeof(double2) * V, d2h, c->stream));
+    CK(cudaMemcpyAsync(Z2, c->at, sizeof(double) * V, d2h, c->stream));
+    CK(cudaMemcpyAsync(Z3, c->ax, sizeof(double) * V, d2h, c->stream));
+    CK(cudaMemcpyAsync(Z4, c->ay, sizeof(double) * V, d2h, c->stream));
+    for (int z = 0; z < c->nz; ++z)
+        CK(cudaMemcpyAsync(rhoi + (size_t)z * c->plane, c->rho, sizeof(double) * c->plane, d2h,
+                           c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return r;
+}
+
+int hqt_step_device(hqt_ctx *c, void *dZ1, void *dZ2, void *dZ3, void *dZ4, void *drhoi,
+                    int64_t nsteps, hqt_diag *diag) {
+    if (!c) return HQT_EINVAL;
+    if (!dZ1 || !dZ2 || !dZ3 || !dZ4 || !drhoi || nsteps < 0)
+        return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    // the kernels act on the caller's arrays directly; only rhoi is reduced
+    // to its boundary slice and replicated back
+    c->cpsi = (double2 *)dZ1;
+    c->cat = (double *)dZ2;
+    c->cax = (double *)dZ3;
+    c->cay = (double *)dZ4;
+    {
+        Prof pr(c, K_RHO);
+        k_rho_gather<<<296, 256, 0, c->stream>>>((const double *)drhoi, c->nz, c->plane, c->rho);
+        CK(cudaGetLastError());
+    }
+    const int r = run_steps(c, nsteps, diag);
+    {
+        Prof pr(c, K_RHO);
+        k_rho_scatter<<<296, 256, 0, c->stream>>>(c->rho, c->nz, c->plane, (double *)drhoi);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return r;
+}
+
+int hqt_profile(hqt_ctx *c, int enable) {
+    if (!c) return HQT_EINVAL;
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &e : c->prof_ev) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    c->prof_ev.clear();
+    c->prof_count.assign(K_NKINDS, 0);
+    c->prof_ms.assign(K_NKINDS, 0.0);
+    c->launches = 0;
+    c->prof_on = enable != 0;
+    return HQT_OK;
+}
+
+int hqt_profile_report(hqt_ctx *c, char *buf, int64_t len) {
+    if (!c || !buf || len <= 0) return HQT_EINVAL;
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->prof_count.size() != K_NKINDS) {
+        c->prof_count.assign(K_NKINDS, 0);
+        c->prof_ms.assign(K_NKINDS, 0.0);
+    }
+    for (auto &e : c->prof_ev) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.a, e.b);
+        c->prof_count[e.kind] += 1;
+        c->prof_ms[e.kind] += ms;
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    c->prof_ev.clear();
+    std::string out = "{\"launches\": " + std::to_string(c->launches) + ", \"kernels\": [";
+    bool first = true;
+    for (int k = 0; k < K_NKINDS; ++k) {
+        if (!c->prof_count[k]) continue;
+        char tmp[160];
+        std::snprintf(tmp, sizeof(tmp), "%s{\"kernel\": \"%s\", \"launches\": %lld, \"ms\": %.6f}",
+                      first ? "" : ", ", kKindName[k], c->prof_count[k], c->prof_ms[k]);
+        out += tmp;
+        first = false;
+    }
+    out += "]}";
+    if ((int64_t)out.size() + 1 > len) return fail(c, HQT_EINVAL, "report buffer too small");
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    return HQT_OK;
+}
+
+int hqt_rhs_device(hqt_ctx *c, const void *dZ1, const void *dZ2, const void *dZ3,
+                   const void *dZ4, void *dF1, void *dF3, void *dF4, void *dF2b) {
+    if (!c) return HQT_EINVAL;
+    if (!dZ1 || !dZ2 || !dZ3 || !dZ4 || !dF1 || !dF3 || !dF4 || !dF2b)
+        return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    const double2 *psi = (const double2 *)dZ1;
+    const double *at = (const double *)dZ2, *ax = (const double *)dZ3, *ay = (const double *)dZ4;
+    RC(launch_x_d1(c, FieldIn<double>{nullptr, at, nullptr}, FieldOut<double>{nullptr, c->dxat, nullptr}));
+    RC(launch_y_d1(c, FieldIn<double>{nullptr, at, nullptr}, nullptr,
+                   FieldOut<double>{nullptr, c->dyat, nullptr}));
+    RC(launch_zcol_misc(c, at, c->dat, nullptr, nullptr));
+    RC(launch_x_rhs(c, psi, ax, ay));
+    RC(launch_y_rhs(c, psi, ax, ay));
+    ZStageArgs<double, double> a{};
+    a.nz = c->nz;
+    a.plane = c->plane;
+    a.h = c->p.dt;
+    a.ypsi = psi;
+    a.yax = ax;
+    a.yay = ay;
+    a.at = at;
+    a.dat = c->dat;
+    a.dxat = c->dxat;
+    a.dyat = c->dyat;
+    a.dxpsi = c->dxpsi;
+    a.dypsi = c->dypsi;
+    a.lap = c->dxxpsi;
+    a.divA = c->divA;
+    a.dxB = c->dxB;
+    a.dyB = c->dyB;
+    a.f1 = (double2 *)dF1;
+    a.f3 = (double *)dF3;
+    a.f4 = (double *)dF4;
+    a.f2b = (double *)dF2b;
+    RC(launch_zstage<0>(c, a));
+    CK(cudaStreamSynchronize(c->stream));
+    return HQT_OK;
+}
+
+int hqt_filter_device(hqt_ctx *c, const void *din, void *dout, int32_t nfields) {
+    if (!c) return HQT_EINVAL;
+    if (!din || !dout || nfields < 0) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    const double *in = (const double *)din;
+    double *out = (double *)dout;
+    const size_t V = (size_t)c->vol;
+    int f = 0;
+    while (f < nfields) {
+        FieldIn<double> fi[3];
+        FieldOut<double> fo[3];
+        int nf = 0;
+        while (nf < 3 && f < nfields) {
+            const bool pair = (f + 1 < nfields);
+            fi[nf] = FieldIn<double>{nullptr, in + f * V, pair ? in + (f + 1) * V : nullptr};
+            fo[nf] = FieldOut<double>{nullptr, out + f * V, pair ? out + (f + 1) * V : nullptr};
+            f += pair ? 2 : 1;
+            ++nf;
+        }
+        RC(launch_filter(c, nf, fi, fo, false, false));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return HQT_OK;
+}
+
+int hqt_boundary_order_parameter_device(hqt_ctx *c, const void *dZ1, void *dO) {
+    if (!c) return HQT_EINVAL;
+    if (!dZ1 || !dO) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    RC(launch_zcol_misc(c, nullptr, nullptr, (const double2 *)dZ1, (double2 *)dO));
+    CK(cudaStreamSynchronize(c->stream));
+    return HQT_OK;
+}
+
+int hqt_winding_device(hqt_ctx *c, const void *dO, int32_t *winding) {
+    if (!c) return HQT_EINVAL;
+    if (!dO || !winding) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    RC(launch_winding(c, (const double2 *)dO, c->d_int + 4));
+    int w = 0;
+    CK(cudaMemcpyAsync(&w, c->d_int + 4, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *winding = w;
+    return HQT_OK;
+}
+
+int hqt_count_vortices_device(hqt_ctx *c, const void *dO, int32_t *n, int32_t *np, int32_t *nm) {
+    if (!c) return HQT_EINVAL;
+    if (!dO) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    return count_vortices_dev(c, (const double2 *)dO, n, np, nm);
+}
+
+int hqt_count_vortices(hqt_ctx *c, const double *O, int32_t *n, int32_t *np, int32_t *nm) {
+    if (!c) return HQT_EINVAL;
+    if (!O) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(c->O, O, sizeof(double2) * c->plane, cudaMemcpyHostToDevice, c->stream));
+    return count_vortices_dev(c, c->O, n, np, nm);
+}
+
+}  // extern "C"

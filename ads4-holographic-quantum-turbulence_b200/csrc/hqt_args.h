@@ -1,0 +1,147 @@
+// hqt_args.h -- kernel argument blocks (plain structs, host and device).
+#pragma once
+#include "hqt_common.cuh"
+
+namespace hqt {
+
+constexpr int kMaxFilt = 4;
+
+template <typename T> struct FieldIn {
+    const C2<T> *c;  // interleaved complex source, or
+    const T *re;     // split real / imaginary sources (im may be null)
+    const T *im;
+};
+
+template <typename T> struct FieldOut {
+    C2<T> *c;
+    T *re;
+    T *im;
+};
+
+template <typename T> struct XRhsArgs {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int NB, nlines;
+    T s1, s2;
+    const C2<T> *psi;
+    const T *ax, *ay;
+    C2<T> *dxpsi, *dxxpsi, *E;
+    T *dxxay;
+};
+
+template <typename T> struct YRhsArgs {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int TX, nx, ny;
+    T s1, s2;
+    const C2<T> *psi;
+    const T *ax, *ay;
+    const C2<T> *E;       // d_x A_x + i d_x A_y
+    const C2<T> *dxxpsi;  // read, may alias lap
+    const T *dxxay;
+    C2<T> *dypsi, *lap;
+    T *divA, *dxB, *dyB;
+};
+
+template <typename T> struct XD1Args {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int NB, nlines;
+    T s1;
+    FieldIn<T> in;
+    FieldOut<T> out;
+};
+
+template <typename T> struct YD1Args {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int TX, nx, ny;
+    T s1;
+    FieldIn<T> in;
+    const T *add_re;  // optional: out.re = add_re + Re(d_y in)
+    FieldOut<T> out;
+};
+
+template <typename T> struct XFiltFwdArgs {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int NB, nlines, ny;
+    int nf;
+    FieldIn<T> in[kMaxFilt];
+    C2<T> *spec[kMaxFilt];
+    const DevStatus *st;  // phase e^{-2 pi i y w/ny} on field 0 when non-null
+};
+
+template <typename T> struct YFiltArgs {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int TX, nx, ny;
+    int nf;
+    C2<T> *spec[kMaxFilt];
+    const T *mx, *my;  // 1 - fx, 1 - fy
+    T scale;           // 1/(nx*ny)
+};
+
+template <typename T> struct XFiltInvArgs {
+    FFTPlan plan;
+    const C2<T> *roots;
+    int NB, nlines;
+    int nf;
+    const C2<T> *spec[kMaxFilt];
+    FieldOut<T> out[kMaxFilt];
+    DevStatus *st;  // non-finite check when non-null
+};
+
+template <typename T, int NZP> struct ZOps {
+    T Lz[NZP][NZP];
+    T Lz1[NZP][NZP];
+    T zz[NZP];
+    T fz[NZP];   // 1 - z^3
+    T lzb[NZP];  // boundary row Lz(nz, :)
+};
+
+template <typename T, typename TS> struct ZStageArgs {
+    int nz;
+    long long plane;  // nx*ny
+    TS h;
+    // stage inputs (type T)
+    const C2<T> *ypsi;
+    const T *yax, *yay;
+    const T *at, *dat, *dxat, *dyat;
+    const C2<T> *dxpsi, *dypsi, *lap;
+    const T *divA, *dxB, *dyB;
+    // RK state and accumulators (type TS)
+    const C2<TS> *zpsi;
+    const TS *zax, *zay, *zrho;
+    C2<TS> *kpsi;
+    TS *kax, *kay, *krho;
+    C2<T> *npsi;  // next stage input
+    T *nax, *nay;
+    C2<TS> *wpsi;  // new state (stage 4)
+    TS *wax, *way, *wrho;
+    // right-hand-side outputs (MODE 0)
+    C2<T> *f1;
+    T *f3, *f4, *f2b;
+};
+
+template <typename T> struct ZConsArgs {
+    int nz;
+    long long plane;
+    T mu, vy;
+    C2<T> *psi;
+    T *ax, *ay, *at, *dat;
+    const T *divA;
+    const T *rho;  // 2-D
+    C2<T> *O;      // 2-D boundary order parameter (may be null)
+};
+
+template <typename T> struct ZColArgs {
+    int nz;
+    long long plane;
+    const T *at;
+    T *dat;
+    const C2<T> *psi;
+    C2<T> *O;
+};
+
+}  // namespace hqt

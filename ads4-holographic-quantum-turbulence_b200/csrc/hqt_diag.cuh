@@ -1,0 +1,142 @@
+// hqt_diag.cuh -- reductions on the boundary order parameter O(x, y).
+//
+// * winding: round(mean_y(sum_x angle(O(x,y+1)/O(x,y)))/(2*pi)) of
+//   scripts/simulation/tevol_driven_cluster.m:137, as a deterministic
+//   two-level sum (fixed per-block trees, then one fixed-order final tree).
+// * countN: the plaquette winding count of src/diagnostics/countN.m:7-21.
+//   The angle of a quotient a/b is taken as atan2 of a*conj(b), which has
+//   the same argument (|b|^2 > 0 only rescales); w is an integer up to
+//   rounding, so the +-1e-4 window classifies it identically.
+#pragma once
+#include "hqt_common.cuh"
+
+namespace hqt {
+
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double quot_angle(double2 a, double2 b) {
+    // angle(a./b)
+    const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+    const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
+    return atan2(im, re);
+}
+
+// partial[blockIdx.x] = sum over this block's sites of angle(O(x,y+1)/O(x,y))
+__global__ void __launch_bounds__(kRedThreads)
+    k_wind_partial(const double2 *O, int nx, int ny, double *partial) {
+    __shared__ double sh[kRedThreads];
+    const long long n = (long long)nx * ny;
+    double acc = 0.0;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(s % nx);
+        const int y = (int)(s / nx);
+        const int y1 = (y + 1 == ny) ? 0 : y + 1;
+        acc += quot_angle(O[(long long)y1 * nx + x], O[s]);
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// MATLAB round: halves away from zero.
+__device__ __forceinline__ double round_half_away(double v) {
+    return v >= 0.0 ? floor(v + 0.5) : -floor(-v + 0.5);
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+    k_wind_final(const double *partial, int nparts, int ny, DevStatus *st, int *out) {
+    __shared__ double sh[kRedThreads];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += partial[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double m = sh[0] / (double)ny;  // mean over y of the x-sums
+        const int w = (int)round_half_away(m / (2.0 * 3.14159265358979323846));
+        if (st) st->winding = w;
+        if (out) *out = w;
+    }
+}
+
+// counts[0..2] += (n, np, nm)
+__global__ void __launch_bounds__(kRedThreads)
+    k_count_vortices(const double2 *O, int nx, int ny, int *counts) {
+    __shared__ int sp[kRedThreads], sm[kRedThreads];
+    const long long n = (long long)nx * ny;
+    int cp = 0, cm = 0;
+    const double inv2pi = 1.0 / (2.0 * 3.14159265358979323846);
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % nx);
+        const int j = (int)(s / nx);
+        const int i1 = (i + 1 == nx) ? 0 : i + 1;
+        const int j1 = (j + 1 == ny) ? 0 : j + 1;
+        const double2 x1 = O[s];
+        const double2 x2 = O[(long long)j * nx + i1];
+        const double2 x3 = O[(long long)j1 * nx + i1];
+        const double2 x4 = O[(long long)j1 * nx + i];
+        const double w = inv2pi * (quot_angle(x1, x2) + quot_angle(x2, x3) +
+                                   quot_angle(x3, x4) + quot_angle(x4, x1));
+        if (w >= 1.0 - 1e-4 && w <= 1.0 + 1e-4) ++cp;
+        if (w <= -1.0 + 1e-4 && w >= -1.0 - 1e-4) ++cm;
+    }
+    sp[threadIdx.x] = cp;
+    sm[threadIdx.x] = cm;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sp[threadIdx.x] += sp[threadIdx.x + w];
+            sm[threadIdx.x] += sm[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&counts[0], sp[0] + sm[0]);
+        atomicAdd(&counts[1], sp[0]);
+        atomicAdd(&counts[2], sm[0]);
+    }
+}
+
+// Psi *= exp(-2 pi i y w / ny) over all z (winding removal without filter).
+__global__ void k_phase_multiply(double2 *psi, int nx, int ny, long long vol,
+                                 const DevStatus *st) {
+    const int w = st->winding;
+    if (w == 0) return;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)((s / nx) % ny);
+        const long long q = ((long long)y * w) % ny;
+        double sn, cs;
+        sincospi(-2.0 * (double)q / (double)ny, &sn, &cs);
+        const double2 v = psi[s];
+        psi[s] = make_double2(v.x * cs - v.y * sn, v.x * sn + v.y * cs);
+    }
+}
+
+// rhoi replicated along z -> 2-D, and back.
+__global__ void k_rho_gather(const double *rho3, int nz, long long plane, double *rho2) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < plane;
+         s += (long long)gridDim.x * blockDim.x)
+        rho2[s] = rho3[(long long)(nz - 1) * plane + s];
+}
+__global__ void k_rho_scatter(const double *rho2, int nz, long long plane, double *rho3) {
+    const long long vol = plane * nz;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
+         s += (long long)gridDim.x * blockDim.x)
+        rho3[s] = rho2[s % plane];
+}
+
+__global__ void k_step_end(DevStatus *st) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) st->step += 1;
+}
+
+}  // namespace hqt

@@ -1,0 +1,270 @@
+// hqt_fft.cuh -- batched mixed-radix FFT of periodic lines held in shared
+// memory.  Replaces the dense Fourier differentiation matrices
+// Lx = (2*pi/L0)*fourdif(nx,1) of scripts/simulation/tevol_driven_cluster.m:47-48
+// (applied by func_Lx / func_Ly, :60-61) and the fft2/ifft2 pair of
+// src/numerics/ff.m:7-11: the fourdif matrix equals the Fourier multiplier
+// i*k (Nyquist mode zeroed for even n), so a line transform, a diagonal
+// multiply and an inverse transform give the same derivative with
+// O(n log n) work instead of O(n^2).
+//
+// Algorithm: Stockham auto-sort, decimation in time, ping-pong between two
+// shared-memory buffers.  Pass p has radix R and Ns = product of the radices
+// of the earlier passes; butterfly j reads x[j + r*n/R], r < R, applies the
+// twiddles w_n^{r*(j mod Ns)*n/(Ns*R)}, does a radix-R DFT in registers and
+// writes to (j - j mod Ns)*R + j mod Ns + k*Ns.  Radices 2,4,8,16 use an
+// in-register radix-2 network; odd primes up to 47 use the real-pair
+// (cos/sin) form of the prime DFT; any other prime falls back to a direct
+// one-output-per-thread sum.
+#pragma once
+#include "hqt_dev.cuh"
+
+namespace hqt {
+
+// Defined here: this header is compiled into exactly one translation unit.
+__constant__ double c_tab_cos_d[kTabTotal];
+__constant__ double c_tab_sin_d[kTabTotal];
+__constant__ float c_tab_cos_f[kTabTotal];
+__constant__ float c_tab_sin_f[kTabTotal];
+
+template <typename T> struct Tab;
+template <> struct Tab<double> {
+    static __device__ __forceinline__ double c(int i) { return c_tab_cos_d[i]; }
+    static __device__ __forceinline__ double s(int i) { return c_tab_sin_d[i]; }
+};
+template <> struct Tab<float> {
+    static __device__ __forceinline__ float c(int i) { return c_tab_cos_f[i]; }
+    static __device__ __forceinline__ float s(int i) { return c_tab_sin_f[i]; }
+};
+
+
+// ---- radix-R DFTs in registers, results stored to shared memory -----------
+template <int R> struct Log2 { static constexpr int v = 1 + Log2<R / 2>::v; };
+template <> struct Log2<1> { static constexpr int v = 0; };
+
+template <int BITS> __host__ __device__ constexpr int bitrev(int i) {
+    int r = 0;
+    for (int b = 0; b < BITS; ++b) r |= ((i >> b) & 1) << (BITS - 1 - b);
+    return r;
+}
+
+// Power-of-two radix: iterative radix-2 DIT on bit-reversed registers.
+template <typename T, int R>
+__device__ __forceinline__ void dft_pow2_store(C2<T> (&v)[R], C2<T> *D, int a0,
+                                               int ks, int sign) {
+    constexpr int LOG = Log2<R>::v;
+    constexpr int off = tab_offset(R);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int r = bitrev<LOG>(i);
+        if (r > i) {
+            C2<T> t = v[i];
+            v[i] = v[r];
+            v[r] = t;
+        }
+    }
+#pragma unroll
+    for (int len = 2; len <= R; len <<= 1) {
+        const int half = len >> 1;
+#pragma unroll
+        for (int i = 0; i < R; i += len) {
+#pragma unroll
+            for (int k = 0; k < half; ++k) {
+                const int tt = k * (R / len);
+                C2<T> u = v[i + k], x = v[i + k + half], t;
+                if (tt == 0) {
+                    t = x;
+                } else if (4 * tt == R) {
+                    t = (sign < 0) ? mk2<T>(x.y, -x.x) : mk2<T>(-x.y, x.x);
+                } else {
+                    const T c = Tab<T>::c(off + tt);
+                    const T s = (sign < 0) ? -Tab<T>::s(off + tt) : Tab<T>::s(off + tt);
+                    t = mk2<T>(x.x * c - x.y * s, x.x * s + x.y * c);
+                }
+                v[i + k] = u + t;
+                v[i + k + half] = u - t;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) D[a0 + k * ks] = v[k];
+}
+
+// Odd prime radix: X[k] = x0 + sum_j a_j cos(2pi jk/R) -+ i sum_j b_j sin(..),
+// a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}; outputs k and R-k share the sums.
+template <typename T, int R>
+__device__ __forceinline__ void dft_odd_store(C2<T> (&v)[R], C2<T> *D, int a0,
+                                              int ks, int sign) {
+    constexpr int M = (R - 1) / 2;
+    constexpr int off = tab_offset(R);
+#pragma unroll
+    for (int j = 1; j <= M; ++j) {
+        const C2<T> a = v[j] + v[R - j];
+        const C2<T> b = v[j] - v[R - j];
+        v[j] = a;
+        v[R - j] = b;
+    }
+    C2<T> s = v[0];
+#pragma unroll
+    for (int j = 1; j <= M; ++j) s = s + v[j];
+    D[a0] = s;
+    const T sg = (sign < 0) ? T(1) : T(-1);
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+        T pr = v[0].x, pi = v[0].y, qr = T(0), qi = T(0);
+#pragma unroll
+        for (int j = 1; j <= M; ++j) {
+            const int t = (j * k) % R;
+            const T c = Tab<T>::c(off + t);
+            const T sn = Tab<T>::s(off + t);
+            pr = fma(v[j].x, c, pr);
+            pi = fma(v[j].y, c, pi);
+            qr = fma(v[R - j].x, sn, qr);
+            qi = fma(v[R - j].y, sn, qi);
+        }
+        qr *= sg;
+        qi *= sg;
+        D[a0 + k * ks] = mk2<T>(pr + qi, pi - qr);
+        D[a0 + (R - k) * ks] = mk2<T>(pr - qi, pi + qr);
+    }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void dft_store(C2<T> (&v)[R], C2<T> *D, int a0, int ks,
+                                          int sign) {
+    if constexpr ((R & (R - 1)) == 0)
+        dft_pow2_store<T, R>(v, D, a0, ks, sign);
+    else
+        dft_odd_store<T, R>(v, D, a0, ks, sign);
+}
+
+// One Stockham pass with a compile-time radix.  Element e of line b sits at
+// e*es + b*bs (shared-memory element offsets).  `bfast` maps consecutive
+// threads to consecutive lines (element-major layout) instead of consecutive
+// butterflies (line-major layout).
+template <typename T, int R>
+__device__ __noinline__ void stockham_pass(int src, int dst, int roots, int n,
+                                              int Ns, int nb, int es, int bs,
+                                              bool bfast, int sign) {
+    const C2<T> *S = sptr<T>(src);
+    C2<T> *D = sptr<T>(dst);
+    const C2<T> *W = sptr<T>(roots);
+    const int nR = n / R;
+    const int total = nb * nR;
+    const int qs = n / (Ns * R);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int b, j;
+        if (bfast) {
+            b = t % nb;
+            j = t / nb;
+        } else {
+            j = t % nR;
+            b = t / nR;
+        }
+        const int m = j % Ns;
+        const int base = b * bs;
+        C2<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = S[(j + r * nR) * es + base];
+        if (m > 0) {
+            const int step = m * qs;
+            int q = 0;
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                q += step;
+                if (q >= n) q -= n;
+                C2<T> w = W[q];
+                if (sign > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        const int idxD = (j - m) * R + m;
+        dft_store<T, R>(v, D, idxD * es + base, Ns * es, sign);
+    }
+}
+
+// Any radix: direct sum, one output element per thread.
+template <typename T>
+__device__ __noinline__ void generic_pass(int src, int dst, int roots, int n, int R,
+                                          int Ns, int nb, int es, int bs, bool bfast,
+                                          int sign) {
+    const C2<T> *S = sptr<T>(src);
+    C2<T> *D = sptr<T>(dst);
+    const C2<T> *W = sptr<T>(roots);
+    const int nR = n / R;
+    const int total = nb * n;
+    const int qs = n / (Ns * R);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int b, o;
+        if (bfast) {
+            b = t % nb;
+            o = t / nb;
+        } else {
+            o = t % n;
+            b = t / n;
+        }
+        const int m = o % Ns;
+        const int k = (o / Ns) % R;
+        const int g = o / (Ns * R);
+        const int j = g * Ns + m;
+        const int qstep = (m + k * Ns) * qs;
+        const int base = b * bs;
+        C2<T> acc = mk2<T>(T(0), T(0));
+        int q = 0;
+        for (int r = 0; r < R; ++r) {
+            C2<T> w = W[q];
+            if (sign > 0) w.y = -w.y;
+            acc = acc + cmul(S[(j + r * nR) * es + base], w);
+            q += qstep;
+            if (q >= n) q -= n;
+        }
+        D[o * es + base] = acc;
+    }
+}
+
+// Runs all passes of `plan` on nb lines starting in buffer `a` (partner `b`);
+// returns the offset of the buffer that holds the result.  sign = -1 forward
+// (exp(-2 pi i jk/n)), +1 inverse (unnormalised).
+template <typename T>
+__device__ __noinline__ int fft_run(int a, int b, int roots, FFTPlan plan, int nb,
+                                    int es, int bs, bool bfast, int sign) {
+    int src = a, dst = b;
+    const int n = plan.n;
+    for (int p = 0; p < plan.npass; ++p) {
+        const int R = plan.radix[p];
+        const int Ns = plan.ns[p];
+        switch (R) {
+#define HQT_PASS(RR)                                                              \
+    case RR:                                                                      \
+        stockham_pass<T, RR>(src, dst, roots, n, Ns, nb, es, bs, bfast, sign);     \
+        break;
+            HQT_PASS(2)
+            HQT_PASS(3)
+            HQT_PASS(4)
+            HQT_PASS(5)
+            HQT_PASS(7)
+            HQT_PASS(8)
+            HQT_PASS(11)
+            HQT_PASS(13)
+            HQT_PASS(16)
+            HQT_PASS(17)
+            HQT_PASS(19)
+            HQT_PASS(23)
+            HQT_PASS(29)
+            HQT_PASS(31)
+            HQT_PASS(37)
+            HQT_PASS(41)
+            HQT_PASS(43)
+            HQT_PASS(47)
+#undef HQT_PASS
+        default:
+            generic_pass<T>(src, dst, roots, n, R, Ns, nb, es, bs, bfast, sign);
+        }
+        __syncthreads();
+        const int t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+}  // namespace hqt

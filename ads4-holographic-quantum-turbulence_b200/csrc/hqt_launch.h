@@ -1,0 +1,58 @@
+// hqt_launch.h -- host entry points of the kernel translation units.
+#pragma once
+#include "hqt_args.h"
+
+namespace hqt {
+
+// Radial operators on the host (row-major): Lz (nz x nz), Lz1 ((nz-1)^2), zz.
+struct ZHost {
+    int nz;
+    const double *Lz;
+    const double *Lz1;
+    const double *zz;
+};
+
+// Upload the radix tables and opt the FFT kernels into large shared memory.
+cudaError_t fft_init(const double *tab_cos, const double *tab_sin, int ntab, int max_smem);
+
+cudaError_t launch_x_rhs(const XRhsArgs<double> &a, int grid, size_t smem, cudaStream_t s);
+cudaError_t launch_y_rhs(const YRhsArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s);
+cudaError_t launch_x_d1(const XD1Args<double> &a, int grid, size_t smem, cudaStream_t s);
+cudaError_t launch_y_d1(const YD1Args<double> &a, dim3 grid, size_t smem, cudaStream_t s);
+cudaError_t launch_x_filt_fwd(const XFiltFwdArgs<double> &a, int grid, size_t smem,
+                              cudaStream_t s);
+cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s);
+cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
+                              cudaStream_t s);
+
+// Column kernels, one translation unit per compile-time column length N.
+// mode 0: right-hand side only, 1..4: RK stage.
+template <int N> cudaError_t z_init(int max_smem);
+template <int N>
+cudaError_t z_stage(int mode, const ZStageArgs<double, double> &a, const ZHost &h, int grid,
+                    int threads, size_t smem, cudaStream_t s);
+template <int N>
+cudaError_t z_cons(const ZConsArgs<double> &a, const ZHost &h, int grid, int threads,
+                   cudaStream_t s);
+template <int N>
+cudaError_t z_misc(const ZColArgs<double> &a, const ZHost &h, int grid, int threads,
+                   cudaStream_t s);
+
+}  // namespace hqt
+
+// Compile-time column lengths of this build; a run uses the smallest >= nz.
+#define HQT_NZP_LIST(X) X(8) X(12) X(16) X(17) X(21) X(25) X(33)
+
+namespace hqt {
+#define HQT_ZDECL(N)                                                                       \
+    template <> cudaError_t z_init<N>(int);                                                \
+    template <>                                                                            \
+    cudaError_t z_stage<N>(int, const ZStageArgs<double, double> &, const ZHost &, int, int, \
+                           size_t, cudaStream_t);                                          \
+    template <>                                                                            \
+    cudaError_t z_cons<N>(const ZConsArgs<double> &, const ZHost &, int, int, cudaStream_t); \
+    template <>                                                                            \
+    cudaError_t z_misc<N>(const ZColArgs<double> &, const ZHost &, int, int, cudaStream_t);
+HQT_NZP_LIST(HQT_ZDECL)
+#undef HQT_ZDECL
+}  // namespace hqt

@@ -1,0 +1,74 @@
+// hqt_z_impl.cuh -- launchers of the column kernels for one column length
+// HQT_ZN (each hqt_z<N>.cu defines HQT_ZN and includes this file).
+#include <cstring>
+
+#include "hqt_launch.h"
+#include "hqt_zcol.cuh"
+
+#ifndef HQT_ZN
+#error "define HQT_ZN"
+#endif
+
+namespace hqt {
+
+static ZOps<double, HQT_ZN> make_zops(const ZHost &h) {
+    ZOps<double, HQT_ZN> op;
+    std::memset(&op, 0, sizeof(op));
+    const int nz = h.nz;
+    for (int i = 0; i < nz; ++i) {
+        for (int j = 0; j < nz; ++j) op.Lz[i][j] = h.Lz[(size_t)i * nz + j];
+        op.zz[i] = h.zz[i];
+        op.fz[i] = 1.0 - h.zz[i] * h.zz[i] * h.zz[i];
+        op.lzb[i] = h.Lz[(size_t)(nz - 1) * nz + i];
+    }
+    for (int i = 0; i < nz - 1; ++i)
+        for (int j = 0; j < nz - 1; ++j) op.Lz1[i][j] = h.Lz1[(size_t)i * (nz - 1) + j];
+    return op;
+}
+
+template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
+    cudaError_t e = cudaSuccess;
+    auto opt = [&](const void *fn) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    };
+    opt((const void *)k_zstage<double, double, HQT_ZN, 0>);
+    opt((const void *)k_zstage<double, double, HQT_ZN, 1>);
+    opt((const void *)k_zstage<double, double, HQT_ZN, 2>);
+    opt((const void *)k_zstage<double, double, HQT_ZN, 3>);
+    opt((const void *)k_zstage<double, double, HQT_ZN, 4>);
+    return e;
+}
+
+template <>
+cudaError_t z_stage<HQT_ZN>(int mode, const ZStageArgs<double, double> &a, const ZHost &h,
+                            int grid, int threads, size_t smem, cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    switch (mode) {
+        case 0: k_zstage<double, double, HQT_ZN, 0><<<grid, threads, smem, s>>>(a, op); break;
+        case 1: k_zstage<double, double, HQT_ZN, 1><<<grid, threads, smem, s>>>(a, op); break;
+        case 2: k_zstage<double, double, HQT_ZN, 2><<<grid, threads, smem, s>>>(a, op); break;
+        case 3: k_zstage<double, double, HQT_ZN, 3><<<grid, threads, smem, s>>>(a, op); break;
+        case 4: k_zstage<double, double, HQT_ZN, 4><<<grid, threads, smem, s>>>(a, op); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <>
+cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, int grid, int threads,
+                           cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    k_zcons<double, HQT_ZN><<<grid, threads, 0, s>>>(a, op);
+    return cudaGetLastError();
+}
+
+template <>
+cudaError_t z_misc<HQT_ZN>(const ZColArgs<double> &a, const ZHost &h, int grid, int threads,
+                           cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    k_zcol_misc<double, HQT_ZN><<<grid, threads, 0, s>>>(a, op);
+    return cudaGetLastError();
+}
+
+}  // namespace hqt

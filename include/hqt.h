@@ -1,0 +1,157 @@
+/*
+ * hqt.h -- C ABI of the B200 (sm_100a) RK4 step of the AdS4 holographic
+ * superfluid (complex bulk scalar Psi = Z1, gauge fields A_t = Z2,
+ * A_x = Z3, A_y = Z4, boundary charge data rhoi).
+ *
+ * The reference has no callable step: its step is the inline loop body of
+ * scripts/simulation/tevol_driven_cluster.m:117-187 (lattice variant
+ * scripts/simulation/tevol_lattice.m:151-218) acting on workspace arrays.
+ * This header is the function boundary that loop would call, one entry point
+ * per operation of that loop body.  Plain C types only.
+ *
+ * Array layout (host and device): MATLAB column-major [nx, ny, nz], x fastest,
+ * z index 0 = horizon (z=1), index nz-1 = AdS boundary (z=0), exactly the
+ * layout of the workspace arrays and of check_point_t=<t>.mat
+ * (docs/DATA_DICTIONARY.md:27-39).  Z1 is interleaved complex double
+ * (re, im), as MATLAB's interleaved complex API and numpy complex128 store it.
+ * rhoi is stored [nx, ny, nz] replicated along z, as the reference keeps it
+ * (tevol_driven_cluster.m:98,128).
+ *
+ * Threading: a context is bound to one device and one stream and is not
+ * thread-safe; callers serialise calls per context.
+ */
+#ifndef HQT_H
+#define HQT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HQT_ABI_VERSION 1
+
+/* status codes */
+#define HQT_OK            0
+#define HQT_EINVAL        1  /* bad parameter, shape or pointer            */
+#define HQT_ENONFINITE    2  /* NaN/Inf in the fields: the reference stops
+                                at the NaN guard tevol_driven_cluster.m:182-185
+                                (smoke-test id hqt:NonfiniteEvolution)     */
+#define HQT_ECUDA         3  /* CUDA runtime error                         */
+#define HQT_ENOMEM        4  /* device allocation failed                   */
+#define HQT_EUNSUPPORTED  5  /* size or mode this build does not handle    */
+
+/* precision modes */
+#define HQT_FP64   0         /* plain FP64 drop-in                          */
+#define HQT_MIXED  1         /* FP32 stage arithmetic, FP64 state/constraint */
+
+typedef struct hqt_ctx hqt_ctx;
+
+/* Run parameters.  Replaces the hard-coded script constants
+ * tevol_driven_cluster.m:11 (nx, ny, nz), :23-24 (L0, L), :79 (mu),
+ * :86 (vy = -2*pi*kk/20), :110 (h). */
+typedef struct {
+    int32_t nx, ny;        /* periodic grid (any size >= 4)                 */
+    int32_t nz;            /* Chebyshev points, chebdif(nz,1) (3..40)       */
+    double  Lx, Ly;        /* box lengths L0, L                            */
+    double  mu;            /* A_t(z=0) = mu                                 */
+    double  vy;            /* A_y(z=0) = -vy  (tevol_driven_cluster.m:133)  */
+    double  dt;            /* RK4 step h                                    */
+    int32_t remove_winding;/* 1: global y-winding removal (:136-139);
+                              0: lattice script (tevol_lattice.m:168-170)   */
+    int32_t precision;     /* HQT_FP64 or HQT_MIXED                         */
+    int32_t diag_every;    /* >0: vortex count every diag_every steps       */
+    int32_t apply_filter;  /* 1: the 2/3 Fourier filter each step (:142)    */
+} hqt_params;
+
+/* Per-call diagnostics. */
+typedef struct {
+    int64_t  steps_done;       /* out: steps completed by this call          */
+    int64_t  nonfinite_step;   /* out: 1-based step of the first non-finite
+                                  value in this call, or -1                  */
+    int32_t  last_winding;     /* out: winding removed at the last step      */
+    int32_t  n_records;        /* out: vortex-count records written          */
+    int32_t  capacity;         /* in: capacity of `records` (records)        */
+    int32_t  reserved;
+    int32_t *records;          /* in: caller buffer, 4*capacity int32 laid out
+                                  as (step, n, np, nm) per record; may be NULL */
+} hqt_diag;
+
+/* Version of this ABI (HQT_ABI_VERSION). */
+int hqt_abi_version(void);
+
+/* Create a context on `device`: builds Lz = 2*chebdif(nz,1),
+ * Lz1 = inv(Lz(1:nz-1,1:nz-1)), the Fourier plans and the filter weights
+ * (tevol_driven_cluster.m:13-54) and allocates the device work buffers. */
+int hqt_create(const hqt_params *params, int device, hqt_ctx **out);
+
+void hqt_destroy(hqt_ctx *ctx);
+
+/* Last error message of `ctx` (or of the last failed hqt_create on this
+ * thread when ctx is NULL).  Never NULL. */
+const char *hqt_last_error(const hqt_ctx *ctx);
+
+/* Launch on the caller's CUDA stream (a cudaStream_t, or NULL for the
+ * context's own stream). */
+int hqt_set_stream(hqt_ctx *ctx, void *cuda_stream);
+
+/* Advance `nsteps` RK4 steps of the loop body tevol_driven_cluster.m:120-142
+ * on HOST arrays, updated in place.  Copies in once, loops on the device,
+ * copies out once.  Returns HQT_ENONFINITE (fields as of the last completed
+ * step) when a step produced NaN/Inf. */
+int hqt_step(hqt_ctx *ctx, double *Z1, double *Z2, double *Z3, double *Z4,
+             double *rhoi, int64_t nsteps, hqt_diag *diag);
+
+/* Same on DEVICE arrays of the same layout: the kernels update the caller's
+ * Z1..Z4 in place (no copies; gpuArray or torch storage); rhoi is read from
+ * its boundary slice and written back replicated.  Synchronises the stream
+ * before returning. */
+int hqt_step_device(hqt_ctx *ctx, void *dZ1, void *dZ2, void *dZ3, void *dZ4,
+                    void *drhoi, int64_t nsteps, hqt_diag *diag);
+
+/* One right-hand-side evaluation, the anonymous functions F1, F3, F4 (full
+ * [nx,ny,nz]) and F2 (boundary slice only, [nx,ny]) of
+ * tevol_driven_cluster.m:72-76, without the factor h.  dF1 is interleaved
+ * complex. */
+int hqt_rhs_device(hqt_ctx *ctx, const void *dZ1, const void *dZ2,
+                   const void *dZ3, const void *dZ4, void *dF1, void *dF3,
+                   void *dF4, void *dF2b);
+
+/* The Fourier filter ff(x, fxyz) (src/numerics/ff.m:7-11 with the mask of
+ * tevol_driven_cluster.m:27-31) applied to `nfields` consecutive real
+ * [nx,ny,nz] device arrays (in may equal out). */
+int hqt_filter_device(hqt_ctx *ctx, const void *din, void *dout,
+                      int32_t nfields);
+
+/* Boundary order parameter O = func_Lz(Z1)(:,:,nz) (tevol_driven_cluster.m:136),
+ * interleaved complex [nx,ny] on the device. */
+int hqt_boundary_order_parameter_device(hqt_ctx *ctx, const void *dZ1,
+                                        void *dO);
+
+/* Global winding round(mean(sum(angle(circshift(O,-1,2)./O),1))/(2*pi))
+ * of a device field O (tevol_driven_cluster.m:137). */
+int hqt_winding_device(hqt_ctx *ctx, const void *dO, int32_t *winding);
+
+/* countN (src/diagnostics/countN.m:7-21) of an interleaved complex [nx,ny]
+ * field: total, +1 and -1 plaquette counts.  Host and device versions. */
+int hqt_count_vortices(hqt_ctx *ctx, const double *O, int32_t *n,
+                       int32_t *np, int32_t *nm);
+int hqt_count_vortices_device(hqt_ctx *ctx, const void *dO, int32_t *n,
+                              int32_t *np, int32_t *nm);
+
+/* Instrumentation (no counterpart in the reference, which times its loop
+ * with tic/toc every 50 steps, tevol_driven_cluster.m:116,144-146).
+ * hqt_profile(ctx, 1) resets the counters and makes every following launch
+ * run outside the step graph, bracketed by CUDA events on the context
+ * stream; hqt_profile(ctx, 0) returns to graph replay.
+ * hqt_profile_report writes a JSON object
+ *   {"launches": N, "kernels": [{"kernel": name, "launches": n, "ms": t}, ...]}
+ * with the kernel launches issued since the last reset and the summed event
+ * times per kernel kind. */
+int hqt_profile(hqt_ctx *ctx, int enable);
+int hqt_profile_report(hqt_ctx *ctx, char *buf, int64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HQT_H */
