@@ -66,6 +66,7 @@ struct hqt_ctx {
     DevStatus *st = nullptr;
     // launch geometry
     int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
+    int smem_optin = 0;
     // state arrays the step acts on (internal buffers, or the caller's
     // device arrays for hqt_step_device)
     double2 *cpsi = nullptr;
@@ -117,8 +118,10 @@ int fail(hqt_ctx *c, int code, const std::string &msg) {
 #define CK(call)                                                                      \
     do {                                                                              \
         cudaError_t e_ = (call);                                                      \
-        if (e_ != cudaSuccess)                                                        \
+        if (e_ != cudaSuccess) {                                                      \
+            cudaGetLastError();                                                       \
             return fail(c, HQT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+        }                                                                             \
     } while (0)
 
 // kernel kinds reported by hqt_profile_report
@@ -760,7 +763,14 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         }
     }
     {
-        const int maxs = 227 * 1024;
+        int maxs = 0;
+        if (cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            c->err = "cannot query the shared-memory limit";
+            return bail(HQT_ECUDA);
+        }
+        c->smem_optin = maxs;
         std::vector<double> tc, ts;
         make_radix_tables(tc, ts);
         cudaError_t e = fft_init(tc.data(), ts.data(), (int)tc.size(), maxs);
@@ -769,6 +779,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         HQT_NZP_LIST(HQT_Z)
 #undef HQT_Z
         if (e != cudaSuccess) {
+            cudaGetLastError();
             c->err = std::string("kernel set-up: ") + cudaGetErrorString(e);
             return bail(HQT_ECUDA);
         }

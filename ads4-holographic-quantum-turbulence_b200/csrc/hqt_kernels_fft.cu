@@ -14,8 +14,12 @@ cudaError_t fft_init(const double *tc, const double *ts, int ntab, int max_smem)
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tab_cos_f, fc.data(), sizeof(float) * ntab);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tab_sin_f, fs.data(), sizeof(float) * ntab);
     auto opt = [&](const void *fn) {
+        // the opt-in limit covers static and dynamic shared memory together
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     max_smem - (int)fa.sharedSizeBytes);
     };
     opt((const void *)k_x_rhs<double>);
     opt((const void *)k_y_rhs<double>);

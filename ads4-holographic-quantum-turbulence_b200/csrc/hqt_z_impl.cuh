@@ -29,8 +29,12 @@ static ZOps<double, HQT_ZN> make_zops(const ZHost &h) {
 template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     cudaError_t e = cudaSuccess;
     auto opt = [&](const void *fn) {
+        // the opt-in limit covers static and dynamic shared memory together
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     max_smem - (int)fa.sharedSizeBytes);
     };
     opt((const void *)k_zstage<double, double, HQT_ZN, 0>);
     opt((const void *)k_zstage<double, double, HQT_ZN, 1>);

@@ -199,7 +199,8 @@ def run_ours(args, w, ws, rank, local):
     # warm-up (also captures the step graph)
     sim.step_device(*T, nsteps=max(args.warmup, 3))
     torch.cuda.synchronize()
-    pci = torch.cuda.get_device_properties(dev).pci_bus_id
+    pr = torch.cuda.get_device_properties(dev)
+    pci = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -258,19 +259,21 @@ def run_ours(args, w, ws, rank, local):
     H = [t.numpy().T for t in pinned]
     per_call = 50
     calls = max(1, int(round(args.steps / per_call)))
-    sim.step(*H, nsteps=per_call, inplace=True)  # warm the host path
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(calls):
-        sim.step(*H, nsteps=per_call, inplace=True)
-    torch.cuda.synchronize()
-    e2e_s = allreduce_max(time.perf_counter() - t0, ws)
-    e2e = {"value": ws * sites * per_call * calls / e2e_s, "unit": "site-updates/s",
-           "h2d_bytes_per_step": (16 + 24) * sites + 8 * nx * ny,
-           "d2h_bytes_per_step": (16 + 24 + 8) * sites,
-           "step": f"one hqt_step call of {per_call} RK4 steps on pinned host arrays"}
+    e2e = None
+    if not args.no_e2e:
+        sim.step(*H, nsteps=per_call, inplace=True)  # warm the host path
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            sim.step(*H, nsteps=per_call, inplace=True)
+        torch.cuda.synchronize()
+        e2e_s = allreduce_max(time.perf_counter() - t0, ws)
+        e2e = {"value": ws * sites * per_call * calls / e2e_s, "unit": "site-updates/s",
+               "h2d_bytes_per_step": (16 + 24) * sites + 8 * nx * ny,
+               "d2h_bytes_per_step": (16 + 24 + 8) * sites,
+               "step": f"one hqt_step call of {per_call} RK4 steps on pinned host arrays"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -307,6 +310,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="driven301", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))
     w = WORKLOADS[args.workload]
