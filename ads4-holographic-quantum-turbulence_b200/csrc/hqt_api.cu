@@ -13,6 +13,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -27,7 +28,7 @@ namespace hqt {
 
 static constexpr int kThreadsFFT = 128;
 static constexpr int kThreadsZ = 64;
-static constexpr size_t kSmemBudget = 72 * 1024;
+static constexpr size_t kSmemBudget = 54 * 1024;
 static constexpr int kPartials = 296;
 
 #define HQT_NZP_VAL(N) N,
@@ -66,6 +67,7 @@ struct hqt_ctx {
     DevStatus *st = nullptr;
     // launch geometry
     int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
+    bool cx = false, cy = false;  // compile-time line transforms along x / y
     int smem_optin = 0;
     // state arrays the step acts on (internal buffers, or the caller's
     // device arrays for hqt_step_device)
@@ -155,6 +157,32 @@ struct Prof {
     }
 };
 
+#define RC(call)                         \
+    do {                                 \
+        int r_ = (call);                 \
+        if (r_ != HQT_OK) return r_;     \
+    } while (0)
+
+bool ct_supported(int n) {
+#define HQT_CS(N) \
+    if (n == N) return true;
+    HQT_CN_LIST(HQT_CS)
+#undef HQT_CS
+    return false;
+}
+
+int ct_dispatch(hqt_ctx *c, int n, int kind, const void *args, dim3 grid, size_t smem) {
+    switch (n) {
+#define HQT_CD(N)                                                    \
+    case N:                                                          \
+        CK(ct_launch<N>(kind, args, grid, smem, c->stream));         \
+        return HQT_OK;
+        HQT_CN_LIST(HQT_CD)
+#undef HQT_CD
+    }
+    return fail(c, HQT_EUNSUPPORTED, "no compile-time transform for this length");
+}
+
 template <typename P> int dalloc(hqt_ctx *c, P **ptr, size_t bytes) {
     void *q = nullptr;
     cudaError_t e = cudaMalloc(&q, bytes);
@@ -197,6 +225,11 @@ int launch_x_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     a.dxxay = c->dxxay;
     const int grid = (a.nlines + a.NB - 1) / a.NB;
     Prof pr(c, K_X_RHS);
+    if (c->cx) {
+        const int nb = ct_lines(c->nx, 3);
+        RC(ct_dispatch(c, c->nx, CT_X_RHS, &a, dim3((a.nlines + nb - 1) / nb), smem_x(c->nx, 3, nb)));
+        return HQT_OK;
+    }
     CK(launch_x_rhs(a, grid, smem_x(c->nx, 3, a.NB), c->stream));
     return HQT_OK;
 }
@@ -224,6 +257,12 @@ int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     a.dyB = c->dyB;
     dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
     Prof pr(c, K_Y_RHS);
+    if (c->cy) {
+        const int nb = ct_lines(c->ny, 3);
+        RC(ct_dispatch(c, c->ny, CT_Y_RHS, &a, dim3((c->nx + nb - 1) / nb, c->nz),
+                       smem_x(c->ny, 3, nb)));
+        return HQT_OK;
+    }
     CK(launch_y_rhs(a, grid, smem_x(c->ny, 4, a.TX), c->stream));
     return HQT_OK;
 }
@@ -239,6 +278,11 @@ int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out) {
     a.out = out;
     const int grid = (a.nlines + a.NB - 1) / a.NB;
     Prof pr(c, K_X_D1);
+    if (c->cx) {
+        const int nb = ct_lines(c->nx, 2);
+        RC(ct_dispatch(c, c->nx, CT_X_D1, &a, dim3((a.nlines + nb - 1) / nb), smem_x(c->nx, 2, nb)));
+        return HQT_OK;
+    }
     CK(launch_x_d1(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
     return HQT_OK;
 }
@@ -256,6 +300,12 @@ int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<d
     a.out = out;
     dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
     Prof pr(c, K_Y_D1);
+    if (c->cy) {
+        const int nb = ct_lines(c->ny, 2);
+        RC(ct_dispatch(c, c->ny, CT_Y_D1, &a, dim3((c->nx + nb - 1) / nb, c->nz),
+                       smem_x(c->ny, 2, nb)));
+        return HQT_OK;
+    }
     CK(launch_y_d1(a, grid, smem_x(c->ny, 2, a.TX), c->stream));
     return HQT_OK;
 }
@@ -279,7 +329,13 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.st = phase ? c->st : nullptr;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_FWD);
-        CK(launch_x_filt_fwd(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+        if (c->cx) {
+            const int nb = ct_lines(c->nx, 2);
+            RC(ct_dispatch(c, c->nx, CT_FX_FWD, &a, dim3((a.nlines + nb - 1) / nb),
+                           smem_x(c->nx, 2, nb)));
+        } else {
+            CK(launch_x_filt_fwd(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+        }
     }
     {
         YFiltArgs<double> a{};
@@ -295,7 +351,13 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.scale = 1.0 / ((double)c->nx * (double)c->ny);
         dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
         Prof pr(c, K_FILT_Y);
-        CK(launch_y_filt(a, grid, smem_x(c->ny, 2, a.TX * 3), c->stream));
+        if (c->cy) {
+            const int tx = ct_lines(c->ny, 6);
+            RC(ct_dispatch(c, c->ny, CT_FY, &a, dim3((c->nx + tx - 1) / tx, c->nz),
+                           smem_x(c->ny, 2, 3 * tx)));
+        } else {
+            CK(launch_y_filt(a, grid, smem_x(c->ny, 2, a.TX * 3), c->stream));
+        }
     }
     {
         XFiltInvArgs<double> a{};
@@ -311,7 +373,13 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.st = check ? c->st : nullptr;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_INV);
-        CK(launch_x_filt_inv(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+        if (c->cx) {
+            const int nb = ct_lines(c->nx, 2);
+            RC(ct_dispatch(c, c->nx, CT_FX_INV, &a, dim3((a.nlines + nb - 1) / nb),
+                           smem_x(c->nx, 2, nb)));
+        } else {
+            CK(launch_x_filt_inv(a, grid, smem_x(c->nx, 2, a.NB), c->stream));
+        }
     }
     return HQT_OK;
 }
@@ -388,11 +456,6 @@ int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
     return HQT_OK;
 }
 
-#define RC(call)                         \
-    do {                                 \
-        int r_ = (call);                 \
-        if (r_ != HQT_OK) return r_;     \
-    } while (0)
 
 // ---------------------------------------------------------------- one step
 int enqueue_step(hqt_ctx *c) {
@@ -752,6 +815,12 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     c->TXy_rhs = pick_lines(p.ny, 4, 16);
     c->TXy_2 = pick_lines(p.ny, 2, 16);
     c->TXy_filt = pick_lines(p.ny, 6, 16);
+    c->cx = ct_supported(p.nx);
+    c->cy = ct_supported(p.ny);
+    if (const char *env = std::getenv("HQT_LINE_ENGINE")) {
+        // "runtime" forces the runtime-plan engine (the tests cover both)
+        if (std::string(env) == "runtime") c->cx = c->cy = false;
+    }
     {
         const size_t lim = 227 * 1024 - 1024;
         const size_t need = std::max({smem_x(p.nx, 3, c->NBx_rhs), smem_x(p.ny, 4, c->TXy_rhs),
@@ -774,6 +843,13 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         std::vector<double> tc, ts;
         make_radix_tables(tc, ts);
         cudaError_t e = fft_init(tc.data(), ts.data(), (int)tc.size(), maxs);
+        std::vector<double> bc, bs;
+        make_big_tables(bc, bs);
+#define HQT_CI(N)                                                                            \
+    if (e == cudaSuccess)                                                                    \
+        e = ct_init<N>(tc.data(), ts.data(), (int)tc.size(), bc.data(), bs.data(), (int)bc.size(), maxs);
+        HQT_CN_LIST(HQT_CI)
+#undef HQT_CI
 #define HQT_Z(N) \
     if (e == cudaSuccess) e = z_init<N>(maxs);
         HQT_NZP_LIST(HQT_Z)

@@ -1,0 +1,78 @@
+// hqt_c_impl.cuh -- launchers of the compile-time line transforms for one
+// line length HQT_CN (each hqt_c<N>.cu defines HQT_CN and includes this).
+#include <vector>
+
+#include "hqt_cpasses.cuh"
+#include "hqt_launch.h"
+
+#ifndef HQT_CN
+#error "define HQT_CN"
+#endif
+
+namespace hqt {
+
+template <>
+cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const double *bc,
+                            const double *bs, int nbig, int max_smem) {
+    if (ntab != kTabTotal || nbig != kBigTotal) return cudaErrorInvalidValue;
+    std::vector<float> fc(tc, tc + ntab), fs(ts, ts + ntab), gc(bc, bc + nbig), gs(bs, bs + nbig);
+    cudaError_t e = cudaMemcpyToSymbol(c_tab_cos_d, tc, sizeof(double) * ntab);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tab_sin_d, ts, sizeof(double) * ntab);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tab_cos_f, fc.data(), sizeof(float) * ntab);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tab_sin_f, fs.data(), sizeof(float) * ntab);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_big_cos_d, bc, sizeof(double) * nbig);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_big_sin_d, bs, sizeof(double) * nbig);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_big_cos_f, gc.data(), sizeof(float) * nbig);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_big_sin_f, gs.data(), sizeof(float) * nbig);
+    auto opt = [&](const void *fn) {
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     max_smem - (int)fa.sharedSizeBytes);
+    };
+    opt((const void *)k_x_rhs_c<double, HQT_CN>);
+    opt((const void *)k_y_rhs_c<double, HQT_CN>);
+    opt((const void *)k_x_d1_c<double, HQT_CN>);
+    opt((const void *)k_y_d1_c<double, HQT_CN>);
+    opt((const void *)k_x_filt_fwd_c<double, HQT_CN>);
+    opt((const void *)k_y_filt_c<double, HQT_CN>);
+    opt((const void *)k_x_filt_inv_c<double, HQT_CN>);
+    return e;
+}
+
+template <>
+cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem,
+                              cudaStream_t s) {
+    constexpr int T = kCtThreads;
+    switch (kind) {
+        case CT_X_RHS:
+            k_x_rhs_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const XRhsArgs<double> *)args);
+            break;
+        case CT_Y_RHS:
+            k_y_rhs_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<double> *)args);
+            break;
+        case CT_X_D1:
+            k_x_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const XD1Args<double> *)args);
+            break;
+        case CT_Y_D1:
+            k_y_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YD1Args<double> *)args);
+            break;
+        case CT_FX_FWD:
+            k_x_filt_fwd_c<double, HQT_CN>
+                <<<grid, T, smem, s>>>(*(const XFiltFwdArgs<double> *)args);
+            break;
+        case CT_FY:
+            k_y_filt_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YFiltArgs<double> *)args);
+            break;
+        case CT_FX_INV:
+            k_x_filt_inv_c<double, HQT_CN>
+                <<<grid, T, smem, s>>>(*(const XFiltInvArgs<double> *)args);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace hqt

@@ -54,8 +54,7 @@ struct FFTPlan {
 };
 
 // ---- constant tables of cos(2*pi*t/R), sin(2*pi*t/R) per radix ------------
-constexpr int kTabRadices[] = {2, 3, 4, 5, 7, 8, 11, 13, 16, 17, 19, 23,
-                               29, 31, 37, 41, 43, 47};
+constexpr int kTabRadices[] = {2, 3, 4, 5, 7, 8, 11, 13, 16};
 constexpr int kNumTabRadices = sizeof(kTabRadices) / sizeof(int);
 
 __host__ __device__ constexpr int tab_offset(int R) {
@@ -66,7 +65,15 @@ __host__ __device__ constexpr int tab_offset(int R) {
     }
     return -1;
 }
-constexpr int kTabTotal = tab_offset(47) + 47;
+constexpr int kTabTotal = tab_offset(16) + 16;
+
+// Lines per block of the compile-time line transforms: a block holds
+// (1 + nbuf*NB) lines of N complex doubles in about 54 KB of shared memory,
+// so that four 128-thread blocks fit on an SM.
+__host__ __device__ constexpr int ct_lines(int N, int nbuf) {
+    const int v = ((54 * 1024) / 16 / N - 1) / nbuf;
+    return v < 1 ? 1 : (v > 16 ? 16 : v);
+}
 
 // Status word shared by the step kernels (device memory).
 struct DevStatus {

@@ -1,0 +1,305 @@
+// hqt_cpasses.cuh -- the spectral passes of hqt_passes.cuh with a
+// compile-time line length N (hqt_cfft.cuh).  One translation unit per N
+// (hqt_c<N>.cu) instantiates them.  A block always transforms its full
+// compile-time batch; lines past the end of the grid are zero-filled and
+// never stored.
+#pragma once
+#include "hqt_cfft.cuh"
+#include "hqt_passes.cuh"
+
+namespace hqt {
+
+#define HQT_CT_BOUNDS __launch_bounds__(kCtThreads, 4)
+
+// x lines: NB consecutive (y, z) rows, contiguous in global memory
+template <typename T, int N, int NB, typename F>
+__device__ __forceinline__ void cx_load(int buf, int valid, F get) {
+    C2<T> *s = sptr<T>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int b = t / N, e = t - b * N;
+        s[e * NB + b] = (b < valid) ? get(t) : mk2<T>(T(0), T(0));
+    }
+}
+template <typename T, int N, int NB, typename F>
+__device__ __forceinline__ void cx_store(int buf, int valid, F put) {
+    const C2<T> *s = sptr<T>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int b = t / N, e = t - b * N;
+        if (b < valid) put(t, s[e * NB + b]);
+    }
+}
+// y lines: NB adjacent columns of one z slice; element (y, b) at y*NB + b
+template <typename T, int N, int NB, typename F>
+__device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zoff, F get) {
+    C2<T> *s = sptr<T>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int y = t / NB, b = t - y * NB;
+        s[t] = (b < valid) ? get(zoff + (long long)y * nx + b) : mk2<T>(T(0), T(0));
+    }
+}
+template <typename T, int N, int NB, typename F>
+__device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long zoff, F put) {
+    const C2<T> *s = sptr<T>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int y = t / NB, b = t - y * NB;
+        if (b < valid) put(zoff + (long long)y * nx + b, s[t]);
+    }
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
+    constexpr int NB = ct_lines(N, 3);
+    const int L0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nlines - L0);
+    constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
+    const long long g0 = (long long)L0 * N;
+    load_roots<T>(R, a.roots, N);
+    cx_load<T, N, NB>(A, valid, [&](int t) { return a.psi[g0 + t]; });
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    const int Y = (X == A) ? B : A;
+    ct_deriv<T, N, NB, 1>(Y, X, a.s1, a.s2);
+    __syncthreads();
+    const int r1 = ct_fft<T, N, NB, +1>(Y, C, R);
+    cx_store<T, N, NB>(r1, valid, [&](int t, C2<T> v) { a.dxpsi[g0 + t] = v; });
+    ct_deriv<T, N, NB, 2>(X, X, a.s1, a.s2);
+    __syncthreads();
+    const int fr = (r1 == Y) ? C : Y;
+    const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
+    cx_store<T, N, NB>(r2, valid, [&](int t, C2<T> v) { a.dxxpsi[g0 + t] = v; });
+    __syncthreads();
+    cx_load<T, N, NB>(A, valid, [&](int t) { return mk2<T>(a.ax[g0 + t], a.ay[g0 + t]); });
+    __syncthreads();
+    const int X2 = ct_fft<T, N, NB, -1>(A, B, R);
+    const int Y2 = (X2 == A) ? B : A;
+    ct_deriv<T, N, NB, 1>(Y2, X2, a.s1, a.s2);
+    __syncthreads();
+    const int r3 = ct_fft<T, N, NB, +1>(Y2, C, R);
+    cx_store<T, N, NB>(r3, valid, [&](int t, C2<T> v) { a.E[g0 + t] = v; });
+    ct_deriv<T, N, NB, 2>(X2, X2, a.s1, a.s2);
+    __syncthreads();
+    const int fr2 = (r3 == Y2) ? C : Y2;
+    const int r4 = ct_fft<T, N, NB, +1>(X2, fr2, R);
+    cx_store<T, N, NB>(r4, valid, [&](int t, C2<T> v) { a.dxxay[g0 + t] = v.y; });
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
+    constexpr int NB = ct_lines(N, 3);
+    const int x0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nx - x0);
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
+    load_roots<T>(R, a.roots, N);
+    // Psi: d_y and d_yy
+    cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return a.psi[g]; });
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    const int Y = (X == A) ? B : A;
+    ct_deriv<T, N, NB, 1>(Y, X, a.s1, a.s2);
+    __syncthreads();
+    const int r1 = ct_fft<T, N, NB, +1>(Y, C, R);
+    cy_store<T, N, NB>(r1, valid, a.nx, zoff, [&](long long g, C2<T> v) { a.dypsi[g] = v; });
+    ct_deriv<T, N, NB, 2>(X, X, a.s1, a.s2);
+    __syncthreads();
+    const int fr = (r1 == Y) ? C : Y;
+    const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
+    cy_store<T, N, NB>(r2, valid, a.nx, zoff,
+                       [&](long long g, C2<T> v) { a.lap[g] = a.dxxpsi[g] + v; });
+    __syncthreads();
+    // C = A_x + i A_y and E = d_x C, each transformed, then paired
+    cy_load<T, N, NB>(A, valid, a.nx, zoff,
+                      [&](long long g) { return mk2<T>(a.ax[g], a.ay[g]); });
+    __syncthreads();
+    const int SC = ct_fft<T, N, NB, -1>(A, B, R);       // C spectrum in A or B
+    const int F1 = (SC == A) ? B : A;                   // free
+    cy_load<T, N, NB>(C, valid, a.nx, zoff, [&](long long g) { return a.E[g]; });
+    __syncthreads();
+    const int SE = ct_fft<T, N, NB, -1>(C, F1, R);      // E spectrum in C or F1
+    {
+        C2<T> *sc = sptr<T>(SC), *se = sptr<T>(SE);
+        const T h = T(0.5);
+        for (int t = threadIdx.x; t < (N / 2 + 1) * NB; t += kCtThreads) {
+            const int b = t % NB, k = t / NB;
+            const int kp = (N - k) % N;
+            const C2<T> Cc = sc[k * NB + b], Cp = sc[kp * NB + b];
+            const C2<T> Ec = se[k * NB + b], Ep = se[kp * NB + b];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1 && kp == k) break;
+                const int kk_ = side == 0 ? k : kp;
+                const C2<T> c1 = side == 0 ? Cc : Cp, c2 = side == 0 ? Cp : Cc;
+                const C2<T> e1 = side == 0 ? Ec : Ep, e2 = side == 0 ? Ep : Ec;
+                const T kk = T(wavenum(kk_, N));
+                const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk;
+                const C2<T> axh = mk2<T>(h * (c1.x + c2.x), h * (c1.y - c2.y));
+                const C2<T> ayh = mk2<T>(h * (c1.y + c2.y), -h * (c1.x - c2.x));
+                const C2<T> exh = mk2<T>(h * (e1.x + e2.x), h * (e1.y - e2.y));
+                const C2<T> eyh = mk2<T>(h * (e1.y + e2.y), -h * (e1.x - e2.x));
+                const C2<T> q1 = mk2<T>(-m1 * ayh.y, m1 * ayh.x);
+                const C2<T> q2 = mk2<T>(m1 * exh.y, -m1 * exh.x);
+                const C2<T> q3 = mk2<T>(-m1 * eyh.y - m2 * axh.x, m1 * eyh.x - m2 * axh.y);
+                sc[kk_ * NB + b] = mk2<T>(q1.x - q2.y, q1.y + q2.x);
+                se[kk_ * NB + b] = q3;
+            }
+        }
+    }
+    __syncthreads();
+    // the third buffer is free: the one that is neither SC nor SE
+    const int F2 = (A != SC && A != SE) ? A : ((B != SC && B != SE) ? B : C);
+    const int P1 = ct_fft<T, N, NB, +1>(SC, F2, R);
+    const int F3 = (P1 == SC) ? F2 : SC;
+    const int P2 = ct_fft<T, N, NB, +1>(SE, F3, R);
+    {
+        const C2<T> *s1 = sptr<T>(P1), *s2 = sptr<T>(P2);
+        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+            const int y = t / NB, b = t - y * NB;
+            if (b < valid) {
+                const long long g = zoff + (long long)y * a.nx + b;
+                a.divA[g] = a.E[g].x + s1[t].x;
+                a.dxB[g] = a.dxxay[g] + s1[t].y;
+                a.dyB[g] = s2[t].x;
+            }
+        }
+    }
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
+    constexpr int NB = ct_lines(N, 2);
+    const int L0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nlines - L0);
+    constexpr int R = 0, A = N, B = N + NB * N;
+    const long long g0 = (long long)L0 * N;
+    load_roots<T>(R, a.roots, N);
+    cx_load<T, N, NB>(A, valid, [&](int t) { return load_field(a.in, g0 + t); });
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
+    __syncthreads();
+    const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    cx_store<T, N, NB>(r, valid, [&](int t, C2<T> v) { store_field(a.out, g0 + t, v); });
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
+    constexpr int NB = ct_lines(N, 2);
+    const int x0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nx - x0);
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    constexpr int R = 0, A = N, B = N + NB * N;
+    load_roots<T>(R, a.roots, N);
+    cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return load_field(a.in, g); });
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
+    __syncthreads();
+    const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    cy_store<T, N, NB>(r, valid, a.nx, zoff, [&](long long g, C2<T> v) {
+        if (a.add_re) v.x += a.add_re[g];
+        store_field(a.out, g, v);
+    });
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
+    constexpr int NB = ct_lines(N, 2);
+    const int L0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nlines - L0);
+    constexpr int R = 0, A = N, B = N + NB * N;
+    const long long g0 = (long long)L0 * N;
+    load_roots<T>(R, a.roots, N);
+    const int w = a.st ? a.st->winding : 0;
+    for (int f = 0; f < a.nf; ++f) {
+        cx_load<T, N, NB>(A, valid, [&](int t) {
+            C2<T> v = load_field(a.in[f], g0 + t);
+            if (f == 0 && w != 0) {
+                // phase -2*pi*y*w/ny of line L0 + t/N (tevol_driven_cluster.m:139)
+                const int y = (L0 + t / N) % a.ny;
+                const long long q = ((long long)y * w) % a.ny;
+                double sn, cs;
+                sincospi(-2.0 * (double)q / (double)a.ny, &sn, &cs);
+                v = mk2<T>(v.x * (T)cs - v.y * (T)sn, v.x * (T)sn + v.y * (T)cs);
+            }
+            return v;
+        });
+        __syncthreads();
+        const int X = ct_fft<T, N, NB, -1>(A, B, R);
+        C2<T> *spec = a.spec[f];
+        cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) { spec[g0 + t] = v; });
+        __syncthreads();
+    }
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
+    constexpr int TX = ct_lines(N, 6);
+    constexpr int NB = 3 * TX;  // up to three fields of TX columns
+    const int x0 = blockIdx.x * TX;
+    const int valid = min(TX, a.nx - x0);
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    constexpr int R = 0, A = N, B = N + NB * N;
+    load_roots<T>(R, a.roots, N);
+    {
+        C2<T> *s = sptr<T>(A);
+        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+            const int bb = t % NB, y = t / NB;
+            const int f = bb / TX, b = bb % TX;
+            s[t] = (f < a.nf && b < valid) ? a.spec[f][zoff + (long long)y * a.nx + b]
+                                           : mk2<T>(T(0), T(0));
+        }
+    }
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    {
+        C2<T> *s = sptr<T>(X);
+        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+            const int bb = t % NB, ky = t / NB;
+            const int kx = x0 + min(bb % TX, valid - 1);
+            const int kxm = (a.nx - kx) % a.nx, kym = (N - ky) % N;
+            const T wgt = T(0.5) * (a.mx[kx] * a.my[ky] + a.mx[kxm] * a.my[kym]) * a.scale;
+            s[t] = wgt * s[t];
+        }
+    }
+    __syncthreads();
+    const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    const C2<T> *s = sptr<T>(r);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int bb = t % NB, y = t / NB;
+        const int f = bb / TX, b = bb % TX;
+        if (f < a.nf && b < valid) a.spec[f][zoff + (long long)y * a.nx + b] = s[t];
+    }
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
+    constexpr int NB = ct_lines(N, 2);
+    const int L0 = blockIdx.x * NB;
+    const int valid = min(NB, a.nlines - L0);
+    constexpr int R = 0, A = N, B = N + NB * N;
+    const long long g0 = (long long)L0 * N;
+    load_roots<T>(R, a.roots, N);
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    int mybad = 0;
+    for (int f = 0; f < a.nf; ++f) {
+        const C2<T> *spec = a.spec[f];
+        cx_load<T, N, NB>(A, valid, [&](int t) { return spec[g0 + t]; });
+        __syncthreads();
+        const int X = ct_fft<T, N, NB, +1>(A, B, R);
+        cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) {
+            if (!(isfinite(v.x) && isfinite(v.y))) mybad = 1;
+            store_field(a.out[f], g0 + t, v);
+        });
+        __syncthreads();
+    }
+    if (a.st) {
+        if (mybad) bad = 1;
+        __syncthreads();
+        if (threadIdx.x == 0 && bad)
+            atomicMin(reinterpret_cast<unsigned long long *>(&a.st->first_bad_step),
+                      (unsigned long long)(a.st->step + 1));
+    }
+}
+
+}  // namespace hqt

@@ -12,19 +12,28 @@
 // of the earlier passes; butterfly j reads x[j + r*n/R], r < R, applies the
 // twiddles w_n^{r*(j mod Ns)*n/(Ns*R)}, does a radix-R DFT in registers and
 // writes to (j - j mod Ns)*R + j mod Ns + k*Ns.  Radices 2,4,8,16 use an
-// in-register radix-2 network; odd primes up to 47 use the real-pair
-// (cos/sin) form of the prime DFT; any other prime falls back to a direct
-// one-output-per-thread sum.
+// in-register radix-2 network and 3,5,7,11,13 the real-pair (cos/sin) form
+// of the prime DFT, one butterfly per thread.  Larger odd primes (e.g. the
+// 43 of n = 301 = 7*43) run in two phases so that many threads share one
+// butterfly: (1) twiddle and fold the inputs in place into a_t = x_t + x_{R-t},
+// b_t = x_t - x_{R-t}; (2) each thread accumulates a block of KB output pairs
+// X[k], X[R-k] = x_0 + sum_t a_t cos(2 pi t k/R) -+ i sum_t b_t sin(..).
+//
+// Shared-memory layout: element e of line b at e*nb + b (element-major), so
+// consecutive threads touch consecutive lines.
 #pragma once
 #include "hqt_dev.cuh"
 
 namespace hqt {
 
-// Defined here: this header is compiled into exactly one translation unit.
+// Each translation unit that includes this header owns a private copy of the
+// radix tables (internal linkage) and uploads it in its set-up function.
+namespace {
 __constant__ double c_tab_cos_d[kTabTotal];
 __constant__ double c_tab_sin_d[kTabTotal];
 __constant__ float c_tab_cos_f[kTabTotal];
 __constant__ float c_tab_sin_f[kTabTotal];
+}  // namespace
 
 template <typename T> struct Tab;
 template <> struct Tab<double> {
@@ -137,14 +146,10 @@ __device__ __forceinline__ void dft_store(C2<T> (&v)[R], C2<T> *D, int a0, int k
         dft_odd_store<T, R>(v, D, a0, ks, sign);
 }
 
-// One Stockham pass with a compile-time radix.  Element e of line b sits at
-// e*es + b*bs (shared-memory element offsets).  `bfast` maps consecutive
-// threads to consecutive lines (element-major layout) instead of consecutive
-// butterflies (line-major layout).
+// One Stockham pass with a compile-time radix, one butterfly per thread.
 template <typename T, int R>
-__device__ __noinline__ void stockham_pass(int src, int dst, int roots, int n,
-                                              int Ns, int nb, int es, int bs,
-                                              bool bfast, int sign) {
+__device__ __forceinline__ void stockham_pass(int src, int dst, int roots, int n,
+                                              int Ns, int nb, int sign) {
     const C2<T> *S = sptr<T>(src);
     C2<T> *D = sptr<T>(dst);
     const C2<T> *W = sptr<T>(roots);
@@ -152,72 +157,113 @@ __device__ __noinline__ void stockham_pass(int src, int dst, int roots, int n,
     const int total = nb * nR;
     const int qs = n / (Ns * R);
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int b, j;
-        if (bfast) {
-            b = t % nb;
-            j = t / nb;
-        } else {
-            j = t % nR;
-            b = t / nR;
-        }
+        const int b = t % nb;
+        const int j = t / nb;
         const int m = j % Ns;
-        const int base = b * bs;
         C2<T> v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = S[(j + r * nR) * es + base];
+        for (int r = 0; r < R; ++r) v[r] = S[(j + r * nR) * nb + b];
         if (m > 0) {
             const int step = m * qs;
             int q = 0;
 #pragma unroll
             for (int r = 1; r < R; ++r) {
                 q += step;
-                if (q >= n) q -= n;
                 C2<T> w = W[q];
                 if (sign > 0) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
         const int idxD = (j - m) * R + m;
-        dft_store<T, R>(v, D, idxD * es + base, Ns * es, sign);
+        dft_store<T, R>(v, D, idxD * nb + b, Ns * nb, sign);
     }
 }
 
-// Any radix: direct sum, one output element per thread.
+// Odd prime radix R >= 17 (runtime), two phases.  KB output pairs per work item.
+constexpr int kBigKB = 6;
+
 template <typename T>
-__device__ __noinline__ void generic_pass(int src, int dst, int roots, int n, int R,
-                                          int Ns, int nb, int es, int bs, bool bfast,
-                                          int sign) {
-    const C2<T> *S = sptr<T>(src);
+__device__ __noinline__ void bigodd_pass(int src, int dst, int roots, int n, int R,
+                                         int Ns, int nb, int sign) {
+    C2<T> *S = sptr<T>(src);
     C2<T> *D = sptr<T>(dst);
     const C2<T> *W = sptr<T>(roots);
     const int nR = n / R;
-    const int total = nb * n;
+    const int M = (R - 1) / 2;
     const int qs = n / (Ns * R);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int b, o;
-        if (bfast) {
-            b = t % nb;
-            o = t / nb;
-        } else {
-            o = t % n;
-            b = t / n;
+    const int stepR = n / R;  // W[q*stepR] = exp(-2 pi i q / R)
+    // phase 1: twiddle and fold, in place
+    const int tot1 = nb * nR * M;
+    for (int it = threadIdx.x; it < tot1; it += blockDim.x) {
+        const int b = it % nb;
+        const int rest = it / nb;
+        const int j = rest % nR;
+        const int t = 1 + rest / nR;
+        const int m = j % Ns;
+        const int e1 = (j + t * nR) * nb + b, e2 = (j + (R - t) * nR) * nb + b;
+        C2<T> u = S[e1], v = S[e2];
+        if (m > 0) {
+            C2<T> w1 = W[t * m * qs], w2 = W[(R - t) * m * qs];
+            if (sign > 0) {
+                w1.y = -w1.y;
+                w2.y = -w2.y;
+            }
+            u = cmul(u, w1);
+            v = cmul(v, w2);
         }
-        const int m = o % Ns;
-        const int k = (o / Ns) % R;
-        const int g = o / (Ns * R);
-        const int j = g * Ns + m;
-        const int qstep = (m + k * Ns) * qs;
-        const int base = b * bs;
-        C2<T> acc = mk2<T>(T(0), T(0));
-        int q = 0;
-        for (int r = 0; r < R; ++r) {
-            C2<T> w = W[q];
-            if (sign > 0) w.y = -w.y;
-            acc = acc + cmul(S[(j + r * nR) * es + base], w);
-            q += qstep;
-            if (q >= n) q -= n;
+        S[e1] = u + v;
+        S[e2] = u - v;
+    }
+    __syncthreads();
+    // phase 2: blocks of KB output pairs; the block index varies slowest so
+    // that a warp mostly reads the same cos/sin entries (broadcast)
+    const int nkb = (M + kBigKB) / kBigKB;  // pairs 0..M
+    const int tot2 = nb * nR * nkb;
+    const T sg = (sign < 0) ? T(1) : T(-1);
+    for (int it = threadIdx.x; it < tot2; it += blockDim.x) {
+        const int b = it % nb;
+        const int rest = it / nb;
+        const int j = rest % nR;
+        const int k0 = (rest / nR) * kBigKB;
+        const int m = j % Ns;
+        const int idxD = (j - m) * R + m;
+        const C2<T> x0 = S[j * nb + b];
+        T pr[kBigKB], pi[kBigKB], qr[kBigKB], qi[kBigKB];
+        int qq[kBigKB];
+#pragma unroll
+        for (int i = 0; i < kBigKB; ++i) {
+            pr[i] = x0.x;
+            pi[i] = x0.y;
+            qr[i] = T(0);
+            qi[i] = T(0);
+            qq[i] = 0;
         }
-        D[o * es + base] = acc;
+        for (int t = 1; t <= M; ++t) {
+            const C2<T> a = S[(j + t * nR) * nb + b];
+            const C2<T> c = S[(j + (R - t) * nR) * nb + b];
+#pragma unroll
+            for (int i = 0; i < kBigKB; ++i) {
+                qq[i] += k0 + i;  // (t*k) mod R, incrementally
+                if (qq[i] >= R) qq[i] -= R;
+                const C2<T> w = W[qq[i] * stepR];  // (cos, -sin)
+                pr[i] = fma(a.x, w.x, pr[i]);
+                pi[i] = fma(a.y, w.x, pi[i]);
+                qr[i] = fma(c.x, -w.y, qr[i]);
+                qi[i] = fma(c.y, -w.y, qi[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kBigKB; ++i) {
+            const int k = k0 + i;
+            if (k > M) break;
+            if (k == 0) {
+                D[idxD * nb + b] = mk2<T>(pr[i], pi[i]);
+            } else {
+                const T yr = qr[i] * sg, yi = qi[i] * sg;
+                D[(idxD + k * Ns) * nb + b] = mk2<T>(pr[i] + yi, pi[i] - yr);
+                D[(idxD + (R - k) * Ns) * nb + b] = mk2<T>(pr[i] - yi, pi[i] + yr);
+            }
+        }
     }
 }
 
@@ -225,17 +271,16 @@ __device__ __noinline__ void generic_pass(int src, int dst, int roots, int n, in
 // returns the offset of the buffer that holds the result.  sign = -1 forward
 // (exp(-2 pi i jk/n)), +1 inverse (unnormalised).
 template <typename T>
-__device__ __noinline__ int fft_run(int a, int b, int roots, FFTPlan plan, int nb,
-                                    int es, int bs, bool bfast, int sign) {
+__device__ __noinline__ int fft_run(int a, int b, int roots, FFTPlan plan, int nb, int sign) {
     int src = a, dst = b;
     const int n = plan.n;
     for (int p = 0; p < plan.npass; ++p) {
         const int R = plan.radix[p];
         const int Ns = plan.ns[p];
         switch (R) {
-#define HQT_PASS(RR)                                                              \
-    case RR:                                                                      \
-        stockham_pass<T, RR>(src, dst, roots, n, Ns, nb, es, bs, bfast, sign);     \
+#define HQT_PASS(RR)                                                   \
+    case RR:                                                           \
+        stockham_pass<T, RR>(src, dst, roots, n, Ns, nb, sign);        \
         break;
             HQT_PASS(2)
             HQT_PASS(3)
@@ -246,18 +291,9 @@ __device__ __noinline__ int fft_run(int a, int b, int roots, FFTPlan plan, int n
             HQT_PASS(11)
             HQT_PASS(13)
             HQT_PASS(16)
-            HQT_PASS(17)
-            HQT_PASS(19)
-            HQT_PASS(23)
-            HQT_PASS(29)
-            HQT_PASS(31)
-            HQT_PASS(37)
-            HQT_PASS(41)
-            HQT_PASS(43)
-            HQT_PASS(47)
 #undef HQT_PASS
         default:
-            generic_pass<T>(src, dst, roots, n, R, Ns, nb, es, bs, bfast, sign);
+            bigodd_pass<T>(src, dst, roots, n, R, Ns, nb, sign);
         }
         __syncthreads();
         const int t = src;

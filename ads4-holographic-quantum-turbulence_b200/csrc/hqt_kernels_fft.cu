@@ -31,6 +31,7 @@ cudaError_t fft_init(const double *tc, const double *ts, int ntab, int max_smem)
     return e;
 }
 
+
 cudaError_t launch_x_rhs(const XRhsArgs<double> &a, int grid, size_t smem, cudaStream_t s) {
     k_x_rhs<double><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();

@@ -25,6 +25,14 @@ cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cu
 cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s);
 
+// Compile-time line lengths (hqt_c<N>.cu): kinds of pass kernel.
+enum CtKind { CT_X_RHS, CT_Y_RHS, CT_X_D1, CT_Y_D1, CT_FX_FWD, CT_FY, CT_FX_INV };
+template <int N> cudaError_t ct_init(const double *tab_cos, const double *tab_sin, int ntab,
+                                     const double *big_cos, const double *big_sin, int nbig,
+                                     int max_smem);
+template <int N>
+cudaError_t ct_launch(int kind, const void *args, dim3 grid, size_t smem, cudaStream_t s);
+
 // Column kernels, one translation unit per compile-time column length N.
 // mode 0: right-hand side only, 1..4: RK stage.
 template <int N> cudaError_t z_init(int max_smem);
@@ -42,6 +50,8 @@ cudaError_t z_misc(const ZColArgs<double> &a, const ZHost &h, int grid, int thre
 
 // Compile-time column lengths of this build; a run uses the smallest >= nz.
 #define HQT_NZP_LIST(X) X(8) X(12) X(16) X(17) X(21) X(25) X(33)
+// Line lengths with compile-time transforms; other lengths use hqt_fft.cuh.
+#define HQT_CN_LIST(X) X(33) X(64) X(128) X(192) X(256) X(301) X(512)
 
 namespace hqt {
 #define HQT_ZDECL(N)                                                                       \
@@ -55,4 +65,11 @@ namespace hqt {
     cudaError_t z_misc<N>(const ZColArgs<double> &, const ZHost &, int, int, cudaStream_t);
 HQT_NZP_LIST(HQT_ZDECL)
 #undef HQT_ZDECL
+#define HQT_CDECL(N)                                                                       \
+    template <>                                                                            \
+    cudaError_t ct_init<N>(const double *, const double *, int, const double *,            \
+                           const double *, int, int);                                      \
+    template <> cudaError_t ct_launch<N>(int, const void *, dim3, size_t, cudaStream_t);
+HQT_CN_LIST(HQT_CDECL)
+#undef HQT_CDECL
 }  // namespace hqt

@@ -144,6 +144,19 @@ void make_radix_tables(std::vector<double> &c, std::vector<double> &s) {
     }
 }
 
+void make_big_tables(std::vector<double> &c, std::vector<double> &s) {
+    static const int primes[] = {17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61};
+    c.clear();
+    s.clear();
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int R : primes)
+        for (int t = 0; t < R; ++t) {
+            const long double a = 2.0L * pi * (long double)t / (long double)R;
+            c.push_back((double)std::cos(a));
+            s.push_back((double)std::sin(a));
+        }
+}
+
 static int matlab_round_pos(double v) { return (int)std::floor(v + 0.5); }
 
 void filter_band(int n, int &lo, int &hi) {

@@ -24,6 +24,9 @@ std::vector<double2> make_roots(int n);
 // cos/sin tables of the radix butterflies, in the order of kTabRadices.
 void make_radix_tables(std::vector<double> &c, std::vector<double> &s);
 
+// cos/sin tables of the large odd primes of the compile-time transforms.
+void make_big_tables(std::vector<double> &c, std::vector<double> &s);
+
 // MATLAB round of the filter band edges: 1-based indices lo..hi of the
 // zeroed modes (tevol_driven_cluster.m:27-30).
 void filter_band(int n, int &lo, int &hi);

@@ -57,42 +57,74 @@ __device__ __forceinline__ void load_roots(int roots, const C2<T> *g, int n) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
 }
 
-// dst[e] = (i*s1*k(e))^order-style multiplier applied to src[e] over a batch.
-// order 1: i*s1*k ; order 2: s2*k^2.  Layout as in fft_run.
+// dst = m(k) * src over a batch (element-major, nb lines): order 1 multiplies
+// by i*s1*k, order 2 by s2*k^2 (k the signed wavenumber, Nyquist -> 0).
 template <typename T>
-__device__ __forceinline__ void apply_deriv(int dst, int src, int n, int nb, int es,
-                                            int bs, bool bfast, int order, T s1,
-                                            T s2) {
+__device__ __forceinline__ void apply_deriv(int dst, int src, int n, int nb, int order,
+                                            T s1, T s2) {
     const C2<T> *S = sptr<T>(src);
     C2<T> *D = sptr<T>(dst);
     const int total = n * nb;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int b, e;
-        if (bfast) {
-            b = t % nb;
-            e = t / nb;
-        } else {
-            e = t % n;
-            b = t / n;
-        }
-        const int a = e * es + b * bs;
-        const T kk = T(wavenum(e, n));
-        const C2<T> v = S[a];
+        const T kk = T(wavenum(t / nb, n));
+        const C2<T> v = S[t];
         if (order == 1) {
             const T m = s1 * kk;
-            D[a] = mk2<T>(-m * v.y, m * v.x);
+            D[t] = mk2<T>(-m * v.y, m * v.x);
         } else {
             const T m = s2 * kk * kk;
-            D[a] = mk2<T>(m * v.x, m * v.y);
+            D[t] = mk2<T>(m * v.x, m * v.y);
         }
     }
 }
 
+// x lines: a batch of nb consecutive lines is one contiguous block of nb*n
+// elements in global memory starting at g0.
+template <typename T, typename F>
+__device__ __forceinline__ void xl_load(int buf, int n, int nb, F get) {
+    C2<T> *s = sptr<T>(buf);
+    const int tot = n * nb;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        const int b = t / n, e = t - b * n;
+        s[e * nb + b] = get(t);
+    }
+}
+template <typename T, typename F>
+__device__ __forceinline__ void xl_store(int buf, int n, int nb, F put) {
+    const C2<T> *s = sptr<T>(buf);
+    const int tot = n * nb;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        const int b = t / n, e = t - b * n;
+        put(t, s[e * nb + b]);
+    }
+}
+// y lines: nb adjacent columns x0..x0+nb-1 of one z-slice; element (y, b) is
+// shared-memory index y*nb + b and global index zoff + y*nx + b.
+template <typename T, typename F>
+__device__ __forceinline__ void yl_load(int buf, int n, int nb, int nx, long long zoff, F get) {
+    C2<T> *s = sptr<T>(buf);
+    const int tot = n * nb;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        const int y = t / nb, b = t - y * nb;
+        s[t] = get(zoff + (long long)y * nx + b);
+    }
+}
+template <typename T, typename F>
+__device__ __forceinline__ void yl_store(int buf, int n, int nb, int nx, long long zoff, F put) {
+    const C2<T> *s = sptr<T>(buf);
+    const int tot = n * nb;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        const int y = t / nb, b = t - y * nb;
+        put(zoff + (long long)y * nx + b, s[t]);
+    }
+}
+
+#define HQT_FFT_BOUNDS __launch_bounds__(128, 4)
+
 // ------------------------------------------------------------------------
 // x pass of a right-hand side
 // ------------------------------------------------------------------------
-
-template <typename T> __global__ void __launch_bounds__(128) k_x_rhs(XRhsArgs<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_x_rhs(XRhsArgs<T> a) {
     const int n = a.plan.n;
     const int L0 = blockIdx.x * a.NB;
     const int nb = min(a.NB, a.nlines - L0);
@@ -100,62 +132,41 @@ template <typename T> __global__ void __launch_bounds__(128) k_x_rhs(XRhsArgs<T>
     const int R = 0, A = n, B = n + a.NB * n, C = n + 2 * a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
-    const int tot = nb * n;
     // ---- Psi ----
-    {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) s[t] = a.psi[g0 + t];
-    }
+    xl_load<T>(A, n, nb, [&](int t) { return a.psi[g0 + t]; });
     __syncthreads();
-    int X = fft_run<T>(A, B, R, a.plan, nb, 1, n, false, -1);
+    int X = fft_run<T>(A, B, R, a.plan, nb, -1);
     int Y = (X == A) ? B : A;
-    apply_deriv<T>(Y, X, n, nb, 1, n, false, 1, a.s1, a.s2);
+    apply_deriv<T>(Y, X, n, nb, 1, a.s1, a.s2);
     __syncthreads();
-    int r1 = fft_run<T>(Y, C, R, a.plan, nb, 1, n, false, +1);
-    {
-        const C2<T> *s = sptr<T>(r1);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) a.dxpsi[g0 + t] = s[t];
-    }
-    apply_deriv<T>(X, X, n, nb, 1, n, false, 2, a.s1, a.s2);
+    int r1 = fft_run<T>(Y, C, R, a.plan, nb, +1);
+    xl_store<T>(r1, n, nb, [&](int t, C2<T> v) { a.dxpsi[g0 + t] = v; });
+    apply_deriv<T>(X, X, n, nb, 2, a.s1, a.s2);
     __syncthreads();
     int fr = (r1 == Y) ? C : Y;
-    int r2 = fft_run<T>(X, fr, R, a.plan, nb, 1, n, false, +1);
-    {
-        const C2<T> *s = sptr<T>(r2);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) a.dxxpsi[g0 + t] = s[t];
-    }
+    int r2 = fft_run<T>(X, fr, R, a.plan, nb, +1);
+    xl_store<T>(r2, n, nb, [&](int t, C2<T> v) { a.dxxpsi[g0 + t] = v; });
     __syncthreads();
     // ---- A_x + i A_y ----
-    {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x)
-            s[t] = mk2<T>(a.ax[g0 + t], a.ay[g0 + t]);
-    }
+    xl_load<T>(A, n, nb, [&](int t) { return mk2<T>(a.ax[g0 + t], a.ay[g0 + t]); });
     __syncthreads();
-    X = fft_run<T>(A, B, R, a.plan, nb, 1, n, false, -1);
+    X = fft_run<T>(A, B, R, a.plan, nb, -1);
     Y = (X == A) ? B : A;
-    apply_deriv<T>(Y, X, n, nb, 1, n, false, 1, a.s1, a.s2);
+    apply_deriv<T>(Y, X, n, nb, 1, a.s1, a.s2);
     __syncthreads();
-    r1 = fft_run<T>(Y, C, R, a.plan, nb, 1, n, false, +1);
-    {
-        const C2<T> *s = sptr<T>(r1);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) a.E[g0 + t] = s[t];
-    }
-    apply_deriv<T>(X, X, n, nb, 1, n, false, 2, a.s1, a.s2);
+    r1 = fft_run<T>(Y, C, R, a.plan, nb, +1);
+    xl_store<T>(r1, n, nb, [&](int t, C2<T> v) { a.E[g0 + t] = v; });
+    apply_deriv<T>(X, X, n, nb, 2, a.s1, a.s2);
     __syncthreads();
     fr = (r1 == Y) ? C : Y;
-    r2 = fft_run<T>(X, fr, R, a.plan, nb, 1, n, false, +1);
-    {
-        const C2<T> *s = sptr<T>(r2);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) a.dxxay[g0 + t] = s[t].y;
-    }
+    r2 = fft_run<T>(X, fr, R, a.plan, nb, +1);
+    xl_store<T>(r2, n, nb, [&](int t, C2<T> v) { a.dxxay[g0 + t] = v.y; });
 }
 
 // ------------------------------------------------------------------------
 // y pass of a right-hand side
 // ------------------------------------------------------------------------
-
-template <typename T> __global__ void __launch_bounds__(128) k_y_rhs(YRhsArgs<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_y_rhs(YRhsArgs<T> a) {
     const int n = a.ny;
     const int x0 = blockIdx.x * a.TX;
     const int nb = min(a.TX, a.nx - x0);
@@ -164,54 +175,36 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_rhs(YRhsArgs<T>
     const int R = 0, A0 = n, A1 = n + a.TX * n, A2 = n + 2 * a.TX * n;
     const int P = n, Q = n + 2 * a.TX * n;
     load_roots<T>(R, a.roots, n);
-    const int tot = nb * n;
     // ---- Psi: d_y and d_yy ----
-    {
-        C2<T> *s = sptr<T>(A0);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
-            s[t] = a.psi[zoff + (long long)y * a.nx + b];
-        }
-    }
+    yl_load<T>(A0, n, nb, a.nx, zoff, [&](long long g) { return a.psi[g]; });
     __syncthreads();
-    int X = fft_run<T>(A0, A1, R, a.plan, nb, nb, 1, true, -1);
+    int X = fft_run<T>(A0, A1, R, a.plan, nb, -1);
     int Y = (X == A0) ? A1 : A0;
-    apply_deriv<T>(Y, X, n, nb, nb, 1, true, 1, a.s1, a.s2);
+    apply_deriv<T>(Y, X, n, nb, 1, a.s1, a.s2);
     __syncthreads();
-    int r1 = fft_run<T>(Y, A2, R, a.plan, nb, nb, 1, true, +1);
-    {
-        const C2<T> *s = sptr<T>(r1);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
-            a.dypsi[zoff + (long long)y * a.nx + b] = s[t];
-        }
-    }
-    apply_deriv<T>(X, X, n, nb, nb, 1, true, 2, a.s1, a.s2);
+    int r1 = fft_run<T>(Y, A2, R, a.plan, nb, +1);
+    yl_store<T>(r1, n, nb, a.nx, zoff, [&](long long g, C2<T> v) { a.dypsi[g] = v; });
+    apply_deriv<T>(X, X, n, nb, 2, a.s1, a.s2);
     __syncthreads();
     int fr = (r1 == Y) ? A2 : Y;
-    int r2 = fft_run<T>(X, fr, R, a.plan, nb, nb, 1, true, +1);
-    {
-        const C2<T> *s = sptr<T>(r2);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
-            const long long g = zoff + (long long)y * a.nx + b;
-            a.lap[g] = a.dxxpsi[g] + s[t];
-        }
-    }
+    int r2 = fft_run<T>(X, fr, R, a.plan, nb, +1);
+    yl_store<T>(r2, n, nb, a.nx, zoff,
+                [&](long long g, C2<T> v) { a.lap[g] = a.dxxpsi[g] + v; });
     __syncthreads();
     // ---- C = A_x + i A_y and E = d_x C as one batch of 2*nb lines ----
     const int nb2 = 2 * nb;
     {
         C2<T> *s = sptr<T>(P);
+        const int tot = nb * n;
         for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
+            const int y = t / nb, b = t - y * nb;
             const long long g = zoff + (long long)y * a.nx + b;
             s[y * nb2 + b] = mk2<T>(a.ax[g], a.ay[g]);
             s[y * nb2 + nb + b] = a.E[g];
         }
     }
     __syncthreads();
-    X = fft_run<T>(P, Q, R, a.plan, nb2, nb2, 1, true, -1);
+    X = fft_run<T>(P, Q, R, a.plan, nb2, -1);
     {
         // split the pair spectra and form P1 = R1 + i R2, P2 = R3 with
         // R1 = d_y A_y, R2 = -d_y d_x A_x, R3 = d_y d_x A_y - d_yy A_x.
@@ -224,44 +217,36 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_rhs(YRhsArgs<T>
             const int kp = (n - k) % n;
             const C2<T> Cc = s[k * nb2 + b], Cp = s[kp * nb2 + b];
             const C2<T> Ec = s[k * nb2 + nb + b], Ep = s[kp * nb2 + nb + b];
-            // k
-            {
-                const T kk = T(wavenum(k, n));
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                if (side == 1 && kp == k) break;
+                const int kk_ = side == 0 ? k : kp;
+                const C2<T> c1 = side == 0 ? Cc : Cp, c2 = side == 0 ? Cp : Cc;
+                const C2<T> e1 = side == 0 ? Ec : Ep, e2 = side == 0 ? Ep : Ec;
+                const T kk = T(wavenum(kk_, n));
                 const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk;
-                // Ax^ = (Cc + conj Cp)/2 ; Ay^ = (Cc - conj Cp)/(2i)
-                const C2<T> axh = mk2<T>(h * (Cc.x + Cp.x), h * (Cc.y - Cp.y));
-                const C2<T> ayh = mk2<T>(h * (Cc.y + Cp.y), -h * (Cc.x - Cp.x));
-                const C2<T> exh = mk2<T>(h * (Ec.x + Ep.x), h * (Ec.y - Ep.y));
-                const C2<T> eyh = mk2<T>(h * (Ec.y + Ep.y), -h * (Ec.x - Ep.x));
+                // Ax^ = (c1 + conj c2)/2 ; Ay^ = (c1 - conj c2)/(2i)
+                const C2<T> axh = mk2<T>(h * (c1.x + c2.x), h * (c1.y - c2.y));
+                const C2<T> ayh = mk2<T>(h * (c1.y + c2.y), -h * (c1.x - c2.x));
+                const C2<T> exh = mk2<T>(h * (e1.x + e2.x), h * (e1.y - e2.y));
+                const C2<T> eyh = mk2<T>(h * (e1.y + e2.y), -h * (e1.x - e2.x));
                 // R1 = i m1 ayh ; R2 = -i m1 exh ; R3 = i m1 eyh - m2 axh
-                const C2<T> r1 = mk2<T>(-m1 * ayh.y, m1 * ayh.x);
-                const C2<T> r2 = mk2<T>(m1 * exh.y, -m1 * exh.x);
-                const C2<T> r3 = mk2<T>(-m1 * eyh.y - m2 * axh.x, m1 * eyh.x - m2 * axh.y);
-                s[k * nb2 + b] = mk2<T>(r1.x - r2.y, r1.y + r2.x);
-                s[k * nb2 + nb + b] = r3;
-            }
-            if (kp != k) {
-                const T kk = T(wavenum(kp, n));
-                const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk;
-                const C2<T> axh = mk2<T>(h * (Cp.x + Cc.x), h * (Cp.y - Cc.y));
-                const C2<T> ayh = mk2<T>(h * (Cp.y + Cc.y), -h * (Cp.x - Cc.x));
-                const C2<T> exh = mk2<T>(h * (Ep.x + Ec.x), h * (Ep.y - Ec.y));
-                const C2<T> eyh = mk2<T>(h * (Ep.y + Ec.y), -h * (Ep.x - Ec.x));
-                const C2<T> r1 = mk2<T>(-m1 * ayh.y, m1 * ayh.x);
-                const C2<T> r2 = mk2<T>(m1 * exh.y, -m1 * exh.x);
-                const C2<T> r3 = mk2<T>(-m1 * eyh.y - m2 * axh.x, m1 * eyh.x - m2 * axh.y);
-                s[kp * nb2 + b] = mk2<T>(r1.x - r2.y, r1.y + r2.x);
-                s[kp * nb2 + nb + b] = r3;
+                const C2<T> q1 = mk2<T>(-m1 * ayh.y, m1 * ayh.x);
+                const C2<T> q2 = mk2<T>(m1 * exh.y, -m1 * exh.x);
+                const C2<T> q3 = mk2<T>(-m1 * eyh.y - m2 * axh.x, m1 * eyh.x - m2 * axh.y);
+                s[kk_ * nb2 + b] = mk2<T>(q1.x - q2.y, q1.y + q2.x);
+                s[kk_ * nb2 + nb + b] = q3;
             }
         }
     }
     __syncthreads();
     const int Xo = (X == P) ? Q : P;
-    const int r3 = fft_run<T>(X, Xo, R, a.plan, nb2, nb2, 1, true, +1);
+    const int r3 = fft_run<T>(X, Xo, R, a.plan, nb2, +1);
     {
         const C2<T> *s = sptr<T>(r3);
+        const int tot = nb * n;
         for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
+            const int y = t / nb, b = t - y * nb;
             const long long g = zoff + (long long)y * a.nx + b;
             const C2<T> p1 = s[y * nb2 + b];
             const C2<T> p2 = s[y * nb2 + nb + b];
@@ -275,8 +260,7 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_rhs(YRhsArgs<T>
 // ------------------------------------------------------------------------
 // single-field first derivatives
 // ------------------------------------------------------------------------
-
-template <typename T> __global__ void __launch_bounds__(128) k_x_d1(XD1Args<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_x_d1(XD1Args<T> a) {
     const int n = a.plan.n;
     const int L0 = blockIdx.x * a.NB;
     const int nb = min(a.NB, a.nlines - L0);
@@ -284,59 +268,40 @@ template <typename T> __global__ void __launch_bounds__(128) k_x_d1(XD1Args<T> a
     const int R = 0, A = n, B = n + a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
-    const int tot = nb * n;
-    {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) s[t] = load_field(a.in, g0 + t);
-    }
+    xl_load<T>(A, n, nb, [&](int t) { return load_field(a.in, g0 + t); });
     __syncthreads();
-    int X = fft_run<T>(A, B, R, a.plan, nb, 1, n, false, -1);
-    apply_deriv<T>(X, X, n, nb, 1, n, false, 1, a.s1, T(0));
+    int X = fft_run<T>(A, B, R, a.plan, nb, -1);
+    apply_deriv<T>(X, X, n, nb, 1, a.s1, T(0));
     __syncthreads();
     const int Y = (X == A) ? B : A;
-    const int r = fft_run<T>(X, Y, R, a.plan, nb, 1, n, false, +1);
-    const C2<T> *s = sptr<T>(r);
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) store_field(a.out, g0 + t, s[t]);
+    const int r = fft_run<T>(X, Y, R, a.plan, nb, +1);
+    xl_store<T>(r, n, nb, [&](int t, C2<T> v) { store_field(a.out, g0 + t, v); });
 }
 
-
-template <typename T> __global__ void __launch_bounds__(128) k_y_d1(YD1Args<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_y_d1(YD1Args<T> a) {
     const int n = a.ny;
     const int x0 = blockIdx.x * a.TX;
     const int nb = min(a.TX, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const int R = 0, A = n, B = n + a.TX * n;
     load_roots<T>(R, a.roots, n);
-    const int tot = nb * n;
-    {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int b = t % nb, y = t / nb;
-            s[t] = load_field(a.in, zoff + (long long)y * a.nx + b);
-        }
-    }
+    yl_load<T>(A, n, nb, a.nx, zoff, [&](long long g) { return load_field(a.in, g); });
     __syncthreads();
-    int X = fft_run<T>(A, B, R, a.plan, nb, nb, 1, true, -1);
-    apply_deriv<T>(X, X, n, nb, nb, 1, true, 1, a.s1, T(0));
+    int X = fft_run<T>(A, B, R, a.plan, nb, -1);
+    apply_deriv<T>(X, X, n, nb, 1, a.s1, T(0));
     __syncthreads();
     const int Y = (X == A) ? B : A;
-    const int r = fft_run<T>(X, Y, R, a.plan, nb, nb, 1, true, +1);
-    const C2<T> *s = sptr<T>(r);
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-        const int b = t % nb, y = t / nb;
-        const long long g = zoff + (long long)y * a.nx + b;
-        C2<T> v = s[t];
+    const int r = fft_run<T>(X, Y, R, a.plan, nb, +1);
+    yl_store<T>(r, n, nb, a.nx, zoff, [&](long long g, C2<T> v) {
         if (a.add_re) v.x += a.add_re[g];
         store_field(a.out, g, v);
-    }
+    });
 }
 
 // ------------------------------------------------------------------------
 // Fourier filter: x forward, y (forward, weight, inverse), x inverse
 // ------------------------------------------------------------------------
-
-template <typename T>
-__global__ void __launch_bounds__(128) k_x_filt_fwd(XFiltFwdArgs<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_fwd(XFiltFwdArgs<T> a) {
     const int n = a.plan.n;
     const int L0 = blockIdx.x * a.NB;
     const int nb = min(a.NB, a.nlines - L0);
@@ -345,31 +310,28 @@ __global__ void __launch_bounds__(128) k_x_filt_fwd(XFiltFwdArgs<T> a) {
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
     const int w = a.st ? a.st->winding : 0;
-    const int tot = nb * n;
     for (int f = 0; f < a.nf; ++f) {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+        xl_load<T>(A, n, nb, [&](int t) {
             C2<T> v = load_field(a.in[f], g0 + t);
             if (f == 0 && w != 0) {
-                // y of line L0 + t/n ; phase -2*pi*y*w/ny (tevol_driven_cluster.m:139)
+                // phase -2*pi*y*w/ny of line L0 + t/n (tevol_driven_cluster.m:139)
                 const int y = (L0 + t / n) % a.ny;
                 const long long q = ((long long)y * w) % a.ny;
                 double sn, cs;
                 sincospi(-2.0 * (double)q / (double)a.ny, &sn, &cs);
                 v = mk2<T>(v.x * (T)cs - v.y * (T)sn, v.x * (T)sn + v.y * (T)cs);
             }
-            s[t] = v;
-        }
+            return v;
+        });
         __syncthreads();
-        const int X = fft_run<T>(A, B, R, a.plan, nb, 1, n, false, -1);
-        const C2<T> *sx = sptr<T>(X);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) a.spec[f][g0 + t] = sx[t];
+        const int X = fft_run<T>(A, B, R, a.plan, nb, -1);
+        C2<T> *spec = a.spec[f];
+        xl_store<T>(X, n, nb, [&](int t, C2<T> v) { spec[g0 + t] = v; });
         __syncthreads();
     }
 }
 
-
-template <typename T> __global__ void __launch_bounds__(128) k_y_filt(YFiltArgs<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_y_filt(YFiltArgs<T> a) {
     const int n = a.ny;
     const int x0 = blockIdx.x * a.TX;
     const int nb = min(a.TX, a.nx - x0);
@@ -387,7 +349,7 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_filt(YFiltArgs<
         }
     }
     __syncthreads();
-    const int X = fft_run<T>(A, B, R, a.plan, nbl, nbl, 1, true, -1);
+    const int X = fft_run<T>(A, B, R, a.plan, nbl, -1);
     {
         C2<T> *s = sptr<T>(X);
         for (int t = threadIdx.x; t < tot; t += blockDim.x) {
@@ -400,7 +362,7 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_filt(YFiltArgs<
     }
     __syncthreads();
     const int Y = (X == A) ? B : A;
-    const int r = fft_run<T>(X, Y, R, a.plan, nbl, nbl, 1, true, +1);
+    const int r = fft_run<T>(X, Y, R, a.plan, nbl, +1);
     const C2<T> *s = sptr<T>(r);
     for (int t = threadIdx.x; t < tot; t += blockDim.x) {
         const int bb = t % nbl, y = t / nbl;
@@ -409,9 +371,7 @@ template <typename T> __global__ void __launch_bounds__(128) k_y_filt(YFiltArgs<
     }
 }
 
-
-template <typename T>
-__global__ void __launch_bounds__(128) k_x_filt_inv(XFiltInvArgs<T> a) {
+template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_inv(XFiltInvArgs<T> a) {
     const int n = a.plan.n;
     const int L0 = blockIdx.x * a.NB;
     const int nb = min(a.NB, a.nlines - L0);
@@ -421,19 +381,16 @@ __global__ void __launch_bounds__(128) k_x_filt_inv(XFiltInvArgs<T> a) {
     load_roots<T>(R, a.roots, n);
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
-    const int tot = nb * n;
     int mybad = 0;
     for (int f = 0; f < a.nf; ++f) {
-        C2<T> *s = sptr<T>(A);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) s[t] = a.spec[f][g0 + t];
+        const C2<T> *spec = a.spec[f];
+        xl_load<T>(A, n, nb, [&](int t) { return spec[g0 + t]; });
         __syncthreads();
-        const int X = fft_run<T>(A, B, R, a.plan, nb, 1, n, false, +1);
-        const C2<T> *sx = sptr<T>(X);
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const C2<T> v = sx[t];
+        const int X = fft_run<T>(A, B, R, a.plan, nb, +1);
+        xl_store<T>(X, n, nb, [&](int t, C2<T> v) {
             if (!(isfinite(v.x) && isfinite(v.y))) mybad = 1;
             store_field(a.out[f], g0 + t, v);
-        }
+        });
         __syncthreads();
     }
     if (a.st) {

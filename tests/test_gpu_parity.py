@@ -230,3 +230,24 @@ def test_nonfinite_guard(hqt, cuda):
         # the context stays usable after the error
         (g1, *_), info = sim.step(*driven_state(hqt, nx, nx, nz), nsteps=1)
         assert np.all(np.isfinite(g1))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 64, 21), (301, 301, 9), (53, 59, 8)])
+def test_runtime_line_engine_parity(hqt, oracle, dev, monkeypatch, nx, ny, nz):
+    """The runtime-plan line-transform engine (used for line lengths without a
+    compile-time transform) on the same RHS and filter checks."""
+    monkeypatch.setenv("HQT_LINE_ENGINE", "runtime")
+    to_d, from_d = dev
+    Lx, Ly = 0.5 * nx, 0.45 * ny
+    Z1, Z2, Z3, Z4 = random_fields(nx, ny, nz, seed=nx + nz)
+    op = oracle.build_operators(nx, ny, nz, Lx, Ly)
+    F1, F2, F3, F4 = oracle.rhs(op, Z1, Z2, Z3, Z4)
+    with hqt.Simulation(nx, ny, nz, Lx=Lx, Ly=Ly) as sim:
+        g1, g2b, g3, g4 = sim.rhs_device(to_d(Z1), to_d(Z2), to_d(Z3), to_d(Z4))
+        x = to_d(Z3)[None].contiguous()
+        y = sim.filter_device(x)
+    assert relmax(from_d(g1), F1) < 1e-11
+    assert relmax(from_d(g3), F3) < 1e-11
+    assert relmax(from_d(g4), F4) < 1e-11
+    assert relmax(g2b.cpu().numpy().T, F2[:, :, -1]) < 1e-11
+    assert relmax(from_d(y[0]), oracle.ff(Z3, op.mask)) < 1e-12
