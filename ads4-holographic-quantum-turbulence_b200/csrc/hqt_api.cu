@@ -27,7 +27,7 @@
 namespace hqt {
 
 static constexpr int kThreadsFFT = 128;
-static constexpr int kThreadsZ = 64;
+static constexpr int kThreadsZ = 128;
 static constexpr size_t kSmemBudget = 54 * 1024;
 static constexpr int kPartials = 296;
 
@@ -55,8 +55,10 @@ struct hqt_ctx {
     double2 *psi = nullptr;
     double *at = nullptr, *ax = nullptr, *ay = nullptr, *rho = nullptr;
     // stage input and accumulators
-    double2 *ypsi = nullptr, *kpsi = nullptr;
-    double *yax = nullptr, *yay = nullptr, *kax = nullptr, *kay = nullptr, *krho = nullptr;
+    // stage inputs, double-buffered: stages 2 and 4 read Y[0], stage 3 reads Y[1]
+    double2 *ypsi2[2] = {nullptr, nullptr}, *kpsi = nullptr;
+    double *yax2[2] = {nullptr, nullptr}, *yay2[2] = {nullptr, nullptr};
+    double *kax = nullptr, *kay = nullptr, *krho = nullptr;
     // derivatives
     double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr;
     double *dxxay = nullptr, *divA = nullptr, *dxB = nullptr, *dyB = nullptr;
@@ -204,7 +206,7 @@ int pick_lines(int n, int nbuf, int cap) {
 
 ZHost zhost(const hqt_ctx *c) { return ZHost{c->nz, c->Lz.data(), c->Lz1.data(), c->zz.data()}; }
 
-size_t smem_z(int NZP) { return sizeof(double) * 4 * (size_t)NZP * kThreadsZ; }
+size_t smem_z(int NZP) { return sizeof(double) * 2 * (size_t)NZP * kThreadsZ; }
 
 // ---------------------------------------------------------------- launches
 int launch_x_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double *ay) {
@@ -387,7 +389,7 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
 template <int MODE> int launch_zstage(hqt_ctx *c, const ZStageArgs<double, double> &a) {
     const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
     const ZHost h = zhost(c);
-    Prof pr(c, K_ZSTAGE);
+    Prof pr(c, K_ZSTAGE, 2);
     switch (c->NZP) {
 #define HQT_Z(N)                                                                      \
     case N:                                                                           \
@@ -467,9 +469,12 @@ int enqueue_step(hqt_ctx *c) {
     RC(launch_y_d1(c, FieldIn<double>{nullptr, at, nullptr}, nullptr,
                    FieldOut<double>{nullptr, c->dyat, nullptr}));
     for (int s = 1; s <= 4; ++s) {
-        const double2 *ypsi = (s == 1) ? psi : c->ypsi;
-        const double *yax = (s == 1) ? ax : c->yax;
-        const double *yay = (s == 1) ? ay : c->yay;
+        // stage s reads Y[(s-2)&1] (the state itself at s = 1) and writes the
+        // next stage input to the other buffer
+        const int yi = (s == 3) ? 1 : 0, ni = (s == 2) ? 1 : 0;
+        const double2 *ypsi = (s == 1) ? psi : c->ypsi2[yi];
+        const double *yax = (s == 1) ? ax : c->yax2[yi];
+        const double *yay = (s == 1) ? ay : c->yay2[yi];
         RC(launch_x_rhs(c, ypsi, yax, yay));
         RC(launch_y_rhs(c, ypsi, yax, yay));
         ZStageArgs<double, double> a{};
@@ -497,9 +502,9 @@ int enqueue_step(hqt_ctx *c) {
         a.kax = c->kax;
         a.kay = c->kay;
         a.krho = c->krho;
-        a.npsi = c->ypsi;
-        a.nax = c->yax;
-        a.nay = c->yay;
+        a.npsi = c->ypsi2[ni];
+        a.nax = c->yax2[ni];
+        a.nay = c->yay2[ni];
         a.wpsi = psi;
         a.wax = ax;
         a.way = ay;
@@ -567,7 +572,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 3 + 2 + 1 + 1;
+    long long n = 2 + 4 * 4 + 2 + 1 + 1;
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -764,9 +769,11 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->ax, sizeof(double) * V);
     A(&c->ay, sizeof(double) * V);
     A(&c->rho, sizeof(double) * P2);
-    A(&c->ypsi, sizeof(double2) * V);
-    A(&c->yax, sizeof(double) * V);
-    A(&c->yay, sizeof(double) * V);
+    for (int b = 0; b < 2; ++b) {
+        A(&c->ypsi2[b], sizeof(double2) * V);
+        A(&c->yax2[b], sizeof(double) * V);
+        A(&c->yay2[b], sizeof(double) * V);
+    }
     A(&c->kpsi, sizeof(double2) * V);
     A(&c->kax, sizeof(double) * V);
     A(&c->kay, sizeof(double) * V);

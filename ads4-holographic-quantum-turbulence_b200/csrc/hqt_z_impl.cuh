@@ -36,25 +36,34 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      max_smem - (int)fa.sharedSizeBytes);
     };
-    opt((const void *)k_zstage<double, double, HQT_ZN, 0>);
-    opt((const void *)k_zstage<double, double, HQT_ZN, 1>);
-    opt((const void *)k_zstage<double, double, HQT_ZN, 2>);
-    opt((const void *)k_zstage<double, double, HQT_ZN, 3>);
-    opt((const void *)k_zstage<double, double, HQT_ZN, 4>);
+    opt((const void *)k_zpsi<double, double, HQT_ZN, 0>);
+    opt((const void *)k_zpsi<double, double, HQT_ZN, 1>);
+    opt((const void *)k_zpsi<double, double, HQT_ZN, 2>);
+    opt((const void *)k_zpsi<double, double, HQT_ZN, 3>);
+    opt((const void *)k_zpsi<double, double, HQT_ZN, 4>);
     return e;
 }
 
 template <>
 cudaError_t z_stage<HQT_ZN>(int mode, const ZStageArgs<double, double> &a, const ZHost &h,
                             int grid, int threads, size_t smem, cudaStream_t s) {
+    // grid/threads/smem describe k_zpsi; k_zgauge uses the same grid and no
+    // shared memory
     const ZOps<double, HQT_ZN> op = make_zops(h);
     switch (mode) {
-        case 0: k_zstage<double, double, HQT_ZN, 0><<<grid, threads, smem, s>>>(a, op); break;
-        case 1: k_zstage<double, double, HQT_ZN, 1><<<grid, threads, smem, s>>>(a, op); break;
-        case 2: k_zstage<double, double, HQT_ZN, 2><<<grid, threads, smem, s>>>(a, op); break;
-        case 3: k_zstage<double, double, HQT_ZN, 3><<<grid, threads, smem, s>>>(a, op); break;
-        case 4: k_zstage<double, double, HQT_ZN, 4><<<grid, threads, smem, s>>>(a, op); break;
-        default: return cudaErrorInvalidValue;
+#define HQT_ZS(M)                                                                    \
+    case M:                                                                          \
+        k_zgauge<double, double, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op);         \
+        k_zpsi<double, double, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op);        \
+        break;
+        HQT_ZS(0)
+        HQT_ZS(1)
+        HQT_ZS(2)
+        HQT_ZS(3)
+        HQT_ZS(4)
+#undef HQT_ZS
+        default:
+            return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }

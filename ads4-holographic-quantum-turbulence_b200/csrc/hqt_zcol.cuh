@@ -9,7 +9,7 @@
 // columns of Lz and Lz1 are zero, so the first nz outputs are exactly those
 // of the nz-point operators.
 //
-// k_zstage fuses, per RK stage (tevol_driven_cluster.m:120-124,128):
+// k_zgauge and k_zpsi fuse, per RK stage (tevol_driven_cluster.m:120-124,128):
 //   d_z Psi, d_zz Psi, d_z A_x, d_z A_y and the two gauge contractions,
 //   the pointwise nonlinear and gauge-coupling terms of F1, F3, F4 (:72-75),
 //   the radial integration func_Lzr (:63-65) of S1, S3, S4,
@@ -64,9 +64,81 @@ __device__ __forceinline__ void rk_update_r(const TS *zsrc, TS *kacc, T *next, T
     }
 }
 
-// MODE 0: right-hand side only (F1, F3, F4, F2 boundary), MODE 1..4: RK stage.
+// The stage is split over two kernels that read the same stage input and
+// write disjoint outputs (the next stage input lives in a different buffer
+// than the current one):
+//   k_zgauge: F3, F4 and the A_x, A_y updates,
+//   k_zpsi:   F1, the Psi update and the boundary row of F2 (rhoi).
+// Contractions stream the input column: out_i += Lz[i][j] * v_j as v_j
+// arrives, so only the outputs are held in registers.
+// MODE 0: right-hand side only, MODE 1..4: RK stage.
 template <typename T, typename TS, int NZP, int MODE>
-__global__ void __launch_bounds__(64) k_zstage(ZStageArgs<T, TS> a, ZOps<T, NZP> op) {
+__global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, NZP> op) {
+    const long long site = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (site >= a.plane) return;
+    const int nz = a.nz;
+    const long long P = a.plane;
+#pragma unroll
+    for (int comp = 0; comp < 2; ++comp) {
+        const T *src = comp == 0 ? a.yax : a.yay;
+        const T *dt = comp == 0 ? a.dxat : a.dyat;
+        const C2<T> *dps = comp == 0 ? a.dxpsi : a.dypsi;
+        // g = d_{x|y} A_t + f * Lz A_{x|y}
+        T g[NZP];
+#pragma unroll
+        for (int i = 0; i < NZP; ++i) g[i] = T(0);
+#pragma unroll
+        for (int j = 0; j < NZP; ++j) {
+            if (j < nz) {
+                const T v = src[(long long)j * P + site];
+#pragma unroll
+                for (int i = 0; i < NZP; ++i) g[i] = fma(op.Lz[i][j], v, g[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NZP; ++i)
+            g[i] = (i < nz) ? dt[(long long)i * P + site] + op.fz[i] * g[i] : T(0);
+        // S = 1/2 Lz g -/+ 1/2 d_{y|x} B + Im(conj(Psi) d Psi) - A |Psi|^2
+        T s[NZP];
+#pragma unroll
+        for (int i = 0; i < NZP; ++i) {
+            if (i < nz) {
+                T d = T(0);
+#pragma unroll
+                for (int j = 0; j < NZP; ++j) d = fma(op.Lz[i][j], g[j], d);
+                const long long gi = (long long)i * P + site;
+                const C2<T> ps = a.ypsi[gi];
+                const C2<T> dd = dps[gi];
+                const T bf = comp == 0 ? -a.dyB[gi] : a.dxB[gi];
+                const T av = src[gi];
+                s[i] = T(0.5) * d + T(0.5) * bf + (ps.x * dd.y - ps.y * dd.x) -
+                       av * (ps.x * ps.x + ps.y * ps.y);
+            } else {
+                s[i] = T(0);
+            }
+        }
+        // F = Lzr(S): rows < nz-1 of Lz1, zero on the boundary row
+#pragma unroll
+        for (int i = 0; i < NZP; ++i) {
+            if (i < nz) {
+                T fr = T(0);
+#pragma unroll
+                for (int j = 0; j < NZP; ++j) fr = fma(op.Lz1[i][j], s[j], fr);
+                const long long gi = (long long)i * P + site;
+                if (MODE == 0) {
+                    (comp == 0 ? a.f3 : a.f4)[gi] = fr;
+                } else if (comp == 0) {
+                    rk_update_r<T, TS, MODE>(a.zax, a.kax, a.nax, a.wax, gi, a.h * TS(fr));
+                } else {
+                    rk_update_r<T, TS, MODE>(a.zay, a.kay, a.nay, a.way, gi, a.h * TS(fr));
+                }
+            }
+        }
+    }
+}
+
+template <typename T, typename TS, int NZP, int MODE>
+__global__ void __launch_bounds__(128, 4) k_zpsi(ZStageArgs<T, TS> a, ZOps<T, NZP> op) {
     const int bd = blockDim.x;
     const int tid = threadIdx.x;
     const long long site = (long long)blockIdx.x * bd + tid;
@@ -74,51 +146,21 @@ __global__ void __launch_bounds__(64) k_zstage(ZStageArgs<T, TS> a, ZOps<T, NZP>
     const int nz = a.nz;
     const long long P = a.plane;
     T *sm = reinterpret_cast<T *>(g_smem);
-    T *s1r = sm, *s1i = sm + NZP * bd, *s3 = sm + 2 * NZP * bd, *s4 = sm + 3 * NZP * bd;
-
-    // ---- gauge parts: S3 <- 1/2 Lz(d_x A_t + f Lz A_x), S4 likewise ----
-#pragma unroll
-    for (int comp = 0; comp < 2; ++comp) {
-        const T *src = comp == 0 ? a.yax : a.yay;
-        const T *dt = comp == 0 ? a.dxat : a.dyat;
-        T *dst = comp == 0 ? s3 : s4;
-        T v[NZP], g[NZP];
-#pragma unroll
-        for (int j = 0; j < NZP; ++j) v[j] = HQT_LD(src, j);
-#pragma unroll
-        for (int i = 0; i < NZP; ++i) {
-            T d = T(0);
-#pragma unroll
-            for (int j = 0; j < NZP; ++j) d = fma(op.Lz[i][j], v[j], d);
-            g[i] = (i < nz) ? dt[(long long)i * P + site] + op.fz[i] * d : T(0);
-        }
-#pragma unroll
-        for (int i = 0; i < NZP; ++i) {
-            T d = T(0);
-#pragma unroll
-            for (int j = 0; j < NZP; ++j) d = fma(op.Lz[i][j], g[j], d);
-            dst[i * bd + tid] = T(0.5) * d;
-        }
-    }
-
-    // ---- Psi: S1 and the pointwise parts of S3, S4 ----
+    T *s1r = sm, *s1i = sm + NZP * bd;
     T kb = T(0);
     {
         C2<T> dp[NZP];
-        {
-            C2<T> p[NZP];
 #pragma unroll
-            for (int j = 0; j < NZP; ++j)
-                p[j] = (j < nz) ? a.ypsi[(long long)j * P + site] : mk2<T>(T(0), T(0));
+        for (int i = 0; i < NZP; ++i) dp[i] = mk2<T>(T(0), T(0));
 #pragma unroll
-            for (int i = 0; i < NZP; ++i) {
-                T dr = T(0), di = T(0);
+        for (int j = 0; j < NZP; ++j) {
+            if (j < nz) {
+                const C2<T> v = a.ypsi[(long long)j * P + site];
 #pragma unroll
-                for (int j = 0; j < NZP; ++j) {
-                    dr = fma(op.Lz[i][j], p[j].x, dr);
-                    di = fma(op.Lz[i][j], p[j].y, di);
+                for (int i = 0; i < NZP; ++i) {
+                    dp[i].x = fma(op.Lz[i][j], v.x, dp[i].x);
+                    dp[i].y = fma(op.Lz[i][j], v.y, dp[i].y);
                 }
-                dp[i] = mk2<T>(dr, di);
             }
         }
 #pragma unroll
@@ -134,28 +176,23 @@ __global__ void __launch_bounds__(64) k_zstage(ZStageArgs<T, TS> a, ZOps<T, NZP>
                 const C2<T> ps = a.ypsi[g];
                 const T at = a.at[g], dat = a.dat[g], ax = a.yax[g], ay = a.yay[g];
                 const C2<T> lp = a.lap[g], dx = a.dxpsi[g], dy = a.dypsi[g];
-                const T dv = a.divA[g], dxb = a.dxB[g], dyb = a.dyB[g];
+                const T dv = a.divA[g];
                 const T z = op.zz[i], f = op.fz[i];
                 const C2<T> d1 = dp[i];
                 const T h = T(0.5);
                 const T a2 = ax * ax + ay * ay;
                 const T u = ax * dx.x + ay * dy.x;
                 const T w = ax * dx.y + ay * dy.y;
-                const T sr = -at * d1.y - h * dat * ps.y + h * f * d2r - T(1.5) * z * z * d1.x -
-                             h * z * ps.x - h * a2 * ps.x + h * lp.x + h * dv * ps.y + w;
-                const T si = at * d1.x + h * dat * ps.x + h * f * d2i - T(1.5) * z * z * d1.y -
-                             h * z * ps.y - h * a2 * ps.y + h * lp.y - h * dv * ps.x - u;
-                s1r[i * bd + tid] = sr;
-                s1i[i * bd + tid] = si;
-                const T rho2 = ps.x * ps.x + ps.y * ps.y;
-                s3[i * bd + tid] += -h * dyb + (ps.x * dx.y - ps.y * dx.x) - ax * rho2;
-                s4[i * bd + tid] += h * dxb + (ps.x * dy.y - ps.y * dy.x) - ay * rho2;
+                s1r[i * bd + tid] = -at * d1.y - h * dat * ps.y + h * f * d2r -
+                                    T(1.5) * z * z * d1.x - h * z * ps.x - h * a2 * ps.x +
+                                    h * lp.x + h * dv * ps.y + w;
+                s1i[i * bd + tid] = at * d1.x + h * dat * ps.x + h * f * d2i -
+                                    T(1.5) * z * z * d1.y - h * z * ps.y - h * a2 * ps.y +
+                                    h * lp.y - h * dv * ps.x - u;
                 kb = fma(op.lzb[i], dv, kb);
             }
         }
     }
-
-    // ---- radial integration Lzr and the RK bookkeeping ----
     {
         C2<T> s[NZP];
 #pragma unroll
@@ -172,38 +209,14 @@ __global__ void __launch_bounds__(64) k_zstage(ZStageArgs<T, TS> a, ZOps<T, NZP>
                     fi = fma(op.Lz1[i][j], s[j].y, fi);
                 }
                 const long long g = (long long)i * P + site;
-                if (MODE == 0) {
+                if (MODE == 0)
                     a.f1[g] = mk2<T>(fr, fi);
-                } else {
+                else
                     rk_update_c<T, TS, MODE>(a, g, mk2<TS>(a.h * TS(fr), a.h * TS(fi)));
-                }
             }
         }
     }
-#pragma unroll
-    for (int comp = 0; comp < 2; ++comp) {
-        const T *src = comp == 0 ? s3 : s4;
-        T s[NZP];
-#pragma unroll
-        for (int j = 0; j < NZP; ++j) s[j] = (j < nz - 1) ? src[j * bd + tid] : T(0);
-#pragma unroll
-        for (int i = 0; i < NZP; ++i) {
-            if (i < nz) {
-                T fr = T(0);
-#pragma unroll
-                for (int j = 0; j < NZP; ++j) fr = fma(op.Lz1[i][j], s[j], fr);
-                const long long g = (long long)i * P + site;
-                if (MODE == 0) {
-                    (comp == 0 ? a.f3 : a.f4)[g] = fr;
-                } else if (comp == 0) {
-                    rk_update_r<T, TS, MODE>(a.zax, a.kax, a.nax, a.wax, g, a.h * TS(fr));
-                } else {
-                    rk_update_r<T, TS, MODE>(a.zay, a.kay, a.nay, a.way, g, a.h * TS(fr));
-                }
-            }
-        }
-    }
-    // ---- F2 at the boundary slice -> rhoi ----
+    // F2 at the boundary slice -> rhoi
     if (MODE == 0) {
         a.f2b[site] = kb;
     } else {
@@ -224,7 +237,7 @@ __global__ void __launch_bounds__(64) k_zstage(ZStageArgs<T, TS> a, ZOps<T, NZP>
 // ------------------------------------------------------------------------
 
 template <typename T, int NZP>
-__global__ void __launch_bounds__(64) k_zcons(ZConsArgs<T> a, ZOps<T, NZP> op) {
+__global__ void __launch_bounds__(128, 4) k_zcons(ZConsArgs<T> a, ZOps<T, NZP> op) {
     const long long site = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (site >= a.plane) return;
     const int nz = a.nz;
@@ -310,7 +323,7 @@ __global__ void __launch_bounds__(64) k_zcons(ZConsArgs<T> a, ZOps<T, NZP> op) {
 // d_z A_t of a given potential, and the boundary order parameter of Psi.
 
 template <typename T, int NZP>
-__global__ void __launch_bounds__(64) k_zcol_misc(ZColArgs<T> a, ZOps<T, NZP> op) {
+__global__ void __launch_bounds__(128, 4) k_zcol_misc(ZColArgs<T> a, ZOps<T, NZP> op) {
     const long long site = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (site >= a.plane) return;
     const int nz = a.nz;
