@@ -81,6 +81,10 @@ def build(verbose: bool = False, ptxas: bool = False) -> Path:
             o, log = f.result()
             objs.append(o)
             logs.append(log)
+    keep = {o.name for o in objs}
+    for stale in OBJDIR.glob("*.o"):
+        if stale.name not in keep:
+            stale.unlink()
     tmp = OUT.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs),
            "-lcudart"]
