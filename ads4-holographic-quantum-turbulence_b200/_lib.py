@@ -29,6 +29,7 @@ EXPORTS = [
     "hqt_filter_device", "hqt_boundary_order_parameter_device",
     "hqt_winding_device", "hqt_count_vortices", "hqt_count_vortices_device",
     "hqt_profile", "hqt_profile_report",
+    "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
 ]
 
 
@@ -96,6 +97,9 @@ def load() -> ctypes.CDLL:
         "hqt_count_vortices_device": (c_int, [c_void_p, c_void_p, ip, ip, ip]),
         "hqt_profile": (c_int, [c_void_p, c_int]),
         "hqt_profile_report": (c_int, [c_void_p, ctypes.c_char_p, c_int64]),
+        "hqt_count_vortices_field_noalloc": (c_int, [c_void_p, c_int32, c_int32,
+                                                     c_int32, ip, ip, ip, c_void_p]),
+        "hqt_noalloc_last_error": (c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -6,6 +6,29 @@
 
 namespace hqt {
 
+void chebdif_row(int N, int i, double *row) {
+    const double pi = 3.14159265358979323846;
+    auto th = [&](int k) { return k * pi / (N - 1); };
+    // DX(i,j) = 2 sin((th_j+th_i)/2) sin((th_j-th_i)/2); rows i >= N/2 use
+    // the flipped form -DX(N-1-i, N-1-j)
+    auto dx_raw = [&](int r, int c) {
+        return 2.0 * std::sin(th(c) / 2 + th(r) / 2) * std::sin(th(c) / 2 - th(r) / 2);
+    };
+    const int n1 = N / 2;
+    double rowsum = 0.0;
+    for (int j = 0; j < N; ++j) {
+        if (j == i) continue;
+        const double dx = (i < n1) ? dx_raw(i, j) : -dx_raw(N - 1 - i, N - 1 - j);
+        double c = ((i + j) % 2 == 0) ? 1.0 : -1.0;
+        if (i == 0 || i == N - 1) c *= 2.0;
+        if (j == 0 || j == N - 1) c /= 2.0;
+        const double v = (1.0 / dx) * c;
+        row[j] = v;
+        rowsum += v;
+    }
+    row[i] = -rowsum;
+}
+
 void chebdif_host(int N, std::vector<double> &x, std::vector<double> &D) {
     x.assign(N, 0.0);
     D.assign((size_t)N * N, 0.0);

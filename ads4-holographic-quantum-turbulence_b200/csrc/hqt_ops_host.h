@@ -11,6 +11,9 @@ namespace hqt {
 // with the flipping trick, diagonal = -(row sum of the off-diagonals).
 void chebdif_host(int N, std::vector<double> &x, std::vector<double> &D);
 
+// Row i of the same D1 (N doubles), without allocating.
+void chebdif_row(int N, int i, double *row);
+
 // Inverse of an n x n row-major matrix by Gauss-Jordan elimination with
 // partial pivoting in long double.  Returns false if singular.
 bool invert_host(int n, const std::vector<double> &A, std::vector<double> &inv);

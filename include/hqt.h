@@ -139,6 +139,25 @@ int hqt_count_vortices(hqt_ctx *ctx, const double *O, int32_t *n,
 int hqt_count_vortices_device(hqt_ctx *ctx, const void *dO, int32_t *n,
                               int32_t *np, int32_t *nm);
 
+/* Allocation-free vortex count (no counterpart in the reference).
+ * countN of the boundary order parameter O = (Lz Z1)(nz) of a DEVICE field
+ * dZ1 (interleaved complex [nx,ny,nz]), computed on `cuda_stream` (NULL: the
+ * legacy default stream) of the current device without any device
+ * allocation and without a context.  It is for callers that cannot call
+ * cudaMalloc: a MEX gateway whose device memory belongs to MATLAB's gpuArray
+ * pool, a framework whose caching allocator owns a fixed device budget, or a
+ * real-time host that must not allocate after start-up.  Its scratch is a
+ * file-scope device array of nx*ny <= 1048576 points (16 MiB, held by every
+ * GPU that loads the library until exit); larger planes return HQT_EINVAL.
+ * The first call on a device looks up the scratch address, so make that first
+ * call before any stream capture.  All calls share the scratch: calls that
+ * overlap on the GPU (other streams, other host threads) race.  Errors are
+ * described by hqt_noalloc_last_error(). */
+int hqt_count_vortices_field_noalloc(const void *dZ1, int32_t nx, int32_t ny,
+                                     int32_t nz, int32_t *n, int32_t *np,
+                                     int32_t *nm, void *cuda_stream);
+const char *hqt_noalloc_last_error(void);
+
 /* Instrumentation (no counterpart in the reference, which times its loop
  * with tic/toc every 50 steps, tevol_driven_cluster.m:116,144-146).
  * hqt_profile(ctx, 1) resets the counters and makes every following launch
