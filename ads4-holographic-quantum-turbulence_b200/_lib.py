@@ -30,6 +30,7 @@ EXPORTS = [
     "hqt_winding_device", "hqt_count_vortices", "hqt_count_vortices_device",
     "hqt_profile", "hqt_profile_report",
     "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
+    "hqt_energy_spectrum_device",
 ]
 
 
@@ -100,6 +101,8 @@ def load() -> ctypes.CDLL:
         "hqt_count_vortices_field_noalloc": (c_int, [c_void_p, c_int32, c_int32,
                                                      c_int32, ip, ip, ip, c_void_p]),
         "hqt_noalloc_last_error": (c_char_p, []),
+        "hqt_energy_spectrum_device": (c_int, [c_void_p, c_void_p, c_int32, dp, dp, dp,
+                                               dp, ip]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -253,6 +253,19 @@ class Simulation:
         self._check(self._lib.hqt_winding_device(self._ctx, p, ctypes.byref(w)))
         return int(w.value)
 
+    def energy_spectrum_device(self, O):
+        """``(k, E, E_c, E_i)`` of the boundary superflow of a ``(ny, nx)``
+        complex CUDA tensor ``O`` (``scripts/analysis/movie_show.m:140-276``)."""
+        cap = self.nx + self.ny + 4
+        k, E, Ec, Ei = (np.zeros(cap) for _ in range(4))
+        nb = ctypes.c_int32()
+        p = self._dev2(O, True)
+        self._sync_stream()
+        self._check(self._lib.hqt_energy_spectrum_device(
+            self._ctx, p, cap, _dptr(k), _dptr(E), _dptr(Ec), _dptr(Ei), ctypes.byref(nb)))
+        n = nb.value
+        return k[:n].copy(), E[:n].copy(), Ec[:n].copy(), Ei[:n].copy()
+
     def count_vortices(self, O) -> tuple[int, int, int]:
         """``countN`` of a host ``(nx, ny)`` complex field."""
         O = np.asarray(O)

@@ -65,6 +65,8 @@ struct hqt_ctx {
     double *dxat = nullptr, *dyat = nullptr, *dat = nullptr, *dxax = nullptr;
     double2 *O = nullptr;
     double *partial = nullptr;
+    double *kxv = nullptr, *kyv = nullptr, *bins = nullptr;  // spectrum scratch
+    int max_bins = 0;
     int *d_int = nullptr;  // scratch ints (winding, counts)
     DevStatus *st = nullptr;
     // launch geometry
@@ -269,12 +271,12 @@ int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     return HQT_OK;
 }
 
-int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out) {
+int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out, int nslices = 0) {
     XD1Args<double> a{};
     a.plan = c->planx;
     a.roots = c->rootsx;
     a.NB = c->NBx_2;
-    a.nlines = c->ny * c->nz;
+    a.nlines = c->ny * (nslices > 0 ? nslices : c->nz);
     a.s1 = 2.0 * 3.14159265358979323846 / c->p.Lx / c->nx;
     a.in = in;
     a.out = out;
@@ -289,7 +291,9 @@ int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out) {
     return HQT_OK;
 }
 
-int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<double> out) {
+int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<double> out,
+                int nslices = 0) {
+    const int nsl = nslices > 0 ? nslices : c->nz;
     YD1Args<double> a{};
     a.plan = c->plany;
     a.roots = c->rootsy;
@@ -300,11 +304,11 @@ int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<d
     a.in = in;
     a.add_re = add_re;
     a.out = out;
-    dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
+    dim3 grid((c->nx + a.TX - 1) / a.TX, nsl);
     Prof pr(c, K_Y_D1);
     if (c->cy) {
         const int nb = ct_lines(c->ny, 2);
-        RC(ct_dispatch(c, c->ny, CT_Y_D1, &a, dim3((c->nx + nb - 1) / nb, c->nz),
+        RC(ct_dispatch(c, c->ny, CT_Y_D1, &a, dim3((c->nx + nb - 1) / nb, nsl),
                        smem_x(c->ny, 2, nb)));
         return HQT_OK;
     }
@@ -667,6 +671,94 @@ void use_internal_state(hqt_ctx *c) {
     c->cay = c->ay;
 }
 
+// signed integer wavenumbers of an n-point transform (even n: [0:n/2-1, -n/2:-1])
+void signed_k(int n, double scale, std::vector<double> &k) {
+    k.resize(n);
+    for (int i = 0; i < n; ++i) {
+        int m;
+        if (n % 2 == 0)
+            m = (i < n / 2) ? i : i - n;
+        else
+            m = (i <= (n - 1) / 2) ? i : i - n;
+        k[i] = scale * (double)m;
+    }
+}
+
+int energy_spectrum(hqt_ctx *c, const double2 *O, int capacity, double *kout, double *E,
+                    double *Ec, double *Ei, int32_t *nbins_out) {
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    std::vector<double> kx, ky;
+    signed_k(c->nx, two_pi / c->p.Lx, kx);
+    signed_k(c->ny, two_pi / c->p.Ly, ky);
+    double kmax2 = 0.0;
+    for (double a : kx)
+        for (double b : ky) kmax2 = std::max(kmax2, a * a + b * b);
+    const double dk = two_pi / c->p.Lx;
+    const double kmax = std::floor(std::sqrt(kmax2));
+    const int nbins = (int)std::floor(kmax / dk);
+    *nbins_out = nbins;
+    if (nbins > c->max_bins) return fail(c, HQT_EUNSUPPORTED, "too many spectrum bins");
+    if (capacity < nbins) return fail(c, HQT_EINVAL, "spectrum capacity too small");
+    const long long P = c->plane;
+    double2 *dOx = c->dxxpsi, *dOy = c->dypsi, *U = c->E, *S = c->dxpsi;
+    RC(launch_x_d1(c, FieldIn<double>{O, nullptr, nullptr}, FieldOut<double>{dOx, nullptr, nullptr}, 1));
+    RC(launch_y_d1(c, FieldIn<double>{O, nullptr, nullptr}, nullptr,
+                   FieldOut<double>{dOy, nullptr, nullptr}, 1));
+    k_spec_absmax<<<kPartials, kRedThreads, 0, c->stream>>>(O, P, c->partial);
+    CK(cudaGetLastError());
+    k_spec_velocity<<<kPartials, 256, 0, c->stream>>>(O, dOx, dOy, P, c->partial, kPartials, U);
+    CK(cudaGetLastError());
+    {
+        XFiltFwdArgs<double> a{};
+        a.plan = c->planx;
+        a.roots = c->rootsx;
+        a.NB = c->NBx_2;
+        a.nlines = c->ny;
+        a.ny = c->ny;
+        a.nf = 1;
+        a.in[0] = FieldIn<double>{U, nullptr, nullptr};
+        a.spec[0] = S;
+        a.st = nullptr;
+        if (c->cx) {
+            const int nb = ct_lines(c->nx, 2);
+            RC(ct_dispatch(c, c->nx, CT_FX_FWD, &a, dim3((c->ny + nb - 1) / nb), smem_x(c->nx, 2, nb)));
+        } else {
+            CK(launch_x_filt_fwd(a, (c->ny + a.NB - 1) / a.NB, smem_x(c->nx, 2, a.NB), c->stream));
+        }
+    }
+    {
+        YFiltArgs<double> a{};
+        a.plan = c->plany;
+        a.roots = c->rootsy;
+        a.TX = c->TXy_2;
+        a.nx = c->nx;
+        a.ny = c->ny;
+        a.nf = 1;
+        a.spec[0] = S;
+        CK(launch_y_fwd(a, dim3((c->nx + a.TX - 1) / a.TX, 1), smem_x(c->ny, 2, a.TX), c->stream));
+    }
+    CK(cudaMemcpyAsync(c->kxv, kx.data(), sizeof(double) * c->nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->kyv, ky.data(), sizeof(double) * c->ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->bins, 0, sizeof(double) * 3 * nbins, c->stream));
+    if (nbins > 0) {
+        k_spec_bins<<<kPartials, 256, 0, c->stream>>>(S, c->nx, c->ny, c->kxv, c->kyv, dk, nbins,
+                                                      c->bins);
+        CK(cudaGetLastError());
+    }
+    std::vector<double> h(3 * (size_t)nbins);
+    if (nbins > 0)
+        CK(cudaMemcpyAsync(h.data(), c->bins, sizeof(double) * 3 * nbins, cudaMemcpyDeviceToHost,
+                           c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < nbins; ++b) {
+        if (kout) kout[b] = (b + 0.5) * dk;
+        if (E) E[b] = h[b];
+        if (Ec) Ec[b] = h[nbins + b];
+        if (Ei) Ei[b] = h[2 * nbins + b];
+    }
+    return HQT_OK;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -792,6 +884,10 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->dxax, sizeof(double) * V);
     A(&c->O, sizeof(double2) * P2);
     A(&c->partial, sizeof(double) * kPartials);
+    c->max_bins = p.nx + p.ny + 4;
+    A(&c->kxv, sizeof(double) * p.nx);
+    A(&c->kyv, sizeof(double) * p.ny);
+    A(&c->bins, sizeof(double) * 3 * c->max_bins);
     A(&c->d_int, sizeof(int) * 8);
     A(&c->st, sizeof(DevStatus));
     if (rc != HQT_OK) return bail(rc);
@@ -1094,6 +1190,14 @@ int hqt_count_vortices_device(hqt_ctx *c, const void *dO, int32_t *n, int32_t *n
     if (!dO) return fail(c, HQT_EINVAL, "bad argument");
     DeviceGuard guard(c->device);
     return count_vortices_dev(c, (const double2 *)dO, n, np, nm);
+}
+
+int hqt_energy_spectrum_device(hqt_ctx *c, const void *dO, int32_t capacity, double *k,
+                               double *E, double *Ec, double *Ei, int32_t *nbins) {
+    if (!c) return HQT_EINVAL;
+    if (!dO || !nbins || capacity < 0) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    return energy_spectrum(c, (const double2 *)dO, capacity, k, E, Ec, Ei, nbins);
 }
 
 int hqt_count_vortices(hqt_ctx *c, const double *O, int32_t *n, int32_t *np, int32_t *nm) {

@@ -139,4 +139,76 @@ __global__ void k_step_end(DevStatus *st) {
     if (threadIdx.x == 0 && blockIdx.x == 0) st->step += 1;
 }
 
+// ---- energy spectrum of the boundary superflow --------------------------
+// partial[b] = max |O| over block b
+__global__ void __launch_bounds__(kRedThreads)
+    k_spec_absmax(const double2 *O, long long n, double *partial) {
+    __shared__ double sh[kRedThreads];
+    double m = 0.0;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, hypot(O[s].x, O[s].y));
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// U = ux + i uy with u = |O|/max|O| * Im(dO/O)  (= Re(-i(dO - d|O| O/|O|)/O))
+__global__ void k_spec_velocity(const double2 *O, const double2 *dOx, const double2 *dOy,
+                                long long n, const double *partial, int nparts, double2 *U) {
+    __shared__ double amax;
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int i = 0; i < nparts; ++i) m = fmax(m, partial[i]);
+        amax = m;
+    }
+    __syncthreads();
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const double2 o = O[s], a = dOx[s], b = dOy[s];
+        const double r2 = o.x * o.x + o.y * o.y;
+        const double w = sqrt(r2) / amax;
+        // Im(d/O) = Im(d conj(O)) / |O|^2
+        const double ux = w * (a.y * o.x - a.x * o.y) / r2;
+        const double uy = w * (b.y * o.x - b.x * o.y) / r2;
+        U[s] = make_double2(ux, uy);
+    }
+}
+
+// shell sums of E, E_c, E_i from the 2-D spectrum Uh of ux + i uy
+__global__ void k_spec_bins(const double2 *Uh, int nx, int ny, const double *kx,
+                            const double *ky, double dk, int nbins, double *bins) {
+    const long long n = (long long)nx * ny;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % nx), j = (int)(s / nx);
+        if (i == 0 && j == 0) continue;  // mean removed
+        const int im = (nx - i) % nx, jm = (ny - j) % ny;
+        const double2 c = Uh[s], p = Uh[(long long)jm * nx + im];
+        // ux^ = (c + conj p)/2, uy^ = (c - conj p)/(2i)
+        const double2 ux = make_double2(0.5 * (c.x + p.x), 0.5 * (c.y - p.y));
+        const double2 uy = make_double2(0.5 * (c.y + p.y), -0.5 * (c.x - p.x));
+        const double k1 = kx[i], k2 = ky[j];
+        const double K2 = __dadd_rn(__dmul_rn(k1, k1), __dmul_rn(k2, k2));
+        const double K = sqrt(K2);
+        const long long b = (long long)floor(K / dk);
+        if (b >= nbins) continue;
+        const double2 kd = make_double2(k1 * ux.x + k2 * uy.x, k1 * ux.y + k2 * uy.y);
+        const double2 sc = K2 > 0 ? make_double2(kd.x / K2, kd.y / K2) : make_double2(0, 0);
+        const double2 cx = make_double2(k1 * sc.x, k1 * sc.y), cy = make_double2(k2 * sc.x, k2 * sc.y);
+        const double2 ix = make_double2(ux.x - cx.x, ux.y - cx.y);
+        const double2 iy = make_double2(uy.x - cy.x, uy.y - cy.y);
+        const double e = 0.5 * (ux.x * ux.x + ux.y * ux.y + uy.x * uy.x + uy.y * uy.y);
+        const double ec = 0.5 * (cx.x * cx.x + cx.y * cx.y + cy.x * cy.x + cy.y * cy.y);
+        const double ei = 0.5 * (ix.x * ix.x + ix.y * ix.y + iy.x * iy.x + iy.y * iy.y);
+        atomicAdd(&bins[b], e);
+        atomicAdd(&bins[nbins + b], ec);
+        atomicAdd(&bins[2 * nbins + b], ei);
+    }
+}
+
 }  // namespace hqt

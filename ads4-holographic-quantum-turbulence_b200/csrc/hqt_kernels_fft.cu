@@ -28,6 +28,7 @@ cudaError_t fft_init(const double *tc, const double *ts, int ntab, int max_smem)
     opt((const void *)k_x_filt_fwd<double>);
     opt((const void *)k_y_filt<double>);
     opt((const void *)k_x_filt_inv<double>);
+    opt((const void *)k_y_fwd<double>);
     return e;
 }
 
@@ -60,6 +61,11 @@ cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cu
 cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s) {
     k_x_filt_inv<double><<<grid, 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_y_fwd(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
+    k_y_fwd<double><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
 }
 

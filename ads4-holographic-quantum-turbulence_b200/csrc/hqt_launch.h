@@ -24,6 +24,7 @@ cudaError_t launch_x_filt_fwd(const XFiltFwdArgs<double> &a, int grid, size_t sm
 cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s);
 cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s);
+cudaError_t launch_y_fwd(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s);
 
 // Compile-time line lengths (hqt_c<N>.cu): kinds of pass kernel.
 enum CtKind { CT_X_RHS, CT_Y_RHS, CT_X_D1, CT_Y_D1, CT_FX_FWD, CT_FY, CT_FX_INV };

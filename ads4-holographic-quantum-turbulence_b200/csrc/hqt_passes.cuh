@@ -402,4 +402,22 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_inv(XFiltInvArgs<T
     }
 }
 
+// forward transform along y of nf complex fields (used by the spectrum)
+template <typename T> __global__ void HQT_FFT_BOUNDS k_y_fwd(YFiltArgs<T> a) {
+    const int n = a.ny;
+    const int x0 = blockIdx.x * a.TX;
+    const int nb = min(a.TX, a.nx - x0);
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    const int R = 0, A = n, B = n + a.TX * n;
+    load_roots<T>(R, a.roots, n);
+    for (int f = 0; f < a.nf; ++f) {
+        C2<T> *spec = a.spec[f];
+        yl_load<T>(A, n, nb, a.nx, zoff, [&](long long g) { return spec[g]; });
+        __syncthreads();
+        const int X = fft_run<T>(A, B, R, a.plan, nb, -1);
+        yl_store<T>(X, n, nb, a.nx, zoff, [&](long long g, C2<T> v) { spec[g] = v; });
+        __syncthreads();
+    }
+}
+
 }  // namespace hqt

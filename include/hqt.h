@@ -139,6 +139,19 @@ int hqt_count_vortices(hqt_ctx *ctx, const double *O, int32_t *n,
 int hqt_count_vortices_device(hqt_ctx *ctx, const void *dO, int32_t *n,
                               int32_t *np, int32_t *nm);
 
+/* Kinetic-energy spectrum of the boundary superflow of a device O
+ * (interleaved complex [nx,ny]), after scripts/analysis/movie_show.m:93-94,
+ * 140-162,217-276: u = |O|/max|O| * Re(-i(dO - d|O| O/|O|)/O) with spectral
+ * derivatives, mean removed, E2d = |u^|^2/2 summed over shells
+ * kbins = 0:dk:kmax (dk = 2*pi/Lx, kmax = floor(max|k|)), and the Helmholtz
+ * split u_c^ = k(k.u^)/|k|^2, u_i^ = u^ - u_c^.  Wavenumbers are the n-point
+ * signed integers for odd and even n (the reference's grid has n-1 entries
+ * for odd n).  Writes *nbins bin centres and E, E_c, E_i (host arrays of
+ * `capacity` doubles; NULL skips an output).  HQT_EINVAL if capacity < *nbins. */
+int hqt_energy_spectrum_device(hqt_ctx *ctx, const void *dO, int32_t capacity,
+                               double *k, double *E, double *Ec, double *Ei,
+                               int32_t *nbins);
+
 /* Allocation-free vortex count (no counterpart in the reference).
  * countN of the boundary order parameter O = (Lz Z1)(nz) of a DEVICE field
  * dZ1 (interleaved complex [nx,ny,nz]), computed on `cuda_stream` (NULL: the

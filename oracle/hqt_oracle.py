@@ -395,3 +395,78 @@ def run(op: Operators, s: OracleState, nsteps: int, h: float, mu: float,
                 or np.isnan(s.Z3).any() or np.isnan(s.Z4).any()):
             break
     return s, windings
+
+
+# ---------------------------------------------------------------------------
+# Energy spectrum of the boundary superflow
+# ---------------------------------------------------------------------------
+def signed_wavenumbers(n: int) -> np.ndarray:
+    """Integer wavenumbers of an n-point FFT: ``[0:n/2-1, -n/2:-1]`` for even
+    n (as ``scripts/analysis/movie_show.m:148-149`` builds them) and
+    ``[0:(n-1)/2, -(n-1)/2:-1]`` for odd n.  The reference's expression yields
+    n-1 entries for odd n (300 for n=301) and mis-shapes its shell mask; this
+    restatement uses the n-point grid for both parities."""
+    if n % 2 == 0:
+        return np.r_[np.arange(0, n // 2), np.arange(-n // 2, 0)].astype(np.float64)
+    h = (n - 1) // 2
+    return np.r_[np.arange(0, h + 1), np.arange(-h, 0)].astype(np.float64)
+
+
+def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
+    """Incompressible/compressible kinetic-energy spectrum of the boundary flow.
+
+    Restates ``scripts/analysis/movie_show.m``: the density-weighted velocity
+    ``u = |O|/max|O| * Re(-i(dO - d|O| O/|O|)/O)`` (:93-94, with spectral
+    derivatives), the mean removed (:140-141), ``E2d = |u^|^2/2`` (:142-145),
+    shell sums ``sum(E2d(K >= kbins(i) & K < kbins(i+1)))`` over
+    ``kbins = 0:dk:kmax``, ``dk = 2*pi/L0``, ``kmax = floor(max K)`` (:146-160),
+    and the Helmholtz split ``u_c = grad Phi``, ``lap Phi = div u`` (:217-233)
+    done in Fourier space as ``u_c^ = k (k.u^)/|k|^2``.  Returns
+    ``(kplot, E, E_c, E_i)``.
+    """
+    O = np.asarray(O, dtype=np.complex128)
+    nx, ny = O.shape
+    kx = (2.0 * np.pi / Lx) * signed_wavenumbers(nx)
+    ky = (2.0 * np.pi / Ly) * signed_wavenumbers(ny)
+    # spectral derivatives (func_Lx / func_Ly on the boundary slice)
+    ikx = 1j * kx
+    iky = 1j * ky
+    if nx % 2 == 0:
+        ikx[nx // 2] = 0
+    if ny % 2 == 0:
+        iky[ny // 2] = 0
+    Ohat = np.fft.fft2(O)
+    dOx = np.fft.ifft2(ikx[:, None] * Ohat)
+    dOy = np.fft.ifft2(iky[None, :] * Ohat)
+    a = np.abs(O)
+    ahat = np.fft.fft2(a)
+    dax = np.real(np.fft.ifft2(ikx[:, None] * ahat))
+    day = np.real(np.fft.ifft2(iky[None, :] * ahat))
+    w = a / np.max(a)
+    ux = w * np.real(-1j * (dOx - dax * O / a) / O)
+    uy = w * np.real(-1j * (dOy - day * O / a) / O)
+    ux = ux - np.mean(ux)
+    uy = uy - np.mean(uy)
+    uxh = np.fft.fft2(ux)
+    uyh = np.fft.fft2(uy)
+    KX, KY = np.meshgrid(kx, ky, indexing="ij")
+    K2 = KX * KX + KY * KY
+    K = np.sqrt(K2)
+    kdotu = KX * uxh + KY * uyh
+    with np.errstate(invalid="ignore", divide="ignore"):
+        s = np.where(K2 > 0, kdotu / np.where(K2 > 0, K2, 1.0), 0.0)
+    ucx, ucy = KX * s, KY * s
+    uix, uiy = uxh - ucx, uyh - ucy
+    E2d = 0.5 * (np.abs(uxh) ** 2 + np.abs(uyh) ** 2)
+    E2c = 0.5 * (np.abs(ucx) ** 2 + np.abs(ucy) ** 2)
+    E2i = 0.5 * (np.abs(uix) ** 2 + np.abs(uiy) ** 2)
+    dk = 2.0 * np.pi / Lx
+    kmax = np.floor(np.max(K))
+    nbins = int(np.floor(kmax / dk))       # len(0:dk:kmax) - 1
+    idx = np.floor(K / dk).astype(np.int64)
+    sel = idx < nbins
+    E = np.bincount(idx[sel], weights=E2d[sel], minlength=nbins)[:nbins]
+    Ec = np.bincount(idx[sel], weights=E2c[sel], minlength=nbins)[:nbins]
+    Ei = np.bincount(idx[sel], weights=E2i[sel], minlength=nbins)[:nbins]
+    kplot = (np.arange(nbins) + 0.5) * dk
+    return kplot, E, Ec, Ei

@@ -251,3 +251,20 @@ def test_runtime_line_engine_parity(hqt, oracle, dev, monkeypatch, nx, ny, nz):
     assert relmax(from_d(g4), F4) < 1e-11
     assert relmax(g2b.cpu().numpy().T, F2[:, :, -1]) < 1e-11
     assert relmax(from_d(y[0]), oracle.ff(Z3, op.mask)) < 1e-12
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 64, 9), (301, 301, 9), (53, 48, 8)])
+def test_energy_spectrum_parity(hqt, oracle, dev, nx, ny, nz):
+    to_d, from_d = dev
+    Lx, Ly = 0.4 * nx, 0.4 * ny
+    Z1 = vortex_field(nx, ny, nz, 4, seed=nx)
+    op = oracle.build_operators(nx, ny, nz, Lx, Ly)
+    O = oracle.boundary_order_parameter(op, Z1)
+    k, E, Ec, Ei = oracle.energy_spectrum(O, Lx, Ly)
+    with hqt.Simulation(nx, ny, nz, Lx=Lx, Ly=Ly) as sim:
+        gk, gE, gEc, gEi = sim.energy_spectrum_device(to_d(O[:, :, None])[0])
+    assert len(gk) == len(k)
+    assert np.allclose(gk, k, rtol=1e-14)
+    scale = E.max()
+    for got, want in ((gE, E), (gEc, Ec), (gEi, Ei)):
+        assert np.max(np.abs(got - want)) < 1e-9 * scale

@@ -83,3 +83,22 @@ def test_rk4_step_finite_smoke_size(oracle, hqt):
         assert np.all(np.isfinite(f))
     assert np.all(s.Z1[:, :, -1] == 0)
     assert np.max(np.abs(s.Z2[:, :, -1] - 6.0)) < 1e-12
+
+
+def test_energy_spectrum_helmholtz_split(oracle):
+    # E = E_c + E_i (the split is orthogonal mode by mode); a single vortex
+    # dipole carries mostly incompressible energy
+    n = 48
+    g = np.arange(n) * 2 * np.pi / n
+    x, y = np.meshgrid(g, g, indexing="ij")
+    O = np.tanh(np.hypot(np.sin((x - 2) / 2), np.sin((y - 3) / 2)) * 6) * 0 + 1.0
+    O = O * (np.sin(x - 2.0) + 1j * np.sin(y - 3.0) + 0.3)
+    k, E, Ec, Ei = oracle.energy_spectrum(O, 2 * np.pi, 2 * np.pi)
+    assert len(k) > 10 and np.all(E >= 0) and np.all(Ec >= 0) and np.all(Ei >= 0)
+    assert np.allclose(E, Ec + Ei, rtol=1e-12, atol=1e-12 * E.max())
+    assert Ei.sum() > Ec.sum()
+
+
+def test_signed_wavenumbers(oracle):
+    assert list(oracle.signed_wavenumbers(4)) == [0, 1, -2, -1]
+    assert list(oracle.signed_wavenumbers(5)) == [0, 1, 2, -2, -1]
