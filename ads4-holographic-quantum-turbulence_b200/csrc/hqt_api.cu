@@ -48,6 +48,7 @@ struct hqt_ctx {
     long long plane = 0, vol = 0;
     FFTPlan planx{}, plany{};
     double2 *rootsx = nullptr, *rootsy = nullptr;
+    float2 *rootsx32 = nullptr, *rootsy32 = nullptr;
     double *mx = nullptr, *my = nullptr;
     // operators (host copies, nz x nz row-major)
     std::vector<double> Lz, Lz1, zz;
@@ -63,6 +64,17 @@ struct hqt_ctx {
     double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr;
     double *dxxay = nullptr, *divA = nullptr, *dxB = nullptr, *dyB = nullptr;
     double *dxat = nullptr, *dyat = nullptr, *dat = nullptr, *dxax = nullptr;
+    // mixed precision: FP32 stage inputs ([0], [1]; [2] = copy of the state)
+    // and FP32 derivative fields of the line passes
+    bool mixed = false;
+    float2 *ypsi32[3] = {nullptr, nullptr, nullptr};
+    float *yax32[3] = {nullptr, nullptr, nullptr}, *yay32[3] = {nullptr, nullptr, nullptr};
+    float *at32 = nullptr;
+    float2 *dxpsi32 = nullptr, *lap32 = nullptr, *E32 = nullptr, *dypsi32 = nullptr;
+    float *dxxay32 = nullptr, *divA32 = nullptr, *dxB32 = nullptr, *dyB32 = nullptr;
+    float *dxat32 = nullptr, *dyat32 = nullptr;
+    double *f2x = nullptr, *f2y = nullptr, *f2 = nullptr;  // 2-D boundary terms
+    double *slice_mean = nullptr;                           // 5 per z-slice
     double2 *O = nullptr;
     double *partial = nullptr;
     double *kxv = nullptr, *kyv = nullptr, *bins = nullptr;  // spectrum scratch
@@ -133,12 +145,12 @@ int fail(hqt_ctx *c, int code, const std::string &msg) {
 // kernel kinds reported by hqt_profile_report
 enum Kind {
     K_X_RHS, K_Y_RHS, K_ZSTAGE, K_X_D1, K_Y_D1, K_ZCONS, K_ZMISC, K_WIND, K_FILT_X_FWD,
-    K_FILT_Y, K_FILT_X_INV, K_PHASE, K_STEP_END, K_COUNT, K_RHO, K_NKINDS
+    K_FILT_Y, K_FILT_X_INV, K_PHASE, K_STEP_END, K_COUNT, K_RHO, K_CONVERT, K_NKINDS
 };
 const char *const kKindName[K_NKINDS] = {
     "x_rhs", "y_rhs", "zstage", "x_d1", "y_d1", "zcons", "zcol_misc", "winding",
     "filter_x_fwd", "filter_y", "filter_x_inv", "phase_multiply", "step_end",
-    "count_vortices", "rho_gather_scatter"};
+    "count_vortices", "rho_gather_scatter", "state_to_f32"};
 
 struct Prof {
     hqt_ctx *c;
@@ -197,7 +209,9 @@ template <typename P> int dalloc(hqt_ctx *c, P **ptr, size_t bytes) {
     return HQT_OK;
 }
 
-size_t smem_x(int n, int nbuf, int NB) { return sizeof(double2) * (size_t)n * (1 + (size_t)nbuf * NB); }
+size_t smem_x(int n, int nbuf, int NB, size_t esize = sizeof(double2)) {
+    return esize * (size_t)n * (1 + (size_t)nbuf * NB);
+}
 
 int pick_lines(int n, int nbuf, int cap) {
     int NB = (int)((kSmemBudget / sizeof(double2) / (size_t)n - 1) / nbuf);
@@ -316,6 +330,112 @@ int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<d
     return HQT_OK;
 }
 
+// ---- FP32 stage passes (mixed precision) ----
+int launch_x_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *ay) {
+    XRhsArgs<float> a{};
+    a.plan = c->planx;
+    a.roots = nullptr;
+    a.NB = c->NBx_rhs;
+    a.nlines = c->ny * c->nz;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    a.s1 = (float)(two_pi / c->p.Lx / c->nx);
+    a.s2 = (float)(-(two_pi / c->p.Lx) * (two_pi / c->p.Lx) / c->nx);
+    a.roots = reinterpret_cast<const float2 *>(c->rootsx32);
+    a.psi = psi;
+    a.ax = ax;
+    a.ay = ay;
+    a.dxpsi = c->dxpsi32;
+    a.dxxpsi = c->lap32;
+    a.E = c->E32;
+    a.dxxay = c->dxxay32;
+    Prof pr(c, K_X_RHS);
+    if (c->cx) {
+        const int nb = ct_lines(c->nx, 3, sizeof(float2));
+        RC(ct_dispatch(c, c->nx, CT_X_RHS_F, &a, dim3((a.nlines + nb - 1) / nb),
+                       smem_x(c->nx, 3, nb, sizeof(float2))));
+        return HQT_OK;
+    }
+    CK(launch_x_rhs_f(a, (a.nlines + a.NB - 1) / a.NB, smem_x(c->nx, 3, a.NB, sizeof(float2)),
+                      c->stream));
+    return HQT_OK;
+}
+
+int launch_y_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *ay) {
+    YRhsArgs<float> a{};
+    a.plan = c->plany;
+    a.roots = reinterpret_cast<const float2 *>(c->rootsy32);
+    a.TX = c->TXy_rhs;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    a.s1 = (float)(two_pi / c->p.Ly / c->ny);
+    a.s2 = (float)(-(two_pi / c->p.Ly) * (two_pi / c->p.Ly) / c->ny);
+    a.psi = psi;
+    a.ax = ax;
+    a.ay = ay;
+    a.E = c->E32;
+    a.dxxpsi = c->lap32;
+    a.dxxay = c->dxxay32;
+    a.dypsi = c->dypsi32;
+    a.lap = c->lap32;
+    a.divA = c->divA32;
+    a.dxB = c->dxB32;
+    a.dyB = c->dyB32;
+    Prof pr(c, K_Y_RHS);
+    if (c->cy) {
+        const int nb = ct_lines(c->ny, 3, sizeof(float2));
+        RC(ct_dispatch(c, c->ny, CT_Y_RHS_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),
+                       smem_x(c->ny, 3, nb, sizeof(float2))));
+        return HQT_OK;
+    }
+    CK(launch_y_rhs_f(a, dim3((c->nx + a.TX - 1) / a.TX, c->nz),
+                      smem_x(c->ny, 4, a.TX, sizeof(float2)), c->stream));
+    return HQT_OK;
+}
+
+int launch_d1_32(hqt_ctx *c, bool along_x, const float *in, float *out) {
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    if (along_x) {
+        XD1Args<float> a{};
+        a.plan = c->planx;
+        a.roots = reinterpret_cast<const float2 *>(c->rootsx32);
+        a.NB = c->NBx_2;
+        a.nlines = c->ny * c->nz;
+        a.s1 = (float)(two_pi / c->p.Lx / c->nx);
+        a.in = FieldIn<float>{nullptr, in, nullptr};
+        a.out = FieldOut<float>{nullptr, out, nullptr};
+        Prof pr(c, K_X_D1);
+        if (c->cx) {
+            const int nb = ct_lines(c->nx, 2, sizeof(float2));
+            RC(ct_dispatch(c, c->nx, CT_X_D1_F, &a, dim3((a.nlines + nb - 1) / nb),
+                           smem_x(c->nx, 2, nb, sizeof(float2))));
+            return HQT_OK;
+        }
+        CK(launch_x_d1_f(a, (a.nlines + a.NB - 1) / a.NB, smem_x(c->nx, 2, a.NB, sizeof(float2)),
+                         c->stream));
+        return HQT_OK;
+    }
+    YD1Args<float> a{};
+    a.plan = c->plany;
+    a.roots = reinterpret_cast<const float2 *>(c->rootsy32);
+    a.TX = c->TXy_2;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.s1 = (float)(two_pi / c->p.Ly / c->ny);
+    a.in = FieldIn<float>{nullptr, in, nullptr};
+    a.out = FieldOut<float>{nullptr, out, nullptr};
+    Prof pr(c, K_Y_D1);
+    if (c->cy) {
+        const int nb = ct_lines(c->ny, 2, sizeof(float2));
+        RC(ct_dispatch(c, c->ny, CT_Y_D1_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),
+                       smem_x(c->ny, 2, nb, sizeof(float2))));
+        return HQT_OK;
+    }
+    CK(launch_y_d1_f(a, dim3((c->nx + a.TX - 1) / a.TX, c->nz),
+                     smem_x(c->ny, 2, a.TX, sizeof(float2)), c->stream));
+    return HQT_OK;
+}
+
 // Filter nf (<= 3) complex fields in place through the x-spectra buffers.
 int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<double> *out,
                   bool phase, bool check) {
@@ -405,6 +525,21 @@ template <int MODE> int launch_zstage(hqt_ctx *c, const ZStageArgs<double, doubl
     return fail(c, HQT_EUNSUPPORTED, "unsupported nz");
 }
 
+int launch_zstage_mixed(hqt_ctx *c, int mode, const ZStageArgs<double, double, float> &a) {
+    const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
+    const ZHost h = zhost(c);
+    Prof pr(c, K_ZSTAGE, 2);
+    switch (c->NZP) {
+#define HQT_Z(N)                                                                       \
+    case N:                                                                            \
+        CK(z_stage_mixed<N>(mode, a, h, grid, kThreadsZ, smem_z(N), c->stream));       \
+        return HQT_OK;
+        HQT_NZP_LIST(HQT_Z)
+#undef HQT_Z
+    }
+    return fail(c, HQT_EUNSUPPORTED, "unsupported nz");
+}
+
 int launch_zcons(hqt_ctx *c) {
     ZConsArgs<double> a{};
     a.nz = c->nz;
@@ -464,9 +599,93 @@ int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
 
 
 // ---------------------------------------------------------------- one step
+// The four stages in mixed precision: the line passes run in FP32 on FP32
+// copies of the stage input; the column kernels contract in FP64 on the FP64
+// stage input (D_z^2 would amplify FP32 storage error by ~|Lz^2|) and keep
+// the state and RK accumulators in FP64.
+int enqueue_stages_mixed(hqt_ctx *c) {
+    double2 *psi = c->cpsi;
+    double *at = c->cat, *ax = c->cax, *ay = c->cay;
+    {
+        Prof pr(c, K_CONVERT, 2);
+        k_slice_means<<<c->nz, kRedThreads, 0, c->stream>>>(psi, at, ax, ay, c->plane,
+                                                            c->slice_mean);
+        CK(cudaGetLastError());
+        k_state_to_f32<<<592, 256, 0, c->stream>>>(psi, at, ax, ay, c->plane, c->vol,
+                                                  c->slice_mean, c->ypsi32[2], c->at32,
+                                                  c->yax32[2], c->yay32[2]);
+        CK(cudaGetLastError());
+    }
+    RC(launch_d1_32(c, true, c->at32, c->dxat32));
+    RC(launch_d1_32(c, false, c->at32, c->dyat32));
+    for (int s = 1; s <= 4; ++s) {
+        const int yi = (s == 3) ? 1 : 0, ni = (s == 2) ? 1 : 0;
+        const int y32 = (s == 1) ? 2 : yi;
+        const double2 *ypsi = (s == 1) ? psi : c->ypsi2[yi];
+        const double *yax = (s == 1) ? ax : c->yax2[yi];
+        const double *yay = (s == 1) ? ay : c->yay2[yi];
+        RC(launch_x_rhs32(c, c->ypsi32[y32], c->yax32[y32], c->yay32[y32]));
+        RC(launch_y_rhs32(c, c->ypsi32[y32], c->yax32[y32], c->yay32[y32]));
+        ZStageArgs<double, double, float> a{};
+        a.nz = c->nz;
+        a.plane = c->plane;
+        a.h = c->p.dt;
+        a.ypsi = ypsi;
+        a.yax = yax;
+        a.yay = yay;
+        a.at = at;
+        a.dat = c->dat;
+        a.dxat = c->dxat32;
+        a.dyat = c->dyat32;
+        a.dxpsi = c->dxpsi32;
+        a.dypsi = c->dypsi32;
+        a.lap = c->lap32;
+        a.divA = c->divA32;
+        a.dxB = c->dxB32;
+        a.dyB = c->dyB32;
+        a.zpsi = psi;
+        a.zax = ax;
+        a.zay = ay;
+        a.zrho = c->rho;
+        a.kpsi = c->kpsi;
+        a.kax = c->kax;
+        a.kay = c->kay;
+        a.krho = c->krho;
+        a.npsi = c->ypsi2[ni];
+        a.nax = c->yax2[ni];
+        a.nay = c->yay2[ni];
+        a.npsi_d = c->ypsi32[ni];
+        a.nax_d = c->yax32[ni];
+        a.nay_d = c->yay32[ni];
+        a.wpsi = psi;
+        a.wax = ax;
+        a.way = ay;
+        a.wrho = c->rho;
+        a.f2x = c->f2x;
+        a.f2y = c->f2y;
+        a.slice_mean = c->slice_mean;
+        RC(launch_zstage_mixed(c, s, a));
+        // F2(z=0) = d_x(Lz(nz,:)A_x) + d_y(Lz(nz,:)A_y) in FP64 on one slice
+        RC(launch_x_d1(c, FieldIn<double>{nullptr, c->f2x, nullptr},
+                       FieldOut<double>{nullptr, c->f2x, nullptr}, 1));
+        RC(launch_y_d1(c, FieldIn<double>{nullptr, c->f2y, nullptr}, c->f2x,
+                       FieldOut<double>{nullptr, c->f2, nullptr}, 1));
+        {
+            Prof pr(c, K_RHO);
+            k_rho_stage<<<148, 256, 0, c->stream>>>(c->f2, c->p.dt, s, c->plane, c->rho, c->krho,
+                                                     c->rho);
+            CK(cudaGetLastError());
+        }
+    }
+    return HQT_OK;
+}
+
 int enqueue_step(hqt_ctx *c) {
     double2 *psi = c->cpsi;
     double *at = c->cat, *ax = c->cax, *ay = c->cay;
+    if (c->mixed) {
+        RC(enqueue_stages_mixed(c));
+    } else {
     // A_t is frozen during the four stages: its horizontal derivatives once
     RC(launch_x_d1(c, FieldIn<double>{nullptr, at, nullptr},
                    FieldOut<double>{nullptr, c->dxat, nullptr}));
@@ -519,6 +738,7 @@ int enqueue_step(hqt_ctx *c) {
             case 3: RC(launch_zstage<3>(c, a)); break;
             default: RC(launch_zstage<4>(c, a)); break;
         }
+    }
     }
     // constraint: div A of the combined fields, then A_t, BCs, O
     RC(launch_x_d1(c, FieldIn<double>{nullptr, ax, nullptr},
@@ -576,7 +796,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 4 + 2 + 1 + 1;
+    long long n = 2 + 4 * 4 + 2 + 1 + 1 + (c->mixed ? 2 + 4 * 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -785,8 +1005,6 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         return fail(nullptr, HQT_EINVAL, "dt, mu, vy must be finite");
     if (p.precision != HQT_FP64 && p.precision != HQT_MIXED)
         return fail(nullptr, HQT_EINVAL, "precision must be HQT_FP64 or HQT_MIXED");
-    if (p.precision == HQT_MIXED)
-        return fail(nullptr, HQT_EUNSUPPORTED, "mixed precision is not built in this library");
     if ((long long)p.nx * p.ny * p.nz > (1LL << 31))
         return fail(nullptr, HQT_EUNSUPPORTED, "grid too large");
     int ndev = 0;
@@ -802,6 +1020,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     c->nz = p.nz;
     c->plane = (long long)p.nx * p.ny;
     c->vol = c->plane * p.nz;
+    c->mixed = (p.precision == HQT_MIXED);
     c->NZP = 0;
     for (int v : kNZP)
         if (v >= p.nz) {
@@ -883,6 +1102,30 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->dat, sizeof(double) * V);
     A(&c->dxax, sizeof(double) * V);
     A(&c->O, sizeof(double2) * P2);
+    if (c->mixed) {
+        for (int b = 0; b < 3; ++b) {
+            A(&c->ypsi32[b], sizeof(float2) * V);
+            A(&c->yax32[b], sizeof(float) * V);
+            A(&c->yay32[b], sizeof(float) * V);
+        }
+        A(&c->at32, sizeof(float) * V);
+        A(&c->dxpsi32, sizeof(float2) * V);
+        A(&c->lap32, sizeof(float2) * V);
+        A(&c->E32, sizeof(float2) * V);
+        A(&c->dypsi32, sizeof(float2) * V);
+        A(&c->dxxay32, sizeof(float) * V);
+        A(&c->divA32, sizeof(float) * V);
+        A(&c->dxB32, sizeof(float) * V);
+        A(&c->dyB32, sizeof(float) * V);
+        A(&c->dxat32, sizeof(float) * V);
+        A(&c->dyat32, sizeof(float) * V);
+        A(&c->f2x, sizeof(double) * P2);
+        A(&c->f2y, sizeof(double) * P2);
+        A(&c->f2, sizeof(double) * P2);
+        A(&c->slice_mean, sizeof(double) * 5 * p.nz);
+    }
+    A(&c->rootsx32, sizeof(float2) * p.nx);
+    A(&c->rootsy32, sizeof(float2) * p.ny);
     A(&c->partial, sizeof(double) * kPartials);
     c->max_bins = p.nx + p.ny + 4;
     A(&c->kxv, sizeof(double) * p.nx);
@@ -903,7 +1146,12 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
             if (i >= 0 && i < p.ny) hmy[i] = 0.0;
         DevStatus s0{};
         s0.first_bad_step = LLONG_MAX;
-        if (cudaMemcpy(c->rootsx, rx.data(), sizeof(double2) * p.nx, cudaMemcpyHostToDevice) ||
+        std::vector<float2> rx32(p.nx), ry32(p.ny);
+        for (int i = 0; i < p.nx; ++i) rx32[i] = make_float2((float)rx[i].x, (float)rx[i].y);
+        for (int i = 0; i < p.ny; ++i) ry32[i] = make_float2((float)ry[i].x, (float)ry[i].y);
+        if (cudaMemcpy(c->rootsx32, rx32.data(), sizeof(float2) * p.nx, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->rootsy32, ry32.data(), sizeof(float2) * p.ny, cudaMemcpyHostToDevice) ||
+            cudaMemcpy(c->rootsx, rx.data(), sizeof(double2) * p.nx, cudaMemcpyHostToDevice) ||
             cudaMemcpy(c->rootsy, ry.data(), sizeof(double2) * p.ny, cudaMemcpyHostToDevice) ||
             cudaMemcpy(c->mx, hmx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice) ||
             cudaMemcpy(c->my, hmy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice) ||

@@ -100,16 +100,19 @@ template <typename T, int NZP> struct ZOps {
     T lzb[NZP];  // boundary row Lz(nz, :)
 };
 
-template <typename T, typename TS> struct ZStageArgs {
+// T: stage-input and arithmetic type, TS: state / accumulator type,
+// TD: type of the horizontal-derivative fields written by the line passes.
+template <typename T, typename TS, typename TD = T> struct ZStageArgs {
     int nz;
     long long plane;  // nx*ny
     TS h;
-    // stage inputs (type T)
+    // stage inputs
     const C2<T> *ypsi;
     const T *yax, *yay;
-    const T *at, *dat, *dxat, *dyat;
-    const C2<T> *dxpsi, *dypsi, *lap;
-    const T *divA, *dxB, *dyB;
+    const T *at, *dat;
+    const TD *dxat, *dyat;
+    const C2<TD> *dxpsi, *dypsi, *lap;
+    const TD *divA, *dxB, *dyB;
     // RK state and accumulators (type TS)
     const C2<TS> *zpsi;
     const TS *zax, *zay, *zrho;
@@ -117,8 +120,18 @@ template <typename T, typename TS> struct ZStageArgs {
     TS *kax, *kay, *krho;
     C2<T> *npsi;  // next stage input
     T *nax, *nay;
+    C2<TD> *npsi_d;  // its copy in the derivative type (mixed precision; may be null)
+    TD *nax_d, *nay_d;
+    // per z-slice plane means (psi re, psi im, A_t, A_x, A_y), subtracted from
+    // the copies above: the line passes only differentiate, and the smaller
+    // magnitude rounds to FP32 with a smaller error
+    const TS *slice_mean;
     C2<TS> *wpsi;  // new state (stage 4)
     TS *wax, *way, *wrho;
+    // When set (mixed precision), k_zgauge writes the boundary-row contractions
+    // Lz(nz,:)*A_x and Lz(nz,:)*A_y (2-D, type T) and k_zpsi leaves rhoi alone:
+    // F2 = d_x(Lz(nz,:)A_x) + d_y(Lz(nz,:)A_y) is then formed in T precision.
+    T *f2x, *f2y;
     // right-hand-side outputs (MODE 0)
     C2<T> *f1;
     T *f3, *f4, *f2b;

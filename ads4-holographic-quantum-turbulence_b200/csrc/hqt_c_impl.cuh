@@ -38,6 +38,10 @@ cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const 
     opt((const void *)k_x_filt_fwd_c<double, HQT_CN>);
     opt((const void *)k_y_filt_c<double, HQT_CN>);
     opt((const void *)k_x_filt_inv_c<double, HQT_CN>);
+    opt((const void *)k_x_rhs_c<float, HQT_CN>);
+    opt((const void *)k_y_rhs_c<float, HQT_CN>);
+    opt((const void *)k_x_d1_c<float, HQT_CN>);
+    opt((const void *)k_y_d1_c<float, HQT_CN>);
     return e;
 }
 
@@ -68,6 +72,18 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
         case CT_FX_INV:
             k_x_filt_inv_c<double, HQT_CN>
                 <<<grid, T, smem, s>>>(*(const XFiltInvArgs<double> *)args);
+            break;
+        case CT_X_RHS_F:
+            k_x_rhs_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const XRhsArgs<float> *)args);
+            break;
+        case CT_Y_RHS_F:
+            k_y_rhs_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<float> *)args);
+            break;
+        case CT_X_D1_F:
+            k_x_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const XD1Args<float> *)args);
+            break;
+        case CT_Y_D1_F:
+            k_y_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const YD1Args<float> *)args);
             break;
         default:
             return cudaErrorInvalidValue;

@@ -68,10 +68,11 @@ __host__ __device__ constexpr int tab_offset(int R) {
 constexpr int kTabTotal = tab_offset(16) + 16;
 
 // Lines per block of the compile-time line transforms: a block holds
-// (1 + nbuf*NB) lines of N complex doubles in about 54 KB of shared memory,
+// (1 + nbuf*NB) lines of N complex values of esize bytes in about 54 KB of
+// shared memory,
 // so that four 128-thread blocks fit on an SM.
-__host__ __device__ constexpr int ct_lines(int N, int nbuf) {
-    const int v = ((54 * 1024) / 16 / N - 1) / nbuf;
+__host__ __device__ constexpr int ct_lines(int N, int nbuf, int esize = 16) {
+    const int v = ((54 * 1024) / esize / N - 1) / nbuf;
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
 

@@ -48,7 +48,7 @@ __device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long z
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
-    constexpr int NB = ct_lines(N, 3);
+    constexpr int NB = ct_lines(N, 3, sizeof(C2<T>));
     const int L0 = blockIdx.x * NB;
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
@@ -85,7 +85,7 @@ __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
-    constexpr int NB = ct_lines(N, 3);
+    constexpr int NB = ct_lines(N, 3, sizeof(C2<T>));
     const int x0 = blockIdx.x * NB;
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -166,7 +166,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
-    constexpr int NB = ct_lines(N, 2);
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
     const int L0 = blockIdx.x * NB;
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;
@@ -183,7 +183,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
-    constexpr int NB = ct_lines(N, 2);
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
     const int x0 = blockIdx.x * NB;
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -203,7 +203,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
-    constexpr int NB = ct_lines(N, 2);
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
     const int L0 = blockIdx.x * NB;
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;
@@ -233,7 +233,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
-    constexpr int TX = ct_lines(N, 6);
+    constexpr int TX = ct_lines(N, 6, sizeof(C2<T>));
     constexpr int NB = 3 * TX;  // up to three fields of TX columns
     const int x0 = blockIdx.x * TX;
     const int valid = min(TX, a.nx - x0);
@@ -273,7 +273,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
-    constexpr int NB = ct_lines(N, 2);
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
     const int L0 = blockIdx.x * NB;
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;

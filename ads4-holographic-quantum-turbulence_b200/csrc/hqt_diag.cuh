@@ -122,6 +122,65 @@ __global__ void k_phase_multiply(double2 *psi, int nx, int ny, long long vol,
     }
 }
 
+// Per z-slice plane means of (Re psi, Im psi, A_t, A_x, A_y): block z sums
+// the slice in a fixed tree (deterministic).
+__global__ void __launch_bounds__(kRedThreads)
+    k_slice_means(const double2 *psi, const double *at, const double *ax, const double *ay,
+                  long long plane, double *mean) {
+    __shared__ double sh[5][kRedThreads];
+    const long long off = (long long)blockIdx.x * plane;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long s = threadIdx.x; s < plane; s += blockDim.x) {
+        const double2 p = psi[off + s];
+        acc[0] += p.x;
+        acc[1] += p.y;
+        acc[2] += at[off + s];
+        acc[3] += ax[off + s];
+        acc[4] += ay[off + s];
+    }
+    for (int f = 0; f < 5; ++f) sh[f][threadIdx.x] = acc[f];
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int f = 0; f < 5; ++f) sh[f][threadIdx.x] += sh[f][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 5) mean[5 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0] / (double)plane;
+}
+
+// FP32 copies of the state minus the slice means, for the FP32 line passes
+// (mixed precision).
+__global__ void k_state_to_f32(const double2 *psi, const double *at, const double *ax,
+                               const double *ay, long long plane, long long vol,
+                               const double *mean, float2 *psi32, float *at32, float *ax32,
+                               float *ay32) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
+         s += (long long)gridDim.x * blockDim.x) {
+        const double *m = mean + 5 * (s / plane);
+        const double2 p = psi[s];
+        psi32[s] = make_float2((float)(p.x - m[0]), (float)(p.y - m[1]));
+        at32[s] = (float)(at[s] - m[2]);
+        ax32[s] = (float)(ax[s] - m[3]);
+        ay32[s] = (float)(ay[s] - m[4]);
+    }
+}
+
+// rhoi bookkeeping of one stage from F2 at the boundary slice (2-D):
+// stages 1-3 accumulate k2 = h*F2, stage 4 applies rhoi -= (1/6)(sum).
+__global__ void k_rho_stage(const double *f2, double h, int mode, long long plane,
+                            const double *zrho, double *krho, double *wrho) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < plane;
+         s += (long long)gridDim.x * blockDim.x) {
+        const double k = h * f2[s];
+        if (mode == 1)
+            krho[s] = k;
+        else if (mode == 2 || mode == 3)
+            krho[s] = krho[s] + 2 * k;
+        else
+            wrho[s] = zrho[s] - (1.0 / 6.0) * (krho[s] + k);
+    }
+}
+
 // rhoi replicated along z -> 2-D, and back.
 __global__ void k_rho_gather(const double *rho3, int nz, long long plane, double *rho2) {
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < plane;

@@ -29,6 +29,10 @@ cudaError_t fft_init(const double *tc, const double *ts, int ntab, int max_smem)
     opt((const void *)k_y_filt<double>);
     opt((const void *)k_x_filt_inv<double>);
     opt((const void *)k_y_fwd<double>);
+    opt((const void *)k_x_rhs<float>);
+    opt((const void *)k_y_rhs<float>);
+    opt((const void *)k_x_d1<float>);
+    opt((const void *)k_y_d1<float>);
     return e;
 }
 
@@ -64,6 +68,22 @@ cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t sm
     return cudaGetLastError();
 }
 
+cudaError_t launch_x_rhs_f(const XRhsArgs<float> &a, int grid, size_t smem, cudaStream_t s) {
+    k_x_rhs<float><<<grid, 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_y_rhs_f(const YRhsArgs<float> &a, dim3 grid, size_t smem, cudaStream_t s) {
+    k_y_rhs<float><<<grid, 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_x_d1_f(const XD1Args<float> &a, int grid, size_t smem, cudaStream_t s) {
+    k_x_d1<float><<<grid, 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_y_d1_f(const YD1Args<float> &a, dim3 grid, size_t smem, cudaStream_t s) {
+    k_y_d1<float><<<grid, 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
 cudaError_t launch_y_fwd(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
     k_y_fwd<double><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();

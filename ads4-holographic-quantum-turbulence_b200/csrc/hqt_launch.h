@@ -25,9 +25,18 @@ cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cu
 cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s);
 cudaError_t launch_y_fwd(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s);
+// FP32 versions of the stage passes (mixed precision)
+cudaError_t launch_x_rhs_f(const XRhsArgs<float> &a, int grid, size_t smem, cudaStream_t s);
+cudaError_t launch_y_rhs_f(const YRhsArgs<float> &a, dim3 grid, size_t smem, cudaStream_t s);
+cudaError_t launch_x_d1_f(const XD1Args<float> &a, int grid, size_t smem, cudaStream_t s);
+cudaError_t launch_y_d1_f(const YD1Args<float> &a, dim3 grid, size_t smem, cudaStream_t s);
 
 // Compile-time line lengths (hqt_c<N>.cu): kinds of pass kernel.
-enum CtKind { CT_X_RHS, CT_Y_RHS, CT_X_D1, CT_Y_D1, CT_FX_FWD, CT_FY, CT_FX_INV };
+enum CtKind {
+    CT_X_RHS, CT_Y_RHS, CT_X_D1, CT_Y_D1, CT_FX_FWD, CT_FY, CT_FX_INV,
+    // FP32 line passes of the mixed-precision stage (args of type <float>)
+    CT_X_RHS_F, CT_Y_RHS_F, CT_X_D1_F, CT_Y_D1_F
+};
 template <int N> cudaError_t ct_init(const double *tab_cos, const double *tab_sin, int ntab,
                                      const double *big_cos, const double *big_sin, int nbig,
                                      int max_smem);
@@ -40,6 +49,9 @@ template <int N> cudaError_t z_init(int max_smem);
 template <int N>
 cudaError_t z_stage(int mode, const ZStageArgs<double, double> &a, const ZHost &h, int grid,
                     int threads, size_t smem, cudaStream_t s);
+template <int N>
+cudaError_t z_stage_mixed(int mode, const ZStageArgs<double, double, float> &a, const ZHost &h,
+                          int grid, int threads, size_t smem, cudaStream_t s);
 template <int N>
 cudaError_t z_cons(const ZConsArgs<double> &a, const ZHost &h, int grid, int threads,
                    cudaStream_t s);
@@ -60,6 +72,9 @@ namespace hqt {
     template <>                                                                            \
     cudaError_t z_stage<N>(int, const ZStageArgs<double, double> &, const ZHost &, int, int, \
                            size_t, cudaStream_t);                                          \
+    template <>                                                                            \
+    cudaError_t z_stage_mixed<N>(int, const ZStageArgs<double, double, float> &,            \
+                                 const ZHost &, int, int, size_t, cudaStream_t);           \
     template <>                                                                            \
     cudaError_t z_cons<N>(const ZConsArgs<double> &, const ZHost &, int, int, cudaStream_t); \
     template <>                                                                            \

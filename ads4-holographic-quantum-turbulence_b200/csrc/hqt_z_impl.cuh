@@ -36,11 +36,15 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      max_smem - (int)fa.sharedSizeBytes);
     };
-    opt((const void *)k_zpsi<double, double, HQT_ZN, 0>);
-    opt((const void *)k_zpsi<double, double, HQT_ZN, 1>);
-    opt((const void *)k_zpsi<double, double, HQT_ZN, 2>);
-    opt((const void *)k_zpsi<double, double, HQT_ZN, 3>);
-    opt((const void *)k_zpsi<double, double, HQT_ZN, 4>);
+    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 0>);
+    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 1>);
+    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 2>);
+    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 3>);
+    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 4>);
+    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 1>);
+    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 2>);
+    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 3>);
+    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 4>);
     return e;
 }
 
@@ -53,10 +57,32 @@ cudaError_t z_stage<HQT_ZN>(int mode, const ZStageArgs<double, double> &a, const
     switch (mode) {
 #define HQT_ZS(M)                                                                    \
     case M:                                                                          \
-        k_zgauge<double, double, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op);         \
-        k_zpsi<double, double, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op);        \
+        k_zgauge<double, double, double, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op); \
+        k_zpsi<double, double, double, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op); \
         break;
         HQT_ZS(0)
+        HQT_ZS(1)
+        HQT_ZS(2)
+        HQT_ZS(3)
+        HQT_ZS(4)
+#undef HQT_ZS
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <>
+cudaError_t z_stage_mixed<HQT_ZN>(int mode, const ZStageArgs<double, double, float> &a,
+                                  const ZHost &h, int grid, int threads, size_t smem,
+                                  cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    switch (mode) {
+#define HQT_ZS(M)                                                                       \
+    case M:                                                                             \
+        k_zgauge<double, double, float, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op);     \
+        k_zpsi<double, double, float, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op);    \
+        break;
         HQT_ZS(1)
         HQT_ZS(2)
         HQT_ZS(3)

@@ -27,21 +27,28 @@ namespace hqt {
 
 #define HQT_LD(ptr, j) (((j) < nz) ? (ptr)[(long long)(j) * P + site] : T(0))
 
-template <typename T, typename TS, int MODE>
-__device__ __forceinline__ void rk_update_c(const ZStageArgs<T, TS> &a, long long g,
+template <typename T, typename TS, typename TD, int MODE>
+__device__ __forceinline__ void rk_update_c(const ZStageArgs<T, TS, TD> &a, long long g, int lev,
                                             C2<TS> k) {
-    if (MODE == 1) {
-        a.kpsi[g] = k;
+    if (MODE >= 1 && MODE <= 3) {
+        C2<TS> nv;
         const C2<TS> z = a.zpsi[g];
-        a.npsi[g] = mk2<T>(T(z.x + k.x / 2), T(z.y + k.y / 2));
-    } else if (MODE == 2 || MODE == 3) {
-        const C2<TS> K = a.kpsi[g];
-        a.kpsi[g] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
-        const C2<TS> z = a.zpsi[g];
-        if (MODE == 2)
-            a.npsi[g] = mk2<T>(T(z.x + k.x / 2), T(z.y + k.y / 2));
+        if (MODE == 1) {
+            a.kpsi[g] = k;
+        } else {
+            const C2<TS> K = a.kpsi[g];
+            a.kpsi[g] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
+        }
+        if (MODE == 3)
+            nv = mk2<TS>(z.x + k.x, z.y + k.y);
         else
-            a.npsi[g] = mk2<T>(T(z.x + k.x), T(z.y + k.y));
+            nv = mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
+        a.npsi[g] = mk2<T>(T(nv.x), T(nv.y));
+        if (a.npsi_d) {
+            const TS mr = a.slice_mean ? a.slice_mean[5 * lev] : TS(0);
+            const TS mi = a.slice_mean ? a.slice_mean[5 * lev + 1] : TS(0);
+            a.npsi_d[g] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
+        }
     } else if (MODE == 4) {
         const C2<TS> K = a.kpsi[g];
         const C2<TS> z = a.zpsi[g];
@@ -50,15 +57,17 @@ __device__ __forceinline__ void rk_update_c(const ZStageArgs<T, TS> &a, long lon
     }
 }
 
-template <typename T, typename TS, int MODE>
-__device__ __forceinline__ void rk_update_r(const TS *zsrc, TS *kacc, T *next, TS *wnew,
-                                            long long g, TS k) {
-    if (MODE == 1) {
-        kacc[g] = k;
-        next[g] = T(zsrc[g] + k / 2);
-    } else if (MODE == 2 || MODE == 3) {
-        kacc[g] = kacc[g] + 2 * k;
-        next[g] = (MODE == 2) ? T(zsrc[g] + k / 2) : T(zsrc[g] + k);
+template <typename T, typename TS, typename TD, int MODE>
+__device__ __forceinline__ void rk_update_r(const TS *zsrc, TS *kacc, T *next, TD *next_d,
+                                            TS mean, TS *wnew, long long g, TS k) {
+    if (MODE >= 1 && MODE <= 3) {
+        if (MODE == 1)
+            kacc[g] = k;
+        else
+            kacc[g] = kacc[g] + 2 * k;
+        const TS nv = (MODE == 3) ? zsrc[g] + k : zsrc[g] + k / 2;
+        next[g] = T(nv);
+        if (next_d) next_d[g] = TD(nv - mean);
     } else if (MODE == 4) {
         wnew[g] = zsrc[g] + (TS(1) / TS(6)) * (kacc[g] + k);
     }
@@ -72,8 +81,8 @@ __device__ __forceinline__ void rk_update_r(const TS *zsrc, TS *kacc, T *next, T
 // Contractions stream the input column: out_i += Lz[i][j] * v_j as v_j
 // arrives, so only the outputs are held in registers.
 // MODE 0: right-hand side only, MODE 1..4: RK stage.
-template <typename T, typename TS, int NZP, int MODE>
-__global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, NZP> op) {
+template <typename T, typename TS, typename TD, int NZP, int MODE>
+__global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS, TD> a, ZOps<T, NZP> op) {
     const long long site = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (site >= a.plane) return;
     const int nz = a.nz;
@@ -81,10 +90,13 @@ __global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, 
 #pragma unroll
     for (int comp = 0; comp < 2; ++comp) {
         const T *src = comp == 0 ? a.yax : a.yay;
-        const T *dt = comp == 0 ? a.dxat : a.dyat;
-        const C2<T> *dps = comp == 0 ? a.dxpsi : a.dypsi;
+        const TD *dt = comp == 0 ? a.dxat : a.dyat;
+        const C2<TD> *dps = comp == 0 ? a.dxpsi : a.dypsi;
+        T *nx_ = comp == 0 ? a.nax : a.nay;
+        TD *nxd_ = comp == 0 ? a.nax_d : a.nay_d;
         // g = d_{x|y} A_t + f * Lz A_{x|y}
         T g[NZP];
+        T bnd = T(0);
 #pragma unroll
         for (int i = 0; i < NZP; ++i) g[i] = T(0);
 #pragma unroll
@@ -93,11 +105,13 @@ __global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, 
                 const T v = src[(long long)j * P + site];
 #pragma unroll
                 for (int i = 0; i < NZP; ++i) g[i] = fma(op.Lz[i][j], v, g[i]);
+                bnd = fma(op.lzb[j], v, bnd);
             }
         }
+        if (a.f2x) (comp == 0 ? a.f2x : a.f2y)[site] = bnd;
 #pragma unroll
         for (int i = 0; i < NZP; ++i)
-            g[i] = (i < nz) ? dt[(long long)i * P + site] + op.fz[i] * g[i] : T(0);
+            g[i] = (i < nz) ? T(dt[(long long)i * P + site]) + op.fz[i] * g[i] : T(0);
         // S = 1/2 Lz g -/+ 1/2 d_{y|x} B + Im(conj(Psi) d Psi) - A |Psi|^2
         T s[NZP];
 #pragma unroll
@@ -108,8 +122,9 @@ __global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, 
                 for (int j = 0; j < NZP; ++j) d = fma(op.Lz[i][j], g[j], d);
                 const long long gi = (long long)i * P + site;
                 const C2<T> ps = a.ypsi[gi];
-                const C2<T> dd = dps[gi];
-                const T bf = comp == 0 ? -a.dyB[gi] : a.dxB[gi];
+                const C2<TD> ddd = dps[gi];
+                const C2<T> dd = mk2<T>(T(ddd.x), T(ddd.y));
+                const T bf = comp == 0 ? -T(a.dyB[gi]) : T(a.dxB[gi]);
                 const T av = src[gi];
                 s[i] = T(0.5) * d + T(0.5) * bf + (ps.x * dd.y - ps.y * dd.x) -
                        av * (ps.x * ps.x + ps.y * ps.y);
@@ -127,18 +142,22 @@ __global__ void __launch_bounds__(128, 4) k_zgauge(ZStageArgs<T, TS> a, ZOps<T, 
                 const long long gi = (long long)i * P + site;
                 if (MODE == 0) {
                     (comp == 0 ? a.f3 : a.f4)[gi] = fr;
-                } else if (comp == 0) {
-                    rk_update_r<T, TS, MODE>(a.zax, a.kax, a.nax, a.wax, gi, a.h * TS(fr));
                 } else {
-                    rk_update_r<T, TS, MODE>(a.zay, a.kay, a.nay, a.way, gi, a.h * TS(fr));
+                    const TS mean = a.slice_mean ? a.slice_mean[5 * i + 3 + comp] : TS(0);
+                    if (comp == 0)
+                        rk_update_r<T, TS, TD, MODE>(a.zax, a.kax, nx_, nxd_, mean, a.wax, gi,
+                                                     a.h * TS(fr));
+                    else
+                        rk_update_r<T, TS, TD, MODE>(a.zay, a.kay, nx_, nxd_, mean, a.way, gi,
+                                                     a.h * TS(fr));
                 }
             }
         }
     }
 }
 
-template <typename T, typename TS, int NZP, int MODE>
-__global__ void __launch_bounds__(128, 4) k_zpsi(ZStageArgs<T, TS> a, ZOps<T, NZP> op) {
+template <typename T, typename TS, typename TD, int NZP, int MODE>
+__global__ void __launch_bounds__(128, 4) k_zpsi(ZStageArgs<T, TS, TD> a, ZOps<T, NZP> op) {
     const int bd = blockDim.x;
     const int tid = threadIdx.x;
     const long long site = (long long)blockIdx.x * bd + tid;
@@ -175,8 +194,10 @@ __global__ void __launch_bounds__(128, 4) k_zpsi(ZStageArgs<T, TS> a, ZOps<T, NZ
                 const long long g = (long long)i * P + site;
                 const C2<T> ps = a.ypsi[g];
                 const T at = a.at[g], dat = a.dat[g], ax = a.yax[g], ay = a.yay[g];
-                const C2<T> lp = a.lap[g], dx = a.dxpsi[g], dy = a.dypsi[g];
-                const T dv = a.divA[g];
+                const C2<TD> lpd = a.lap[g], dxd = a.dxpsi[g], dyd = a.dypsi[g];
+                const C2<T> lp = mk2<T>(T(lpd.x), T(lpd.y)), dx = mk2<T>(T(dxd.x), T(dxd.y));
+                const C2<T> dy = mk2<T>(T(dyd.x), T(dyd.y));
+                const T dv = T(a.divA[g]);
                 const T z = op.zz[i], f = op.fz[i];
                 const C2<T> d1 = dp[i];
                 const T h = T(0.5);
@@ -212,13 +233,15 @@ __global__ void __launch_bounds__(128, 4) k_zpsi(ZStageArgs<T, TS> a, ZOps<T, NZ
                 if (MODE == 0)
                     a.f1[g] = mk2<T>(fr, fi);
                 else
-                    rk_update_c<T, TS, MODE>(a, g, mk2<TS>(a.h * TS(fr), a.h * TS(fi)));
+                    rk_update_c<T, TS, TD, MODE>(a, g, i, mk2<TS>(a.h * TS(fr), a.h * TS(fi)));
             }
         }
     }
     // F2 at the boundary slice -> rhoi
     if (MODE == 0) {
         a.f2b[site] = kb;
+    } else if (a.f2x) {
+        // formed from the boundary contractions by k_rho_stage
     } else {
         const TS k = a.h * TS(kb);
         if (MODE == 1) {

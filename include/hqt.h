@@ -43,7 +43,7 @@ extern "C" {
 
 /* precision modes */
 #define HQT_FP64   0         /* plain FP64 drop-in                          */
-#define HQT_MIXED  1         /* FP32 stage arithmetic, FP64 state/constraint */
+#define HQT_MIXED  1         /* FP32 x/y line passes; FP64 z columns, state, constraint */
 
 typedef struct hqt_ctx hqt_ctx;
 

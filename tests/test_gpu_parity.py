@@ -268,3 +268,42 @@ def test_energy_spectrum_parity(hqt, oracle, dev, nx, ny, nz):
     scale = E.max()
     for got, want in ((gE, E), (gEc, Ec), (gEi, Ei)):
         assert np.max(np.abs(got - want)) < 1e-9 * scale
+
+
+def test_mixed_precision_error_100_steps(hqt, oracle, cuda):
+    """Mixed precision (FP32 line passes on slice-mean-removed copies, FP64
+    columns and state) against the FP64 oracle after 100 steps at 64x64x21.
+    Relative L2 per field; A_x and A_y start at zero without a drive, so they
+    are measured against the gauge-field scale max|A_t|."""
+    nx, nz, L = 64, 21, 50.0
+    state = driven_state(hqt, nx, nx, nz, noise="complex", amp=1e-3, vy=0.0)
+    ref, _ = run_oracle(oracle, nx, nx, nz, L, state, 100, 0.02, 6.0, 0.0)
+    with hqt.Simulation(nx, nx, nz, Lx=L, mu=6.0, vy=0.0, dt=0.02, precision="mixed") as sim:
+        (g1, g2, g3, g4, gr), info = sim.step(*state, nsteps=100)
+    scale = np.max(np.abs(ref.Z2))
+    errs = {"Z1": rel_l2(g1, ref.Z1), "Z2": rel_l2(g2, ref.Z2), "rhoi": rel_l2(gr, ref.rhoi),
+            "Z3_abs": float(np.max(np.abs(g3 - ref.Z3)) / scale),
+            "Z4_abs": float(np.max(np.abs(g4 - ref.Z4)) / scale)}
+    print("mixed-precision errors after 100 steps:", errs)
+    assert max(errs.values()) < 1e-8, errs
+
+
+def test_mixed_precision_driven_301(hqt, cuda, dev):
+    """301x301x21 driven: mixed against the FP64 GPU path (itself pinned to the
+    oracle) after 100 steps.  A_x, which the drive keeps small, is measured
+    against the gauge-field scale max|A_t|; the others by relative L2."""
+    to_d, from_d = dev
+    nx, nz, L = 301, 21, 100.0
+    state = driven_state(hqt, nx, nx, nz, noise="complex", amp=1e-3)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        t = [to_d(a) for a in state]
+        with hqt.Simulation(nx, nx, nz, Lx=L, mu=6.0, vy=VY7, dt=0.02, precision=prec) as sim:
+            sim.step_device(*t, nsteps=100)
+        out[prec] = [from_d(x) for x in t]
+    m, f = out["mixed"], out["fp64"]
+    errs = {"Z1": rel_l2(m[0], f[0]), "Z2": rel_l2(m[1], f[1]), "Z4": rel_l2(m[3], f[3]),
+            "rhoi": rel_l2(m[4], f[4]),
+            "Z3_abs": float(np.max(np.abs(m[2] - f[2])) / np.max(np.abs(f[1])))}
+    print("mixed vs fp64 after 100 steps (301^2x21):", errs)
+    assert max(errs.values()) < 1e-8, errs
