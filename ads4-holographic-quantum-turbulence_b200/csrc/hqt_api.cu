@@ -513,7 +513,7 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
 template <int MODE> int launch_zstage(hqt_ctx *c, const ZStageArgs<double, double> &a) {
     const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
     const ZHost h = zhost(c);
-    Prof pr(c, K_ZSTAGE, 2);
+    Prof pr(c, K_ZSTAGE);
     switch (c->NZP) {
 #define HQT_Z(N)                                                                      \
     case N:                                                                           \
@@ -528,7 +528,7 @@ template <int MODE> int launch_zstage(hqt_ctx *c, const ZStageArgs<double, doubl
 int launch_zstage_mixed(hqt_ctx *c, int mode, const ZStageArgs<double, double, float> &a) {
     const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
     const ZHost h = zhost(c);
-    Prof pr(c, K_ZSTAGE, 2);
+    Prof pr(c, K_ZSTAGE);
     switch (c->NZP) {
 #define HQT_Z(N)                                                                       \
     case N:                                                                            \
@@ -796,7 +796,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 4 + 2 + 1 + 1 + (c->mixed ? 2 + 4 * 3 : 0);
+    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 2 + 4 * 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -1271,11 +1271,22 @@ int hqt_step(hqt_ctx *c, double *Z1, double *Z2, double *Z3, double *Z4, double 
     return r;
 }
 
+// The column kernels copy complex elements as 16-byte and real ones as
+// 8-byte units, so device arrays must be aligned to their element size.
+static bool aligned_fields(const void *z1, const void *z2, const void *z3, const void *z4) {
+    return (reinterpret_cast<uintptr_t>(z1) % 16 == 0) &&
+           (reinterpret_cast<uintptr_t>(z2) % 8 == 0) &&
+           (reinterpret_cast<uintptr_t>(z3) % 8 == 0) &&
+           (reinterpret_cast<uintptr_t>(z4) % 8 == 0);
+}
+
 int hqt_step_device(hqt_ctx *c, void *dZ1, void *dZ2, void *dZ3, void *dZ4, void *drhoi,
                     int64_t nsteps, hqt_diag *diag) {
     if (!c) return HQT_EINVAL;
     if (!dZ1 || !dZ2 || !dZ3 || !dZ4 || !drhoi || nsteps < 0)
         return fail(c, HQT_EINVAL, "bad argument");
+    if (!aligned_fields(dZ1, dZ2, dZ3, dZ4) || reinterpret_cast<uintptr_t>(drhoi) % 8 != 0)
+        return fail(c, HQT_EINVAL, "device arrays must be aligned to their element size");
     DeviceGuard guard(c->device);
     // the kernels act on the caller's arrays directly; only rhoi is reduced
     // to its boundary slice and replicated back
@@ -1352,6 +1363,8 @@ int hqt_rhs_device(hqt_ctx *c, const void *dZ1, const void *dZ2, const void *dZ3
     if (!c) return HQT_EINVAL;
     if (!dZ1 || !dZ2 || !dZ3 || !dZ4 || !dF1 || !dF3 || !dF4 || !dF2b)
         return fail(c, HQT_EINVAL, "bad argument");
+    if (!aligned_fields(dZ1, dZ2, dZ3, dZ4) || !aligned_fields(dF1, dF3, dF4, dF2b))
+        return fail(c, HQT_EINVAL, "device arrays must be aligned to their element size");
     DeviceGuard guard(c->device);
     const double2 *psi = (const double2 *)dZ1;
     const double *at = (const double *)dZ2, *ax = (const double *)dZ3, *ay = (const double *)dZ4;

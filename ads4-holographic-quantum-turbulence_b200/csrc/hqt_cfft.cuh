@@ -87,8 +87,8 @@ template <> struct BigTab<float> {
 constexpr int kCtThreads = 128;
 constexpr int kCtKB = 6;  // output pairs per warp task of a large odd radix
 
-template <typename T, int N, int NB, int R, int Ns, int SIGN>
-__device__ __forceinline__ void ct_small(int src, int dst, int roots) {
+template <typename T, int N, int NB, int R, int Ns>
+__device__ __forceinline__ void ct_small(int src, int dst, int roots, int sign) {
     const C2<T> *S = sptr<T>(src);
     C2<T> *D = sptr<T>(dst);
     const C2<T> *W = sptr<T>(roots);
@@ -107,17 +107,17 @@ __device__ __forceinline__ void ct_small(int src, int dst, int roots) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
                 C2<T> w = W[r * step];
-                if (SIGN > 0) w.y = -w.y;
+                if (sign > 0) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
         const int idxD = (j - m) * R + m;
-        dft_store<T, R>(v, D, idxD * NB + b, Ns * NB, SIGN);
+        dft_store<T, R>(v, D, idxD * NB + b, Ns * NB, sign);
     }
 }
 
-template <typename T, int N, int NB, int R, int Ns, int SIGN>
-__device__ __forceinline__ void ct_big(int src, int dst, int roots) {
+template <typename T, int N, int NB, int R, int Ns>
+__device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
     C2<T> *S = sptr<T>(src);
     C2<T> *D = sptr<T>(dst);
     const C2<T> *W = sptr<T>(roots);
@@ -138,7 +138,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots) {
         C2<T> u = S[e1], v = S[e2];
         if (Ns > 1 && m > 0) {
             C2<T> w1 = W[t * m * qs], w2 = W[(R - t) * m * qs];
-            if (SIGN > 0) {
+            if (sign > 0) {
                 w1.y = -w1.y;
                 w2.y = -w2.y;
             }
@@ -153,7 +153,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots) {
     constexpr int NBF = NB * nR;                  // butterflies in the batch
     constexpr int NKB = (M + kCtKB) / kCtKB;      // pair blocks covering 0..M
     constexpr int NG = (NBF + 31) / 32;           // butterfly groups
-    constexpr T sg = (SIGN < 0) ? T(1) : T(-1);
+    const T sg = (sign < 0) ? T(1) : T(-1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int task = warp; task < NKB * NG; task += kCtThreads / 32) {
         const int kb = task % NKB;
@@ -213,8 +213,8 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots) {
     }
 }
 
-template <typename T, int N, int NB, int SIGN, int P>
-__device__ __forceinline__ int ct_fft_from(int src, int dst, int roots) {
+template <typename T, int N, int NB, int P>
+__device__ __forceinline__ int ct_fft_from(int src, int dst, int roots, int sign) {
     constexpr CtPlan pl = ct_plan(N);
     if constexpr (P >= pl.np) {
         return src;
@@ -222,18 +222,25 @@ __device__ __forceinline__ int ct_fft_from(int src, int dst, int roots) {
         constexpr int R = pl.R[P];
         constexpr int Ns = pl.Ns[P];
         if constexpr (ct_small_radix(R))
-            ct_small<T, N, NB, R, Ns, SIGN>(src, dst, roots);
+            ct_small<T, N, NB, R, Ns>(src, dst, roots, sign);
         else
-            ct_big<T, N, NB, R, Ns, SIGN>(src, dst, roots);
+            ct_big<T, N, NB, R, Ns>(src, dst, roots, sign);
         __syncthreads();
-        return ct_fft_from<T, N, NB, SIGN, P + 1>(dst, src, roots);
+        return ct_fft_from<T, N, NB, P + 1>(dst, src, roots, sign);
     }
 }
 
 // All passes on NB lines in buffer a (partner b); returns the result buffer.
+// One out-of-line copy per (T, N, NB) serves both directions and every call
+// site of a kernel: inlined per call site, the unrolled large-prime radix
+// (2016 FMAs at N = 301) overflowed the instruction cache.
+template <typename T, int N, int NB>
+__device__ __noinline__ int ct_fft_rt(int a, int b, int roots, int sign) {
+    return ct_fft_from<T, N, NB, 0>(a, b, roots, sign);
+}
 template <typename T, int N, int NB, int SIGN>
 __device__ __forceinline__ int ct_fft(int a, int b, int roots) {
-    return ct_fft_from<T, N, NB, SIGN, 0>(a, b, roots);
+    return ct_fft_rt<T, N, NB>(a, b, roots, SIGN);
 }
 
 // dst = m(k) src over the batch (order 1: i*s1*k, order 2: s2*k^2)

@@ -1,9 +1,11 @@
 // hqt_z_impl.cuh -- launchers of the column kernels for one column length
 // HQT_ZN (each hqt_z<N>.cu defines HQT_ZN and includes this file).
 #include <cstring>
+#include <type_traits>
 
 #include "hqt_launch.h"
 #include "hqt_zcol.cuh"
+#include "hqt_zfused.cuh"
 
 #ifndef HQT_ZN
 #error "define HQT_ZN"
@@ -36,62 +38,58 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      max_smem - (int)fa.sharedSizeBytes);
     };
-    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 0>);
-    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 1>);
-    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 2>);
-    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 3>);
-    opt((const void *)k_zpsi<double, double, double, HQT_ZN, 4>);
-    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 1>);
-    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 2>);
-    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 3>);
-    opt((const void *)k_zpsi<double, double, float, HQT_ZN, 4>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 0>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 1>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 2>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 3>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 4>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 1>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 2>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 3>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 4>);
     return e;
+}
+
+// One fused launch per stage over tiles of kZTile columns (hqt_zfused.cuh).
+template <typename TD>
+static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> &a,
+                                 const ZHost &h, cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    const int grid = (int)((a.plane + kZTile - 1) / kZTile);
+    constexpr int threads = 32 * zf_warps(HQT_ZN);
+    constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN>();
+    switch (mode) {
+#define HQT_ZS(M)                                                                   \
+    case M:                                                                         \
+        k_zstage<double, double, TD, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op); \
+        break;
+        HQT_ZS(1)
+        HQT_ZS(2)
+        HQT_ZS(3)
+        HQT_ZS(4)
+#undef HQT_ZS
+        case 0:
+            if constexpr (std::is_same<TD, double>::value) {
+                k_zstage<double, double, double, HQT_ZN, 0><<<grid, threads, smem, s>>>(a, op);
+                break;
+            }
+            return cudaErrorInvalidValue;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 template <>
 cudaError_t z_stage<HQT_ZN>(int mode, const ZStageArgs<double, double> &a, const ZHost &h,
-                            int grid, int threads, size_t smem, cudaStream_t s) {
-    // grid/threads/smem describe k_zpsi; k_zgauge uses the same grid and no
-    // shared memory
-    const ZOps<double, HQT_ZN> op = make_zops(h);
-    switch (mode) {
-#define HQT_ZS(M)                                                                    \
-    case M:                                                                          \
-        k_zgauge<double, double, double, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op); \
-        k_zpsi<double, double, double, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op); \
-        break;
-        HQT_ZS(0)
-        HQT_ZS(1)
-        HQT_ZS(2)
-        HQT_ZS(3)
-        HQT_ZS(4)
-#undef HQT_ZS
-        default:
-            return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+                            int, int, size_t, cudaStream_t s) {
+    return z_stage_fused<double>(mode, a, h, s);
 }
 
 template <>
 cudaError_t z_stage_mixed<HQT_ZN>(int mode, const ZStageArgs<double, double, float> &a,
-                                  const ZHost &h, int grid, int threads, size_t smem,
-                                  cudaStream_t s) {
-    const ZOps<double, HQT_ZN> op = make_zops(h);
-    switch (mode) {
-#define HQT_ZS(M)                                                                       \
-    case M:                                                                             \
-        k_zgauge<double, double, float, HQT_ZN, M><<<grid, threads, 0, s>>>(a, op);     \
-        k_zpsi<double, double, float, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op);    \
-        break;
-        HQT_ZS(1)
-        HQT_ZS(2)
-        HQT_ZS(3)
-        HQT_ZS(4)
-#undef HQT_ZS
-        default:
-            return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+                                  const ZHost &h, int, int, size_t, cudaStream_t s) {
+    return z_stage_fused<float>(mode, a, h, s);
 }
 
 template <>
