@@ -50,18 +50,34 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     return e;
 }
 
-// One fused launch per stage over tiles of kZTile columns (hqt_zfused.cuh).
+// One fused launch per stage (hqt_zfused.cuh): persistent one-warp blocks,
+// as many as fit on the device at once, each looping over column tiles.
+template <typename TD, int M> static int z_stage_grid(long long plane) {
+    static int per_sm = 0, nsm = 0;
+    if (per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_zstage<double, double, TD, HQT_ZN, M>, 32,
+            zf_smem_bytes<double, double, TD, HQT_ZN>());
+        if (per_sm < 1) per_sm = 1;
+    }
+    const long long tiles = (plane + kZCols - 1) / kZCols;
+    const long long full = (long long)per_sm * (nsm > 0 ? nsm : 1);
+    return (int)(tiles < full ? tiles : full);
+}
+
 template <typename TD>
 static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> &a,
                                  const ZHost &h, cudaStream_t s) {
     const ZOps<double, HQT_ZN> op = make_zops(h);
-    const int grid = (int)((a.plane + kZTile - 1) / kZTile);
-    constexpr int threads = 32 * zf_warps(HQT_ZN);
     constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN>();
     switch (mode) {
-#define HQT_ZS(M)                                                                   \
-    case M:                                                                         \
-        k_zstage<double, double, TD, HQT_ZN, M><<<grid, threads, smem, s>>>(a, op); \
+#define HQT_ZS(M)                                                                            \
+    case M:                                                                                  \
+        k_zstage<double, double, TD, HQT_ZN, M>                                              \
+            <<<z_stage_grid<TD, M>(a.plane), 32, smem, s>>>(a, op);                          \
         break;
         HQT_ZS(1)
         HQT_ZS(2)
@@ -70,7 +86,8 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
 #undef HQT_ZS
         case 0:
             if constexpr (std::is_same<TD, double>::value) {
-                k_zstage<double, double, double, HQT_ZN, 0><<<grid, threads, smem, s>>>(a, op);
+                k_zstage<double, double, double, HQT_ZN, 0>
+                    <<<z_stage_grid<double, 0>(a.plane), 32, smem, s>>>(a, op);
                 break;
             }
             return cudaErrorInvalidValue;

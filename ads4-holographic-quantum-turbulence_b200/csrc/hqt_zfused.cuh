@@ -4,19 +4,21 @@
 // func_Lzr (:63-65), k = h*F with k(:,:,nz) = 0 and the RK4 bookkeeping
 // (:120-124,128).
 //
-// A block owns a tile of 32 adjacent (x, y) columns; lane = column.  Its
-// inputs are staged into shared memory with cp.async in phase groups, so
-// that a thread has tens of loads in flight without holding them in
-// registers, and buffers of finished phases are refilled with the inputs of
-// later ones while the current phase computes.  The output rows of every
-// Nz x Nz contraction are split over the warps (kRowsPerWarp rows each), so
-// a warp's accumulators are a few registers.  Lz, Lz1 and the boundary row
-// are a __grid_constant__ kernel parameter that a warp reads through the
-// constant cache at a warp-uniform row, so all warps run one copy of the
-// code (compile-time rows per warp multiply the code by the warp count and
-// overflow the instruction cache).  Each contraction sums j in ascending
-// order with one fma per term, the same order as a column-per-thread
-// evaluation.
+// Every radial operator is an Nz x Nz matrix applied to all columns, i.e. a
+// product (Nz x Nz) x (Nz x columns).  A warp owns a tile of kZCols = 8
+// adjacent (x, y) columns and runs each product on the FP64 tensor cores
+// (mma.sync m8n8k4 f64): the zero-padded Lz and Lz1 stay in the warp's
+// registers as A fragments for the life of the (persistent) warp, and the
+// column data is the B operand, read from the warp's own shared-memory tile.
+// The tile's inputs are staged there with cp.async in phase groups, so a
+// lane has tens of loads in flight, and buffers of finished phases are
+// refilled with the inputs of later ones while the current phase computes.
+// Warps share nothing, so there are no block barriers.
+//
+// Fragment layouts (g = lane/4, q = lane%4): A a0 = L[8m+g][4s+q];
+// B b0 = V[4s+q][col g]; C c_i = out[8m+g][col 2q+i].  Pointwise terms are
+// evaluated where the C fragments live: lane owns levels 8m+g, columns 2q
+// and 2q+1.
 //
 // Phases of a tile (MODE 1..4 = RK stage, MODE 0 = right-hand side only):
 //   G0  Psi, A_x, A_y, d_x Psi, d_y Psi (kept) and A_t, d_z A_t, lap Psi,
@@ -30,17 +32,14 @@
 //   P4  for A_x then A_y: g = d A_t + f Lz A, S = 1/2 Lz g +- 1/2 d B
 //       + Im(conj(Psi) d Psi) - A |Psi|^2 (:74-75), F = Lzr(S), RK update
 #pragma once
+#include <type_traits>
+
 #include "hqt_dev.cuh"
 #include "hqt_args.h"
 
 namespace hqt {
 
-constexpr int kZTile = 32;       // columns per block (one per lane)
-constexpr int kRowsPerWarp = 3;  // contraction rows per warp
-
-__host__ __device__ constexpr int zf_warps(int nzp) {
-    return (nzp + kRowsPerWarp - 1) / kRowsPerWarp;
-}
+constexpr int kZCols = 8;  // columns per warp tile (the n extent of one mma)
 
 // ---- cp.async (global -> shared, 4/8/16 bytes, completes per group) -------
 template <int BYTES>
@@ -51,25 +50,31 @@ __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Column field of a tile in shared memory: element (level l, lane c) at l*32+c.
-template <typename V> struct ZTileF {
-    V *p;
-    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZTile + c]; }
+// d += a * b on one 8x8x4 FP64 tensor-core tile
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+template <int NZP> struct ZmDims {
+    static constexpr int MT = (NZP + 7) / 8;  // 8-row output tiles
+    static constexpr int KS = (NZP + 3) / 4;  // 4-deep reduction steps
+    static constexpr int MP = 8 * MT, KP = 4 * KS;
+    static constexpr int LV = MP > KP ? MP : KP;  // levels stored per tile field
 };
 
-// Issue the copies of levels warp, warp+NW, ... of one field for this lane.
-template <typename V, int NW>
-__device__ __forceinline__ void zf_stage(ZTileF<V> dst, const V *src, int nz, long long P,
-                                         long long site, bool ok, int warp, int lane) {
-    if (!src || !ok) return;
-    for (int l = warp; l < nz; l += NW) cp_async<sizeof(V)>(&dst(l, lane), src + l * P + site);
-}
+// Field of a tile in shared memory: element (level l, column c) at l*8 + c.
+template <typename V> struct ZTileF {
+    V *p;
+    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZCols + c]; }
+};
 
 template <typename T, typename TS, typename TD, int NZP> struct ZfLayout {
-    static constexpr int L = NZP * kZTile;
+    static constexpr int L = ZmDims<NZP>::LV * kZCols;
     static constexpr int c = L * (int)sizeof(C2<T>), r = L * (int)sizeof(T);
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
     static constexpr int sc = L * (int)sizeof(C2<TS>), sr = L * (int)sizeof(TS);
@@ -86,8 +91,7 @@ template <typename T, typename TS, typename TD, int NZP> struct ZfLayout {
     static constexpr int oV = oX2 + x2;
     // V: dp then S1 (complex); later g and S of a gauge component (real)
     static constexpr int v = mx(c, 2 * r);
-    static constexpr int oKB = oV + v;
-    static constexpr int bytes = oKB + kZTile * (int)sizeof(T);
+    static constexpr int bytes = oV + v;
 };
 
 template <typename T, typename TS, typename TD, int NZP>
@@ -95,39 +99,99 @@ __host__ __device__ constexpr int zf_smem_bytes() {
     return ZfLayout<T, TS, TD, NZP>::bytes;
 }
 
+// Stage levels 0..nz-1 of one field of the tile starting at site0.
+template <typename V>
+__device__ __forceinline__ void zf_stage(ZTileF<V> dst, const V *src, int nz, long long P,
+                                         long long site0, int lane) {
+    if (!src) return;
+    for (int e = lane; e < nz * kZCols; e += 32) {
+        const int l = e >> 3, c = e & 7;
+        if (site0 + c < P) cp_async<sizeof(V)>(&dst(l, c), src + l * P + site0 + c);
+    }
+}
+
+// out = L V for a real tile field V (levels >= nz hold zero)
+template <int MT, int KS>
+__device__ __forceinline__ void zm_real(const double (&A)[MT][KS], ZTileF<double> V,
+                                        double (&C)[MT][2], int g, int q) {
+#pragma unroll
+    for (int m = 0; m < MT; ++m) C[m][0] = C[m][1] = 0.0;
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+        const double b = V(4 * s + q, g);
+#pragma unroll
+        for (int m = 0; m < MT; ++m) dmma(C[m][0], C[m][1], A[m][s], b);
+    }
+}
+// re/im of out = L V for a complex tile field
+template <int MT, int KS>
+__device__ __forceinline__ void zm_cplx(const double (&A)[MT][KS], ZTileF<double2> V,
+                                        double (&Cr)[MT][2], double (&Ci)[MT][2], int g, int q) {
+#pragma unroll
+    for (int m = 0; m < MT; ++m) Cr[m][0] = Cr[m][1] = Ci[m][0] = Ci[m][1] = 0.0;
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+        const double2 b = V(4 * s + q, g);
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            dmma(Cr[m][0], Cr[m][1], A[m][s], b.x);
+            dmma(Ci[m][0], Ci[m][1], A[m][s], b.y);
+        }
+    }
+}
+
+// T = TS = double (state and arithmetic); TD = double or float (derivative
+// fields of the line passes).
 template <typename T, typename TS, typename TD, int NZP, int MODE>
-__global__ void __launch_bounds__(32 * zf_warps(NZP))
+__global__ void __launch_bounds__(32)
     k_zstage(const __grid_constant__ ZStageArgs<T, TS, TD> a,
              const __grid_constant__ ZOps<T, NZP> op) {
+    static_assert(std::is_same<T, double>::value && std::is_same<TS, double>::value,
+                  "FP64 columns");
     using Lay = ZfLayout<T, TS, TD, NZP>;
-    constexpr int NW = zf_warps(NZP);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    using D = ZmDims<NZP>;
+    constexpr int MT = D::MT, KS = D::KS;
+    const int lane = threadIdx.x, g = lane >> 2, q = lane & 3;
     const int nz = a.nz;
     const long long P = a.plane;
-    const long long site = (long long)blockIdx.x * kZTile + lane;
-    const bool ok = site < P;
-    // rows i0 .. i0+kRowsPerWarp-1 of every contraction belong to this warp
-    const int i0 = warp * kRowsPerWarp;
     unsigned char *sm = g_smem;
+    // zero the tile once: padded levels must read as 0 in every product
+    for (int i = lane; i < Lay::bytes / 16; i += 32)
+        reinterpret_cast<double2 *>(sm)[i] = make_double2(0.0, 0.0);
+    // operator fragments (padded rows and columns of op are zero)
+    double ALz[MT][KS], ALz1[MT][KS];
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            const int i = 8 * m + g, j = 4 * s + q;
+            const bool in = (i < NZP) && (j < NZP);
+            ALz[m][s] = in ? op.Lz[in ? i : 0][in ? j : 0] : 0.0;
+            ALz1[m][s] = in ? op.Lz1[in ? i : 0][in ? j : 0] : 0.0;
+        }
+    double zr[MT], fzr[MT];  // z and f = 1 - z^3 at this lane's levels
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+        const int i = 8 * m + g;
+        zr[m] = i < NZP ? op.zz[i < NZP ? i : 0] : 0.0;
+        fzr[m] = i < NZP ? op.fz[i < NZP ? i : 0] : 0.0;
+    }
+    __syncwarp();
+
     const ZTileF<C2<T>> PS{reinterpret_cast<C2<T> *>(sm + Lay::oPS)};
     const ZTileF<T> AX{reinterpret_cast<T *>(sm + Lay::oAX)};
     const ZTileF<T> AY{reinterpret_cast<T *>(sm + Lay::oAY)};
     const ZTileF<C2<TD>> DXP{reinterpret_cast<C2<TD> *>(sm + Lay::oDXP)};
     const ZTileF<C2<TD>> DYP{reinterpret_cast<C2<TD> *>(sm + Lay::oDYP)};
-    // X1, phase P2
     const ZTileF<T> AT{reinterpret_cast<T *>(sm + Lay::oX1)};
     const ZTileF<T> DAT{reinterpret_cast<T *>(sm + Lay::oX1 + Lay::r)};
     const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(sm + Lay::oX1 + 2 * Lay::r)};
     const ZTileF<TD> DIV{reinterpret_cast<TD *>(sm + Lay::oX1 + 2 * Lay::r + Lay::dc)};
-    // X2, phase P3
     const ZTileF<C2<TS>> ZP{reinterpret_cast<C2<TS> *>(sm + Lay::oX2)};
     const ZTileF<C2<TS>> KP{reinterpret_cast<C2<TS> *>(sm + Lay::oX2 + Lay::sc)};
-    // V
     const ZTileF<C2<T>> VC{reinterpret_cast<C2<T> *>(sm + Lay::oV)};
     const ZTileF<T> VG{reinterpret_cast<T *>(sm + Lay::oV)};
     const ZTileF<T> VS{reinterpret_cast<T *>(sm + Lay::oV + Lay::r)};
-    T *KB = reinterpret_cast<T *>(sm + Lay::oKB);
-    // gauge-component inputs inside X1 (A_x) or X2 (A_y)
     auto gauge_tiles = [&](int off, ZTileF<TD> &dt, ZTileF<TD> &bf, ZTileF<TS> &za,
                            ZTileF<TS> &ka) {
         dt.p = reinterpret_cast<TD *>(sm + off);
@@ -136,303 +200,259 @@ __global__ void __launch_bounds__(32 * zf_warps(NZP))
         ka.p = reinterpret_cast<TS *>(sm + off + 2 * Lay::dr + Lay::sr);
     };
     constexpr bool kReadK = (MODE >= 2);
-    auto stage_gauge = [&](int comp, int off) {
-        ZTileF<TD> dt, bf;
-        ZTileF<TS> za, ka;
-        gauge_tiles(off, dt, bf, za, ka);
-        zf_stage<TD, NW>(dt, comp == 0 ? a.dxat : a.dyat, nz, P, site, ok, warp, lane);
-        zf_stage<TD, NW>(bf, comp == 0 ? a.dyB : a.dxB, nz, P, site, ok, warp, lane);
-        if (MODE >= 1) {
-            zf_stage<TS, NW>(za, comp == 0 ? a.zax : a.zay, nz, P, site, ok, warp, lane);
-            if (kReadK)
-                zf_stage<TS, NW>(ka, comp == 0 ? a.kax : a.kay, nz, P, site, ok, warp, lane);
-        }
-    };
 
-    // ---- G0, G1 ------------------------------------------------------------
-    zf_stage<C2<T>, NW>(PS, a.ypsi, nz, P, site, ok, warp, lane);
-    zf_stage<T, NW>(AX, a.yax, nz, P, site, ok, warp, lane);
-    zf_stage<T, NW>(AY, a.yay, nz, P, site, ok, warp, lane);
-    zf_stage<C2<TD>, NW>(DXP, a.dxpsi, nz, P, site, ok, warp, lane);
-    zf_stage<C2<TD>, NW>(DYP, a.dypsi, nz, P, site, ok, warp, lane);
-    zf_stage<T, NW>(AT, a.at, nz, P, site, ok, warp, lane);
-    zf_stage<T, NW>(DAT, a.dat, nz, P, site, ok, warp, lane);
-    zf_stage<C2<TD>, NW>(LAP, a.lap, nz, P, site, ok, warp, lane);
-    zf_stage<TD, NW>(DIV, a.divA, nz, P, site, ok, warp, lane);
-    cp_commit();
-    if (MODE >= 1) {
-        zf_stage<C2<TS>, NW>(ZP, a.zpsi, nz, P, site, ok, warp, lane);
-        if (kReadK) zf_stage<C2<TS>, NW>(KP, a.kpsi, nz, P, site, ok, warp, lane);
-    }
-    cp_commit();
-    cp_wait<1>();
-    __syncthreads();
-
-    // ---- P1: dp = Lz Psi ---------------------------------------------------
-    {
-        C2<T> acc[kRowsPerWarp];
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = mk2<T>(T(0), T(0));
-#pragma unroll
-        for (int j = 0; j < NZP; ++j) {
-            if (j < nz) {
-                const C2<T> v = PS(j, lane);
-#pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r) {
-                    if (i0 + r < NZP) {
-                        const T c = op.Lz[i0 + r][j];
-                        acc[r].x = fma(c, v.x, acc[r].x);
-                        acc[r].y = fma(c, v.y, acc[r].y);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r)
-            if (i0 + r < NZP) VC(i0 + r, lane) = acc[r];
-    }
-    __syncthreads();
-
-    // ---- P2: d2 = Lz dp and S1; the boundary row of F2 ----------------------
-    if (warp == 0) {
-        T kb = T(0);
-#pragma unroll
-        for (int i = 0; i < NZP; ++i)
-            if (i < nz) kb = fma(op.lzb[i], T(DIV(i, lane)), kb);
-        KB[lane] = kb;
-    }
-    C2<T> s1[kRowsPerWarp];
-    {
-        T d2r[kRowsPerWarp], d2i[kRowsPerWarp];
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) d2r[r] = d2i[r] = T(0);
-#pragma unroll
-        for (int j = 0; j < NZP; ++j) {
-            const C2<T> v = VC(j, lane);  // rows >= nz hold zero sums
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                if (i0 + r < NZP) {
-                    const T c = op.Lz[i0 + r][j];
-                    d2r[r] = fma(c, v.x, d2r[r]);
-                    d2i[r] = fma(c, v.y, d2i[r]);
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) {
-            const int i = i0 + r;
-            s1[r] = mk2<T>(T(0), T(0));
-            if (i < NZP && i < nz - 1) {
-                const C2<T> ps = PS(i, lane);
-                const T at = AT(i, lane), dat = DAT(i, lane), ax = AX(i, lane), ay = AY(i, lane);
-                const C2<TD> lpd = LAP(i, lane), dxd = DXP(i, lane), dyd = DYP(i, lane);
-                const C2<T> lp = mk2<T>(T(lpd.x), T(lpd.y)), dx = mk2<T>(T(dxd.x), T(dxd.y));
-                const C2<T> dy = mk2<T>(T(dyd.x), T(dyd.y));
-                const T dv = T(DIV(i, lane));
-                const T z = op.zz[i], f = op.fz[i];
-                const C2<T> d1 = VC(i, lane);
-                const T h = T(0.5);
-                const T a2 = ax * ax + ay * ay;
-                const T u = ax * dx.x + ay * dy.x;
-                const T w = ax * dx.y + ay * dy.y;
-                s1[r].x = -at * d1.y - h * dat * ps.y + h * f * d2r[r] -
-                          T(1.5) * z * z * d1.x - h * z * ps.x - h * a2 * ps.x + h * lp.x +
-                          h * dv * ps.y + w;
-                s1[r].y = at * d1.x + h * dat * ps.x + h * f * d2i[r] -
-                          T(1.5) * z * z * d1.y - h * z * ps.y - h * a2 * ps.y + h * lp.y -
-                          h * dv * ps.x - u;
-            }
-        }
-    }
-    __syncthreads();  // every read of dp and of X1 is done
-#pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r)
-        if (i0 + r < NZP) VC(i0 + r, lane) = s1[r];
-    stage_gauge(0, Lay::oX1);  // G2
-    cp_commit();
-    cp_wait<1>();  // G1
-    __syncthreads();
-
-    // ---- P3: F1 = Lzr(S1) and the RK update of Psi ----------------------------
-    {
-        T fr[kRowsPerWarp], fi[kRowsPerWarp];
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) fr[r] = fi[r] = T(0);
-#pragma unroll
-        for (int j = 0; j < NZP; ++j) {
-            const C2<T> v = VC(j, lane);
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                if (i0 + r < NZP) {
-                    const T c = op.Lz1[i0 + r][j];
-                    fr[r] = fma(c, v.x, fr[r]);
-                    fi[r] = fma(c, v.y, fi[r]);
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) {
-            const int i = i0 + r;
-            if (!ok || i >= NZP || i >= nz) continue;
-            const long long g = (long long)i * P + site;
-            if (MODE == 0) {
-                a.f1[g] = mk2<T>(fr[r], fi[r]);
-                continue;
-            }
-            const C2<TS> k = mk2<TS>(a.h * TS(fr[r]), a.h * TS(fi[r]));
-            const C2<TS> z = ZP(i, lane);
-            if (MODE == 4) {
-                const C2<TS> K = KP(i, lane);
-                const TS s = TS(1) / TS(6);
-                a.wpsi[g] = mk2<TS>(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
-                continue;
-            }
-            if (MODE == 1) {
-                a.kpsi[g] = k;
-            } else {
-                const C2<TS> K = KP(i, lane);
-                a.kpsi[g] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
-            }
-            const C2<TS> nv = (MODE == 3) ? mk2<TS>(z.x + k.x, z.y + k.y)
-                                          : mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
-            a.npsi[g] = mk2<T>(T(nv.x), T(nv.y));
-            if (a.npsi_d) {
-                const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
-                const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
-                a.npsi_d[g] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
-            }
-        }
-    }
-    if (warp == 0 && ok) {
-        const T kb = KB[lane];
-        if (MODE == 0) {
-            a.f2b[site] = kb;
-        } else if (!a.f2x) {
-            const TS k = a.h * TS(kb);
-            if (MODE == 1)
-                a.krho[site] = k;
-            else if (MODE == 2 || MODE == 3)
-                a.krho[site] = a.krho[site] + 2 * k;
-            else  // rhoi = rhoi - k2(:,:,nz), k2 = (1/6)(k21+2k22+2k23+k24)
-                a.wrho[site] = a.zrho[site] - (TS(1) / TS(6)) * (a.krho[site] + k);
-        }
-    }
-    __syncthreads();  // X2 and V are free
-    stage_gauge(1, Lay::oX2);  // G3
-    cp_commit();
-
-    // ---- P4: F3 (A_x), then F4 (A_y) ----------------------------------------
+    const long long ntiles = (P + kZCols - 1) / kZCols;
 #pragma unroll 1
-    for (int comp = 0; comp < 2; ++comp) {
-        if (comp == 0)
-            cp_wait<1>();  // G2
-        else
-            cp_wait<0>();  // G3
-        __syncthreads();
-        ZTileF<TD> DT, BF;
-        ZTileF<TS> ZA, KA;
-        gauge_tiles(comp == 0 ? Lay::oX1 : Lay::oX2, DT, BF, ZA, KA);
-        const ZTileF<T> A = comp == 0 ? AX : AY;
-        const ZTileF<C2<TD>> DPS = comp == 0 ? DXP : DYP;
-        // boundary-row contraction Lz(nz,:) A (mixed precision forms F2 from it)
-        if (a.f2x && warp == NW - 1 && ok) {
-            T bnd = T(0);
-#pragma unroll
-            for (int j = 0; j < NZP; ++j)
-                if (j < nz) bnd = fma(op.lzb[j], A(j, lane), bnd);
-            (comp == 0 ? a.f2x : a.f2y)[site] = bnd;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long site0 = tile * kZCols;
+        auto stage_gauge = [&](int comp, int off) {
+            ZTileF<TD> dt, bf;
+            ZTileF<TS> za, ka;
+            gauge_tiles(off, dt, bf, za, ka);
+            zf_stage<TD>(dt, comp == 0 ? a.dxat : a.dyat, nz, P, site0, lane);
+            zf_stage<TD>(bf, comp == 0 ? a.dyB : a.dxB, nz, P, site0, lane);
+            if (MODE >= 1) {
+                zf_stage<TS>(za, comp == 0 ? a.zax : a.zay, nz, P, site0, lane);
+                if (kReadK) zf_stage<TS>(ka, comp == 0 ? a.kax : a.kay, nz, P, site0, lane);
+            }
+        };
+
+        // ---- G0, G1 --------------------------------------------------------
+        zf_stage<C2<T>>(PS, a.ypsi, nz, P, site0, lane);
+        zf_stage<T>(AX, a.yax, nz, P, site0, lane);
+        zf_stage<T>(AY, a.yay, nz, P, site0, lane);
+        zf_stage<C2<TD>>(DXP, a.dxpsi, nz, P, site0, lane);
+        zf_stage<C2<TD>>(DYP, a.dypsi, nz, P, site0, lane);
+        zf_stage<T>(AT, a.at, nz, P, site0, lane);
+        zf_stage<T>(DAT, a.dat, nz, P, site0, lane);
+        zf_stage<C2<TD>>(LAP, a.lap, nz, P, site0, lane);
+        zf_stage<TD>(DIV, a.divA, nz, P, site0, lane);
+        cp_commit();
+        if (MODE >= 1) {
+            zf_stage<C2<TS>>(ZP, a.zpsi, nz, P, site0, lane);
+            if (kReadK) zf_stage<C2<TS>>(KP, a.kpsi, nz, P, site0, lane);
         }
-        // g = d A_t + f Lz A
+        cp_commit();
+        cp_wait<1>();
+        __syncwarp();
+
+        // ---- P1: dp = Lz Psi -------------------------------------------------
         {
-            T g[kRowsPerWarp];
+            double cr[MT][2], ci[MT][2];
+            zm_cplx<MT, KS>(ALz, PS, cr, ci, g, q);
+            __syncwarp();
 #pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) g[r] = T(0);
+            for (int m = 0; m < MT; ++m)
 #pragma unroll
-            for (int j = 0; j < NZP; ++j) {
-                if (j < nz) {
-                    const T v = A(j, lane);
-#pragma unroll
-                    for (int r = 0; r < kRowsPerWarp; ++r)
-                        if (i0 + r < NZP) g[r] = fma(op.Lz[i0 + r][j], v, g[r]);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                const int i = i0 + r;
-                if (i < NZP) VG(i, lane) = (i < nz) ? T(DT(i, lane)) + op.fz[i] * g[r] : T(0);
-            }
+                for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(cr[m][h], ci[m][h]);
         }
-        __syncthreads();
-        // S = 1/2 Lz g -/+ 1/2 d B + Im(conj(Psi) d Psi) - A |Psi|^2
+        __syncwarp();
+
+        // ---- P2: d2 = Lz dp, S1, and the boundary row of F2 ------------------
+        T kb = T(0);  // lanes 0..7: column `lane`
+        if (lane < kZCols) {
+#pragma unroll
+            for (int i = 0; i < NZP; ++i)
+                if (i < nz) kb = fma(op.lzb[i], T(DIV(i, lane)), kb);
+        }
+        double s1r[MT][2], s1i[MT][2];
         {
-            T d[kRowsPerWarp];
+            double d2r[MT][2], d2i[MT][2];
+            zm_cplx<MT, KS>(ALz, VC, d2r, d2i, g, q);
 #pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) d[r] = T(0);
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
 #pragma unroll
-            for (int j = 0; j < NZP; ++j) {
-                const T v = VG(j, lane);
-#pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r)
-                    if (i0 + r < NZP) d[r] = fma(op.Lz[i0 + r][j], v, d[r]);
-            }
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                const int i = i0 + r;
-                if (i < NZP) {
-                    T s = T(0);
-                    if (i < nz) {
-                        const C2<T> ps = PS(i, lane);
-                        const C2<TD> ddd = DPS(i, lane);
-                        const C2<T> dd = mk2<T>(T(ddd.x), T(ddd.y));
-                        const T bf = comp == 0 ? -T(BF(i, lane)) : T(BF(i, lane));
-                        const T av = A(i, lane);
-                        s = T(0.5) * d[r] + T(0.5) * bf + (ps.x * dd.y - ps.y * dd.x) -
-                            av * (ps.x * ps.x + ps.y * ps.y);
+                for (int h = 0; h < 2; ++h) {
+                    const int cc = 2 * q + h;
+                    s1r[m][h] = s1i[m][h] = 0.0;
+                    if (i < nz - 1) {
+                        const C2<T> ps = PS(i, cc);
+                        const T at = AT(i, cc), dat = DAT(i, cc), ax = AX(i, cc), ay = AY(i, cc);
+                        const C2<TD> lpd = LAP(i, cc), dxd = DXP(i, cc), dyd = DYP(i, cc);
+                        const T dv = T(DIV(i, cc));
+                        const C2<T> d1 = VC(i, cc);
+                        const T z = zr[m], f = fzr[m], hh = T(0.5);
+                        const T a2 = ax * ax + ay * ay;
+                        const T u = ax * T(dxd.x) + ay * T(dyd.x);
+                        const T w = ax * T(dxd.y) + ay * T(dyd.y);
+                        s1r[m][h] = -at * d1.y - hh * dat * ps.y + hh * f * d2r[m][h] -
+                                    T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
+                                    hh * T(lpd.x) + hh * dv * ps.y + w;
+                        s1i[m][h] = at * d1.x + hh * dat * ps.x + hh * f * d2i[m][h] -
+                                    T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
+                                    hh * T(lpd.y) - hh * dv * ps.x - u;
                     }
-                    VS(i, lane) = s;
                 }
             }
         }
-        __syncthreads();
-        // F = Lzr(S) (rows < nz-1 of Lz1, zero on the boundary row) and the update
+        __syncwarp();  // every read of dp and of X1 is done
+#pragma unroll
+        for (int m = 0; m < MT; ++m)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(s1r[m][h], s1i[m][h]);
+        stage_gauge(0, Lay::oX1);  // G2
+        cp_commit();
+        cp_wait<1>();  // G1
+        __syncwarp();
+
+        // ---- P3: F1 = Lzr(S1) and the RK update of Psi --------------------------
         {
-            T fr[kRowsPerWarp];
+            double fr[MT][2], fi[MT][2];
+            zm_cplx<MT, KS>(ALz1, VC, fr, fi, g, q);
 #pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) fr[r] = T(0);
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
 #pragma unroll
-            for (int j = 0; j < NZP; ++j) {
-                const T v = VS(j, lane);
-#pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r)
-                    if (i0 + r < NZP) fr[r] = fma(op.Lz1[i0 + r][j], v, fr[r]);
-            }
-#pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                const int i = i0 + r;
-                if (!ok || i >= NZP || i >= nz) continue;
-                const long long gi = (long long)i * P + site;
-                if (MODE == 0) {
-                    (comp == 0 ? a.f3 : a.f4)[gi] = fr[r];
-                    continue;
-                }
-                const TS k = a.h * TS(fr[r]);
-                const TS z = ZA(i, lane);
-                if (MODE == 4) {
-                    (comp == 0 ? a.wax : a.way)[gi] = z + (TS(1) / TS(6)) * (KA(i, lane) + k);
-                    continue;
-                }
-                TS *kacc = comp == 0 ? a.kax : a.kay;
-                kacc[gi] = (MODE == 1) ? k : KA(i, lane) + 2 * k;
-                const TS nv = (MODE == 3) ? z + k : z + k / 2;
-                (comp == 0 ? a.nax : a.nay)[gi] = T(nv);
-                TD *nd = comp == 0 ? a.nax_d : a.nay_d;
-                if (nd) {
-                    const TS mean = a.slice_mean ? a.slice_mean[5 * i + 3 + comp] : TS(0);
-                    nd[gi] = TD(nv - mean);
+                for (int h = 0; h < 2; ++h) {
+                    const int cc = 2 * q + h;
+                    const long long site = site0 + cc;
+                    if (i >= nz || site >= P) continue;
+                    const long long gi = (long long)i * P + site;
+                    if (MODE == 0) {
+                        a.f1[gi] = mk2<T>(fr[m][h], fi[m][h]);
+                        continue;
+                    }
+                    const C2<TS> k = mk2<TS>(a.h * TS(fr[m][h]), a.h * TS(fi[m][h]));
+                    const C2<TS> z = ZP(i, cc);
+                    if (MODE == 4) {
+                        const C2<TS> K = KP(i, cc);
+                        const TS s = TS(1) / TS(6);
+                        a.wpsi[gi] = mk2<TS>(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
+                        continue;
+                    }
+                    if (MODE == 1) {
+                        a.kpsi[gi] = k;
+                    } else {
+                        const C2<TS> K = KP(i, cc);
+                        a.kpsi[gi] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
+                    }
+                    const C2<TS> nv = (MODE == 3) ? mk2<TS>(z.x + k.x, z.y + k.y)
+                                                  : mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
+                    a.npsi[gi] = mk2<T>(T(nv.x), T(nv.y));
+                    if (a.npsi_d) {
+                        const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
+                        const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
+                        a.npsi_d[gi] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
+                    }
                 }
             }
         }
-        __syncthreads();  // V is reused by the next component
+        if (lane < kZCols && site0 + lane < P) {
+            const long long site = site0 + lane;
+            if (MODE == 0) {
+                a.f2b[site] = kb;
+            } else if (!a.f2x) {
+                const TS k = a.h * TS(kb);
+                if (MODE == 1)
+                    a.krho[site] = k;
+                else if (MODE == 2 || MODE == 3)
+                    a.krho[site] = a.krho[site] + 2 * k;
+                else  // rhoi = rhoi - k2(:,:,nz), k2 = (1/6)(k21+2k22+2k23+k24)
+                    a.wrho[site] = a.zrho[site] - (TS(1) / TS(6)) * (a.krho[site] + k);
+            }
+        }
+        __syncwarp();  // X2 and V are free
+        stage_gauge(1, Lay::oX2);  // G3
+        cp_commit();
+
+        // ---- P4: F3 (A_x), then F4 (A_y) ------------------------------------
+#pragma unroll 1
+        for (int comp = 0; comp < 2; ++comp) {
+            if (comp == 0)
+                cp_wait<1>();  // G2
+            else
+                cp_wait<0>();  // G3
+            __syncwarp();
+            ZTileF<TD> DT, BF;
+            ZTileF<TS> ZA, KA;
+            gauge_tiles(comp == 0 ? Lay::oX1 : Lay::oX2, DT, BF, ZA, KA);
+            const ZTileF<T> A = comp == 0 ? AX : AY;
+            const ZTileF<C2<TD>> DPS = comp == 0 ? DXP : DYP;
+            // boundary-row contraction Lz(nz,:) A (mixed precision forms F2 from it)
+            if (a.f2x && lane < kZCols && site0 + lane < P) {
+                T bnd = T(0);
+#pragma unroll
+                for (int j = 0; j < NZP; ++j)
+                    if (j < nz) bnd = fma(op.lzb[j], A(j, lane), bnd);
+                (comp == 0 ? a.f2x : a.f2y)[site0 + lane] = bnd;
+            }
+            // g = d A_t + f Lz A
+            {
+                double c[MT][2];
+                zm_real<MT, KS>(ALz, A, c, g, q);
+#pragma unroll
+                for (int m = 0; m < MT; ++m) {
+                    const int i = 8 * m + g;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        VG(i, 2 * q + h) = (i < nz) ? T(DT(i, 2 * q + h)) + fzr[m] * c[m][h] : T(0);
+                }
+            }
+            __syncwarp();
+            // S = 1/2 Lz g -/+ 1/2 d B + Im(conj(Psi) d Psi) - A |Psi|^2
+            {
+                double d[MT][2];
+                zm_real<MT, KS>(ALz, VG, d, g, q);
+#pragma unroll
+                for (int m = 0; m < MT; ++m) {
+                    const int i = 8 * m + g;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int cc = 2 * q + h;
+                        T s = T(0);
+                        if (i < nz) {
+                            const C2<T> ps = PS(i, cc);
+                            const C2<TD> ddd = DPS(i, cc);
+                            const T bf = comp == 0 ? -T(BF(i, cc)) : T(BF(i, cc));
+                            const T av = A(i, cc);
+                            s = T(0.5) * d[m][h] + T(0.5) * bf +
+                                (ps.x * T(ddd.y) - ps.y * T(ddd.x)) -
+                                av * (ps.x * ps.x + ps.y * ps.y);
+                        }
+                        VS(i, cc) = s;
+                    }
+                }
+            }
+            __syncwarp();
+            // F = Lzr(S) (rows < nz-1 of Lz1, zero on the boundary row) and the update
+            {
+                double fr[MT][2];
+                zm_real<MT, KS>(ALz1, VS, fr, g, q);
+#pragma unroll
+                for (int m = 0; m < MT; ++m) {
+                    const int i = 8 * m + g;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int cc = 2 * q + h;
+                        const long long site = site0 + cc;
+                        if (i >= nz || site >= P) continue;
+                        const long long gi = (long long)i * P + site;
+                        if (MODE == 0) {
+                            (comp == 0 ? a.f3 : a.f4)[gi] = fr[m][h];
+                            continue;
+                        }
+                        const TS k = a.h * TS(fr[m][h]);
+                        const TS z = ZA(i, cc);
+                        if (MODE == 4) {
+                            (comp == 0 ? a.wax : a.way)[gi] = z + (TS(1) / TS(6)) * (KA(i, cc) + k);
+                            continue;
+                        }
+                        TS *kacc = comp == 0 ? a.kax : a.kay;
+                        kacc[gi] = (MODE == 1) ? k : KA(i, cc) + 2 * k;
+                        const TS nv = (MODE == 3) ? z + k : z + k / 2;
+                        (comp == 0 ? a.nax : a.nay)[gi] = T(nv);
+                        TD *nd = comp == 0 ? a.nax_d : a.nay_d;
+                        if (nd) {
+                            const TS mean =
+                                a.slice_mean ? a.slice_mean[5 * i + 3 + comp] : TS(0);
+                            nd[gi] = TD(nv - mean);
+                        }
+                    }
+                }
+            }
+            __syncwarp();  // V is reused next
+        }
     }
 }
 
