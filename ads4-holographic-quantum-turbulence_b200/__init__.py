@@ -8,8 +8,8 @@ import it with ``importlib.import_module("ads4-holographic-quantum-turbulence_b2
 """
 from . import seed
 from ._lib import HQTError, NonfiniteEvolution
-from .api import Simulation, StepInfo, from_device, to_device
+from .api import Ensemble, Simulation, StepInfo, assign_runs, from_device, to_device
 from .checkpoint import load_checkpoint, save_checkpoint
 
-__all__ = ["Simulation", "StepInfo", "HQTError", "NonfiniteEvolution", "seed",
+__all__ = ["Simulation", "Ensemble", "assign_runs", "StepInfo", "HQTError", "NonfiniteEvolution", "seed",
            "to_device", "from_device", "save_checkpoint", "load_checkpoint"]

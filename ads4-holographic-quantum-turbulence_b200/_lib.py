@@ -31,6 +31,8 @@ EXPORTS = [
     "hqt_profile", "hqt_profile_report",
     "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
     "hqt_energy_spectrum_device",
+    "hqt_ensemble_create", "hqt_ensemble_destroy", "hqt_ensemble_set_stream",
+    "hqt_ensemble_last_error", "hqt_ensemble_step_device",
 ]
 
 
@@ -103,6 +105,12 @@ def load() -> ctypes.CDLL:
         "hqt_noalloc_last_error": (c_char_p, []),
         "hqt_energy_spectrum_device": (c_int, [c_void_p, c_void_p, c_int32, dp, dp, dp,
                                                dp, ip]),
+        "hqt_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
+        "hqt_ensemble_destroy": (None, [c_void_p]),
+        "hqt_ensemble_set_stream": (c_int, [c_void_p, c_void_p]),
+        "hqt_ensemble_last_error": (c_char_p, [c_void_p]),
+        "hqt_ensemble_step_device": (c_int, [c_void_p] + [POINTER(c_void_p)] * 5
+                                     + [c_int64, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

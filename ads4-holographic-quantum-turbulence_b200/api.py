@@ -22,7 +22,8 @@ import numpy as np
 from . import _lib
 from ._lib import HQT_FP64, HQT_MIXED, HQTError, NonfiniteEvolution, check
 
-__all__ = ["Simulation", "StepInfo", "HQTError", "NonfiniteEvolution"]
+__all__ = ["Simulation", "Ensemble", "StepInfo", "HQTError", "NonfiniteEvolution",
+           "assign_runs"]
 
 
 @dataclass
@@ -285,6 +286,98 @@ class Simulation:
         self._check(self._lib.hqt_count_vortices_device(
             self._ctx, ptr, ctypes.byref(n), ctypes.byref(p), ctypes.byref(m)))
         return int(n.value), int(p.value), int(m.value)
+
+
+class Ensemble:
+    """Independent runs advanced together (``hqt_ensemble_*`` of the C ABI).
+
+    The reference runs one simulation per MATLAB session; a parameter scan
+    (grids, ``nz``, ``mu``, seeds) is many such runs.  ``Ensemble`` groups
+    :class:`Simulation` objects of one GPU and advances all of them with one
+    CUDA-graph launch per step: each member's captured step graph is a child
+    node of the ensemble graph, with no dependencies between members.  The
+    members stay owned by the caller and must outlive the ensemble.
+    """
+
+    def __init__(self, members):
+        self.members = list(members)
+        if not self.members:
+            raise ValueError("an ensemble needs members")
+        self._lib = _lib.load()
+        arr = (ctypes.c_void_p * len(self.members))(*[m._ctx for m in self.members])
+        h = ctypes.c_void_p()
+        code = self._lib.hqt_ensemble_create(arr, len(self.members), ctypes.byref(h))
+        if code:
+            raise HQTError(code, self._lib.hqt_ensemble_last_error(None).decode())
+        self._ens = h
+
+    def close(self) -> None:
+        if getattr(self, "_ens", None):
+            self._lib.hqt_ensemble_destroy(self._ens)
+            self._ens = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step_device(self, states, nsteps: int = 1) -> list[StepInfo]:
+        """Advance every member ``nsteps`` RK4 steps in place.  ``states[i]``
+        is member i's ``(Z1, Z2, Z3, Z4, rhoi)`` as CUDA tensors of shape
+        ``(nz, ny, nx)``.  Raises :class:`NonfiniteEvolution` (with ``.info``,
+        one :class:`StepInfo` per member) when a member's fields became
+        non-finite."""
+        import torch
+        if len(states) != len(self.members):
+            raise ValueError("one state per member")
+        cols = [[], [], [], [], []]
+        for m, st in zip(self.members, states):
+            ptrs = [m._dev3(st[0], True), m._dev3(st[1]), m._dev3(st[2]),
+                    m._dev3(st[3]), m._dev3(st[4])]
+            for c, p in zip(cols, ptrs):
+                c.append(p.value)
+        arrs = [(ctypes.c_void_p * len(c))(*c) for c in cols]
+        diags = (_lib.hqt_diag * len(self.members))()
+        # the graph runs on torch's current stream when it is a side stream
+        # (the legacy default stream cannot hold graph launches ordered with
+        # torch's work, so the device is synchronised instead)
+        s = torch.cuda.current_stream(self.members[0].device).cuda_stream
+        self._lib.hqt_ensemble_set_stream(self._ens, ctypes.c_void_p(s or None))
+        torch.cuda.synchronize(self.members[0].device)
+        code = self._lib.hqt_ensemble_step_device(self._ens, *arrs, int(nsteps), diags)
+        infos = [StepInfo(int(d.steps_done), int(d.nonfinite_step), int(d.last_winding))
+                 for d in diags]
+        if code:
+            msg = self._lib.hqt_ensemble_last_error(self._ens).decode()
+            err = (NonfiniteEvolution(code, msg) if code == _lib.HQT_ENONFINITE
+                   else HQTError(code, msg))
+            err.info = infos
+            raise err
+        return infos
+
+
+def assign_runs(costs, world_size: int) -> list[list[int]]:
+    """Bin-pack independent runs onto ``world_size`` GPUs: longest run
+    first onto the least-loaded GPU (costs are site counts or any additive
+    work measure).  Returns the run indices of each rank, each list in
+    ascending order; every run appears exactly once."""
+    if world_size < 1:
+        raise ValueError("world_size must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world_size
+    out: list[list[int]] = [[] for _ in range(world_size)]
+    for i in order:
+        r = min(range(world_size), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
 
 
 def to_device(a: np.ndarray, device: int = 0):

@@ -1469,4 +1469,209 @@ int hqt_count_vortices(hqt_ctx *c, const double *O, int32_t *n, int32_t *np, int
     return count_vortices_dev(c, c->O, n, np, nm);
 }
 
+
+// ---------------------------------------------------------------- ensembles
+// Independent runs (each its own context: grid, nz, mu, seed, precision)
+// advanced together.  Each member's step is its captured step graph; the
+// ensemble graph holds one child-graph node per member with no edges between
+// them, so a single cudaGraphLaunch advances every member one step and the
+// members' kernels overlap on the device.
+
+}  // extern "C"
+
+struct hqt_ensemble {
+    std::vector<hqt_ctx *> m;
+    int device = 0;
+    cudaStream_t stream = nullptr;  // launch stream (own or the caller's)
+    cudaStream_t own = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<cudaGraph_t> key;  // member graphs the ensemble graph holds copies of
+    std::string err;
+};
+
+namespace {
+
+int efail(hqt_ensemble *e, int code, const std::string &msg) {
+    if (e)
+        e->err = msg;
+    else
+        g_create_err = msg;
+    return code;
+}
+
+#define EK(call)                                                                       \
+    do {                                                                               \
+        const cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                       \
+            cudaGetLastError();                                                        \
+            return efail(e, HQT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+        }                                                                              \
+    } while (0)
+
+void drop_ensemble_graph(hqt_ensemble *e) {
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+    e->key.clear();
+}
+
+int build_ensemble_graph(hqt_ensemble *e) {
+    std::vector<cudaGraph_t> key;
+    for (hqt_ctx *c : e->m) key.push_back(c->graph);
+    if (e->gexec && key == e->key) return HQT_OK;
+    drop_ensemble_graph(e);
+    EK(cudaGraphCreate(&e->graph, 0));
+    for (hqt_ctx *c : e->m) {
+        cudaGraphNode_t node;
+        EK(cudaGraphAddChildGraphNode(&node, e->graph, nullptr, 0, c->graph));
+    }
+    EK(cudaGraphInstantiate(&e->gexec, e->graph, 0));
+    e->key = key;
+    return HQT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hqt_ensemble_create(hqt_ctx *const *members, int32_t n, hqt_ensemble **out) {
+    if (!out) return efail(nullptr, HQT_EINVAL, "bad argument");
+    *out = nullptr;
+    if (!members || n < 1) return efail(nullptr, HQT_EINVAL, "an ensemble needs members");
+    auto *e = new hqt_ensemble();
+    for (int i = 0; i < n; ++i) {
+        hqt_ctx *c = members[i];
+        const bool dup = std::find(e->m.begin(), e->m.end(), c) != e->m.end();
+        if (!c || dup || (i > 0 && c->device != e->device)) {
+            delete e;
+            return efail(nullptr, HQT_EINVAL,
+                         "ensemble members must be distinct contexts on one device");
+        }
+        if (i == 0) e->device = c->device;
+        e->m.push_back(c);
+    }
+    DeviceGuard guard(e->device);
+    if (cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete e;
+        return efail(nullptr, HQT_ECUDA, "stream creation failed");
+    }
+    e->stream = e->own;
+    *out = e;
+    return HQT_OK;
+}
+
+int hqt_ensemble_set_stream(hqt_ensemble *e, void *s) {
+    if (!e) return HQT_EINVAL;
+    e->stream = s ? (cudaStream_t)s : e->own;
+    return HQT_OK;
+}
+
+void hqt_ensemble_destroy(hqt_ensemble *e) {
+    if (!e) return;
+    DeviceGuard guard(e->device);
+    drop_ensemble_graph(e);
+    if (e->own) cudaStreamDestroy(e->own);
+    delete e;
+}
+
+const char *hqt_ensemble_last_error(const hqt_ensemble *e) {
+    return e ? e->err.c_str() : g_create_err.c_str();
+}
+
+int hqt_ensemble_step_device(hqt_ensemble *e, void *const *dZ1, void *const *dZ2,
+                             void *const *dZ3, void *const *dZ4, void *const *drhoi,
+                             int64_t nsteps, hqt_diag *diags) {
+    if (!e) return HQT_EINVAL;
+    if (!dZ1 || !dZ2 || !dZ3 || !dZ4 || !drhoi || nsteps < 0)
+        return efail(e, HQT_EINVAL, "bad argument");
+    const size_t n = e->m.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (!dZ1[i] || !dZ2[i] || !dZ3[i] || !dZ4[i] || !drhoi[i])
+            return efail(e, HQT_EINVAL, "bad argument");
+        if (!aligned_fields(dZ1[i], dZ2[i], dZ3[i], dZ4[i]) ||
+            reinterpret_cast<uintptr_t>(drhoi[i]) % 8 != 0)
+            return efail(e, HQT_EINVAL, "device arrays must be aligned to their element size");
+    }
+    DeviceGuard guard(e->device);
+    // per member: state pointers, status, rhoi boundary slice, d_z A_t, step graph
+    std::vector<long long> step0(n);
+    for (size_t i = 0; i < n; ++i) {
+        hqt_ctx *c = e->m[i];
+        c->cpsi = (double2 *)dZ1[i];
+        c->cat = (double *)dZ2[i];
+        c->cax = (double *)dZ3[i];
+        c->cay = (double *)dZ4[i];
+        DevStatus h0{};
+        int r = HQT_OK;
+        auto member = [&]() -> int {
+            CK(cudaMemcpyAsync(&h0, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            step0[i] = h0.step;
+            h0.first_bad_step = LLONG_MAX;
+            h0.winding = 0;
+            CK(cudaMemcpyAsync(c->st, &h0, sizeof(DevStatus), cudaMemcpyHostToDevice, c->stream));
+            {
+                Prof pr(c, K_RHO);
+                k_rho_gather<<<296, 256, 0, c->stream>>>((const double *)drhoi[i], c->nz,
+                                                         c->plane, c->rho);
+                CK(cudaGetLastError());
+            }
+            RC(launch_zcol_misc(c, c->cat, c->dat, nullptr, nullptr));
+            RC(build_graph(c));
+            CK(cudaStreamSynchronize(c->stream));
+            return HQT_OK;
+        };
+        r = member();
+        if (r != HQT_OK) return efail(e, r, "member " + std::to_string(i) + ": " + c->err);
+    }
+    {
+        const int r = build_ensemble_graph(e);
+        if (r != HQT_OK) return r;
+    }
+    if (diags)
+        for (size_t i = 0; i < n; ++i) {
+            diags[i].n_records = 0;
+            diags[i].nonfinite_step = -1;
+            diags[i].steps_done = 0;
+        }
+    std::vector<DevStatus> hs(n);
+    int64_t done = 0;
+    bool bad = false;
+    for (int64_t s = 0; s < nsteps; ++s) {
+        EK(cudaGraphLaunch(e->gexec, e->stream));
+        for (hqt_ctx *c : e->m) c->launches += launches_per_step(c);
+        ++done;
+        if ((done % 64) == 0 || done == nsteps) {
+            for (size_t i = 0; i < n; ++i)
+                EK(cudaMemcpyAsync(&hs[i], e->m[i]->st, sizeof(DevStatus),
+                                   cudaMemcpyDeviceToHost, e->stream));
+            EK(cudaStreamSynchronize(e->stream));
+            for (size_t i = 0; i < n; ++i)
+                if (hs[i].first_bad_step != LLONG_MAX) {
+                    bad = true;
+                    if (diags) diags[i].nonfinite_step = hs[i].first_bad_step - step0[i];
+                }
+            if (bad) break;
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        hqt_ctx *c = e->m[i];
+        k_rho_scatter<<<296, 256, 0, e->stream>>>(c->rho, c->nz, c->plane, (double *)drhoi[i]);
+        EK(cudaGetLastError());
+        c->launches += 1;
+        EK(cudaMemcpyAsync(&hs[i], c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, e->stream));
+    }
+    EK(cudaStreamSynchronize(e->stream));
+    if (diags)
+        for (size_t i = 0; i < n; ++i) {
+            diags[i].steps_done = done;
+            diags[i].last_winding = hs[i].winding;
+        }
+    if (bad) return efail(e, HQT_ENONFINITE, "non-finite value in the fields of a member");
+    return HQT_OK;
+}
+
 }  // extern "C"

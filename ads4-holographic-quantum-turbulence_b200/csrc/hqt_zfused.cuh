@@ -20,17 +20,19 @@
 // evaluated where the C fragments live: lane owns levels 8m+g, columns 2q
 // and 2q+1.
 //
-// Phases of a tile (MODE 1..4 = RK stage, MODE 0 = right-hand side only):
-//   G0  Psi, A_x, A_y, d_x Psi, d_y Psi (kept) and A_t, d_z A_t, lap Psi,
-//       div A (phase P2)                                         -> R, X1
-//   G1  Psi state and accumulator (phase P3)                       -> X2
-//   P1  dp = Lz Psi                                                 -> V
-//   P2  d2 = Lz dp, S1 (:72-73), boundary row kb = Lz(nz,:) div A   -> V
-//   G2  A_x: d_x A_t, d_y B, state, accumulator                     -> X1
-//   P3  F1 = Lzr(S1), RK update of Psi (and of rhoi from kb)
-//   G3  A_y: d_y A_t, d_x B, state, accumulator                     -> X2
-//   P4  for A_x then A_y: g = d A_t + f Lz A, S = 1/2 Lz g +- 1/2 d B
+// Phases of a tile (MODE 1..4 = RK stage, MODE 0 = right-hand side only);
+// R, X1, X2 and V are the shared-memory regions of the warp:
+//   Gm  Psi, A_x, A_y, d_x Psi, d_y Psi -> R; A_x: d_x A_t, d_y B, state,
+//       accumulator -> X1 (issued while the previous tile finishes)
+//   Gy  A_y: d_y A_t, d_x B, state, accumulator -> X2
+//   Fx, Fy  g = d A_t + f Lz A, S = 1/2 Lz g +- 1/2 d B
 //       + Im(conj(Psi) d Psi) - A |Psi|^2 (:74-75), F = Lzr(S), RK update
+//   G2  A_t, d_z A_t, lap Psi, div A -> X1;  dp = Lz Psi -> V
+//   S1  d2 = Lz dp, S1 (:72-73), boundary row kb = Lz(nz,:) div A -> V
+//   G3  Psi state and accumulator -> X2, then Gm of the next tile
+//   F1  F1 = Lzr(S1), RK update of Psi (and of rhoi from kb)
+// Reordering the stage's outputs this way is exact: they are disjoint and all
+// read the same stage inputs.
 #pragma once
 #include <type_traits>
 
@@ -67,10 +69,15 @@ template <int NZP> struct ZmDims {
     static constexpr int LV = MP > KP ? MP : KP;  // levels stored per tile field
 };
 
-// Field of a tile in shared memory: element (level l, column c) at l*8 + c.
+// Field of a tile in shared memory: element (level l, column c) at
+// l*8 + (c ^ ((l >> 1) & 7)).  Operand reads (4 levels x 8 columns) and the
+// fill stay permutations of whole rows; the swizzle makes the accesses at
+// the C-fragment positions (8 levels x 4 column pairs) conflict-free.
 template <typename V> struct ZTileF {
     V *p;
-    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZCols + c]; }
+    __device__ __forceinline__ V &operator()(int l, int c) const {
+        return p[l * kZCols + (c ^ ((l >> 1) & 7))];
+    }
 };
 
 template <typename T, typename TS, typename TD, int NZP> struct ZfLayout {
@@ -200,169 +207,43 @@ __global__ void __launch_bounds__(32)
         ka.p = reinterpret_cast<TS *>(sm + off + 2 * Lay::dr + Lay::sr);
     };
     constexpr bool kReadK = (MODE >= 2);
-
+    // inputs of one gauge component: d A_t, d B, state, accumulator
+    auto stage_gauge = [&](int comp, int off, long long site0) {
+        ZTileF<TD> dt, bf;
+        ZTileF<TS> za, ka;
+        gauge_tiles(off, dt, bf, za, ka);
+        zf_stage<TD>(dt, comp == 0 ? a.dxat : a.dyat, nz, P, site0, lane);
+        zf_stage<TD>(bf, comp == 0 ? a.dyB : a.dxB, nz, P, site0, lane);
+        if (MODE >= 1) {
+            zf_stage<TS>(za, comp == 0 ? a.zax : a.zay, nz, P, site0, lane);
+            if (kReadK) zf_stage<TS>(ka, comp == 0 ? a.kax : a.kay, nz, P, site0, lane);
+        }
+    };
     const long long ntiles = (P + kZCols - 1) / kZCols;
-#pragma unroll 1
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long site0 = tile * kZCols;
-        auto stage_gauge = [&](int comp, int off) {
-            ZTileF<TD> dt, bf;
-            ZTileF<TS> za, ka;
-            gauge_tiles(off, dt, bf, za, ka);
-            zf_stage<TD>(dt, comp == 0 ? a.dxat : a.dyat, nz, P, site0, lane);
-            zf_stage<TD>(bf, comp == 0 ? a.dyB : a.dxB, nz, P, site0, lane);
-            if (MODE >= 1) {
-                zf_stage<TS>(za, comp == 0 ? a.zax : a.zay, nz, P, site0, lane);
-                if (kReadK) zf_stage<TS>(ka, comp == 0 ? a.kax : a.kay, nz, P, site0, lane);
-            }
-        };
-
-        // ---- G0, G1 --------------------------------------------------------
+    // G_main: Psi, A_x, A_y, d_x Psi, d_y Psi (R) and the A_x inputs (X1)
+    auto stage_main = [&](long long site0) {
         zf_stage<C2<T>>(PS, a.ypsi, nz, P, site0, lane);
         zf_stage<T>(AX, a.yax, nz, P, site0, lane);
         zf_stage<T>(AY, a.yay, nz, P, site0, lane);
         zf_stage<C2<TD>>(DXP, a.dxpsi, nz, P, site0, lane);
         zf_stage<C2<TD>>(DYP, a.dypsi, nz, P, site0, lane);
-        zf_stage<T>(AT, a.at, nz, P, site0, lane);
-        zf_stage<T>(DAT, a.dat, nz, P, site0, lane);
-        zf_stage<C2<TD>>(LAP, a.lap, nz, P, site0, lane);
-        zf_stage<TD>(DIV, a.divA, nz, P, site0, lane);
-        cp_commit();
-        if (MODE >= 1) {
-            zf_stage<C2<TS>>(ZP, a.zpsi, nz, P, site0, lane);
-            if (kReadK) zf_stage<C2<TS>>(KP, a.kpsi, nz, P, site0, lane);
-        }
-        cp_commit();
-        cp_wait<1>();
-        __syncwarp();
-
-        // ---- P1: dp = Lz Psi -------------------------------------------------
-        {
-            double cr[MT][2], ci[MT][2];
-            zm_cplx<MT, KS>(ALz, PS, cr, ci, g, q);
-            __syncwarp();
-#pragma unroll
-            for (int m = 0; m < MT; ++m)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(cr[m][h], ci[m][h]);
-        }
-        __syncwarp();
-
-        // ---- P2: d2 = Lz dp, S1, and the boundary row of F2 ------------------
-        T kb = T(0);  // lanes 0..7: column `lane`
-        if (lane < kZCols) {
-#pragma unroll
-            for (int i = 0; i < NZP; ++i)
-                if (i < nz) kb = fma(op.lzb[i], T(DIV(i, lane)), kb);
-        }
-        double s1r[MT][2], s1i[MT][2];
-        {
-            double d2r[MT][2], d2i[MT][2];
-            zm_cplx<MT, KS>(ALz, VC, d2r, d2i, g, q);
-#pragma unroll
-            for (int m = 0; m < MT; ++m) {
-                const int i = 8 * m + g;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int cc = 2 * q + h;
-                    s1r[m][h] = s1i[m][h] = 0.0;
-                    if (i < nz - 1) {
-                        const C2<T> ps = PS(i, cc);
-                        const T at = AT(i, cc), dat = DAT(i, cc), ax = AX(i, cc), ay = AY(i, cc);
-                        const C2<TD> lpd = LAP(i, cc), dxd = DXP(i, cc), dyd = DYP(i, cc);
-                        const T dv = T(DIV(i, cc));
-                        const C2<T> d1 = VC(i, cc);
-                        const T z = zr[m], f = fzr[m], hh = T(0.5);
-                        const T a2 = ax * ax + ay * ay;
-                        const T u = ax * T(dxd.x) + ay * T(dyd.x);
-                        const T w = ax * T(dxd.y) + ay * T(dyd.y);
-                        s1r[m][h] = -at * d1.y - hh * dat * ps.y + hh * f * d2r[m][h] -
-                                    T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
-                                    hh * T(lpd.x) + hh * dv * ps.y + w;
-                        s1i[m][h] = at * d1.x + hh * dat * ps.x + hh * f * d2i[m][h] -
-                                    T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
-                                    hh * T(lpd.y) - hh * dv * ps.x - u;
-                    }
-                }
-            }
-        }
-        __syncwarp();  // every read of dp and of X1 is done
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(s1r[m][h], s1i[m][h]);
-        stage_gauge(0, Lay::oX1);  // G2
-        cp_commit();
-        cp_wait<1>();  // G1
-        __syncwarp();
-
-        // ---- P3: F1 = Lzr(S1) and the RK update of Psi --------------------------
-        {
-            double fr[MT][2], fi[MT][2];
-            zm_cplx<MT, KS>(ALz1, VC, fr, fi, g, q);
-#pragma unroll
-            for (int m = 0; m < MT; ++m) {
-                const int i = 8 * m + g;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int cc = 2 * q + h;
-                    const long long site = site0 + cc;
-                    if (i >= nz || site >= P) continue;
-                    const long long gi = (long long)i * P + site;
-                    if (MODE == 0) {
-                        a.f1[gi] = mk2<T>(fr[m][h], fi[m][h]);
-                        continue;
-                    }
-                    const C2<TS> k = mk2<TS>(a.h * TS(fr[m][h]), a.h * TS(fi[m][h]));
-                    const C2<TS> z = ZP(i, cc);
-                    if (MODE == 4) {
-                        const C2<TS> K = KP(i, cc);
-                        const TS s = TS(1) / TS(6);
-                        a.wpsi[gi] = mk2<TS>(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
-                        continue;
-                    }
-                    if (MODE == 1) {
-                        a.kpsi[gi] = k;
-                    } else {
-                        const C2<TS> K = KP(i, cc);
-                        a.kpsi[gi] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
-                    }
-                    const C2<TS> nv = (MODE == 3) ? mk2<TS>(z.x + k.x, z.y + k.y)
-                                                  : mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
-                    a.npsi[gi] = mk2<T>(T(nv.x), T(nv.y));
-                    if (a.npsi_d) {
-                        const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
-                        const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
-                        a.npsi_d[gi] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
-                    }
-                }
-            }
-        }
-        if (lane < kZCols && site0 + lane < P) {
-            const long long site = site0 + lane;
-            if (MODE == 0) {
-                a.f2b[site] = kb;
-            } else if (!a.f2x) {
-                const TS k = a.h * TS(kb);
-                if (MODE == 1)
-                    a.krho[site] = k;
-                else if (MODE == 2 || MODE == 3)
-                    a.krho[site] = a.krho[site] + 2 * k;
-                else  // rhoi = rhoi - k2(:,:,nz), k2 = (1/6)(k21+2k22+2k23+k24)
-                    a.wrho[site] = a.zrho[site] - (TS(1) / TS(6)) * (a.krho[site] + k);
-            }
-        }
-        __syncwarp();  // X2 and V are free
-        stage_gauge(1, Lay::oX2);  // G3
+        stage_gauge(0, Lay::oX1, site0);
+    };
+    if ((long long)blockIdx.x < ntiles) stage_main((long long)blockIdx.x * kZCols);
+    cp_commit();
+#pragma unroll 1
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long site0 = tile * kZCols;
+        stage_gauge(1, Lay::oX2, site0);  // G_y
         cp_commit();
 
-        // ---- P4: F3 (A_x), then F4 (A_y) ------------------------------------
+        // ---- F3 (A_x), then F4 (A_y) --------------------------------------
 #pragma unroll 1
         for (int comp = 0; comp < 2; ++comp) {
             if (comp == 0)
-                cp_wait<1>();  // G2
+                cp_wait<1>();  // G_main
             else
-                cp_wait<0>();  // G3
+                cp_wait<0>();  // G_y
             __syncwarp();
             ZTileF<TD> DT, BF;
             ZTileF<TS> ZA, KA;
@@ -451,9 +332,141 @@ __global__ void __launch_bounds__(32)
                     }
                 }
             }
-            __syncwarp();  // V is reused next
+            __syncwarp();  // V (and, after A_x, the X1 inputs) are free
         }
+
+        // ---- Psi: A_t, d_z A_t, lap Psi, div A into X1 -----------------------
+        zf_stage<T>(AT, a.at, nz, P, site0, lane);
+        zf_stage<T>(DAT, a.dat, nz, P, site0, lane);
+        zf_stage<C2<TD>>(LAP, a.lap, nz, P, site0, lane);
+        zf_stage<TD>(DIV, a.divA, nz, P, site0, lane);
+        cp_commit();
+
+        // dp = Lz Psi
+        {
+            double cr[MT][2], ci[MT][2];
+            zm_cplx<MT, KS>(ALz, PS, cr, ci, g, q);
+#pragma unroll
+            for (int m = 0; m < MT; ++m)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(cr[m][h], ci[m][h]);
+        }
+        cp_wait<0>();
+        __syncwarp();
+
+        // d2 = Lz dp, S1, and the boundary row of F2
+        T kb = T(0);  // lanes 0..7: column `lane`
+        if (lane < kZCols) {
+#pragma unroll
+            for (int i = 0; i < NZP; ++i)
+                if (i < nz) kb = fma(op.lzb[i], T(DIV(i, lane)), kb);
+        }
+        double s1r[MT][2], s1i[MT][2];
+        {
+            double d2r[MT][2], d2i[MT][2];
+            zm_cplx<MT, KS>(ALz, VC, d2r, d2i, g, q);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int cc = 2 * q + h;
+                    s1r[m][h] = s1i[m][h] = 0.0;
+                    if (i < nz - 1) {
+                        const C2<T> ps = PS(i, cc);
+                        const T at = AT(i, cc), dat = DAT(i, cc), ax = AX(i, cc), ay = AY(i, cc);
+                        const C2<TD> lpd = LAP(i, cc), dxd = DXP(i, cc), dyd = DYP(i, cc);
+                        const T dv = T(DIV(i, cc));
+                        const C2<T> d1 = VC(i, cc);
+                        const T z = zr[m], f = fzr[m], hh = T(0.5);
+                        const T a2 = ax * ax + ay * ay;
+                        const T u = ax * T(dxd.x) + ay * T(dyd.x);
+                        const T w = ax * T(dxd.y) + ay * T(dyd.y);
+                        s1r[m][h] = -at * d1.y - hh * dat * ps.y + hh * f * d2r[m][h] -
+                                    T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
+                                    hh * T(lpd.x) + hh * dv * ps.y + w;
+                        s1i[m][h] = at * d1.x + hh * dat * ps.x + hh * f * d2i[m][h] -
+                                    T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
+                                    hh * T(lpd.y) - hh * dv * ps.x - u;
+                    }
+                }
+            }
+        }
+        __syncwarp();  // every read of dp, R and X1 is done
+#pragma unroll
+        for (int m = 0; m < MT; ++m)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(s1r[m][h], s1i[m][h]);
+        if (MODE >= 1) {  // Psi state and accumulator into X2
+            zf_stage<C2<TS>>(ZP, a.zpsi, nz, P, site0, lane);
+            if (kReadK) zf_stage<C2<TS>>(KP, a.kpsi, nz, P, site0, lane);
+        }
+        cp_commit();
+        // the next tile's main inputs load while this tile finishes
+        if (tile + gridDim.x < ntiles) stage_main((tile + gridDim.x) * kZCols);
+        cp_commit();
+        cp_wait<1>();
+        __syncwarp();
+
+        // ---- F1 = Lzr(S1) and the RK update of Psi ------------------------------
+        {
+            double fr[MT][2], fi[MT][2];
+            zm_cplx<MT, KS>(ALz1, VC, fr, fi, g, q);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int cc = 2 * q + h;
+                    const long long site = site0 + cc;
+                    if (i >= nz || site >= P) continue;
+                    const long long gi = (long long)i * P + site;
+                    if (MODE == 0) {
+                        a.f1[gi] = mk2<T>(fr[m][h], fi[m][h]);
+                        continue;
+                    }
+                    const C2<TS> k = mk2<TS>(a.h * TS(fr[m][h]), a.h * TS(fi[m][h]));
+                    const C2<TS> z = ZP(i, cc);
+                    if (MODE == 4) {
+                        const C2<TS> K = KP(i, cc);
+                        const TS s = TS(1) / TS(6);
+                        a.wpsi[gi] = mk2<TS>(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
+                        continue;
+                    }
+                    if (MODE == 1) {
+                        a.kpsi[gi] = k;
+                    } else {
+                        const C2<TS> K = KP(i, cc);
+                        a.kpsi[gi] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
+                    }
+                    const C2<TS> nv = (MODE == 3) ? mk2<TS>(z.x + k.x, z.y + k.y)
+                                                  : mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
+                    a.npsi[gi] = mk2<T>(T(nv.x), T(nv.y));
+                    if (a.npsi_d) {
+                        const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
+                        const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
+                        a.npsi_d[gi] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
+                    }
+                }
+            }
+        }
+        if (lane < kZCols && site0 + lane < P) {
+            const long long site = site0 + lane;
+            if (MODE == 0) {
+                a.f2b[site] = kb;
+            } else if (!a.f2x) {
+                const TS k = a.h * TS(kb);
+                if (MODE == 1)
+                    a.krho[site] = k;
+                else if (MODE == 2 || MODE == 3)
+                    a.krho[site] = a.krho[site] + 2 * k;
+                else  // rhoi = rhoi - k2(:,:,nz), k2 = (1/6)(k21+2k22+2k23+k24)
+                    a.wrho[site] = a.zrho[site] - (TS(1) / TS(6)) * (a.krho[site] + k);
+            }
+        }
+        __syncwarp();  // X2 and V are free for the next tile
     }
+    cp_wait<0>();
 }
 
 }  // namespace hqt

@@ -42,6 +42,21 @@ WORKLOADS = {
                        remove_winding=False, noise="complex", amp=1e-3, seed=1),
 }
 
+# The batched-ensemble workload: 32 independent runs, grids {128,192,256}^2,
+# nz+1 in {17,21,25} Chebyshev points, mu ~ U[4.5, 8], seeds 0..31, Gaussian
+# noise 1e-3, dt = 0.02, zero flow, L = n/2 (drawn once from default_rng(0)).
+def ensemble_runs(n_runs: int = 32):
+    rng = np.random.default_rng(0)
+    runs = []
+    for i in range(n_runs):
+        n = int(rng.choice([128, 192, 256]))
+        nz = int(rng.choice([17, 21, 25]))
+        mu = float(rng.uniform(4.5, 8.0))
+        runs.append(dict(nx=n, ny=n, nz=nz, L=n / 2, mu=mu, vy=0.0, dt=0.02,
+                         remove_winding=True, noise="complex", amp=1e-3, seed=i))
+    return runs
+
+
 # Algorithmic bytes per site of one launch of each kernel kind (FP64): the
 # arrays the kernel must read once and write once.
 ALG_BYTES = {"x_rhs": 88, "y_rhs": 128, "zstage": 248, "x_d1": 16, "y_d1": 20,
@@ -153,7 +168,8 @@ def allreduce_max(x: float, ws: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -326,19 +342,109 @@ def run_ours(args, w, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, ws, rank, local):
+    """The batched ensemble: runs bin-packed over ranks (no data-path
+    collective), each rank advancing its runs with one graph launch per
+    step.  value = site-updates of all runs / max-over-ranks device time."""
+    import torch
+    hqt = importlib.import_module(PKG)
+    api = importlib.import_module(PKG + ".api")
+    torch.cuda.set_device(local)
+    runs = ensemble_runs()
+    costs = [r["nx"] * r["ny"] * r["nz"] for r in runs]
+    mine = hqt.assign_runs(costs, ws)[rank]
+    stream = torch.cuda.Stream(local)
+    torch.cuda.set_stream(stream)
+    sims, T = [], []
+    for i in mine:
+        r = runs[i]
+        prof = hqt.seed.stationary_profile(r["mu"], r["vy"])
+        st = hqt.seed.init_driven(r["nx"], r["ny"], r["nz"], prof, noise=r["noise"],
+                                  amplitude=r["amp"], seed=r["seed"])
+        sims.append(hqt.Simulation(r["nx"], r["ny"], r["nz"], Lx=r["L"], Ly=r["L"],
+                                   mu=r["mu"], vy=r["vy"], dt=r["dt"],
+                                   remove_winding=r["remove_winding"], device=local))
+        T.append([api.to_device(a, local) for a in st])
+    ens = hqt.Ensemble(sims)
+    ens.step_device(T, nsteps=max(args.warmup, 3))
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    pr = torch.cuda.get_device_properties(local)
+    sampler = ClockSampler(f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0")
+    time.sleep(0.3)
+    for s in sims:
+        s.profile(False)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.step_device(T, nsteps=args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = allreduce_max(e0.elapsed_time(e1), ws)
+    launches = sum(s.profile_report()["launches"] for s in sims)
+    ens.close()
+    for s in sims:
+        s.close()
+    total = sum(costs)
+    value = total * args.steps / (ms / 1e3)
+    peak, peak_kind = peaks()
+    step_gbs = STEP_BYTES_FP64 * total * args.steps / (ms / 1e3) / 1e9
+    if rank == 0:
+        line = {"metric": "RK4 site-updates/s", "value": value, "unit": "site-updates/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (Newton stationary profile per mu + seeded complex noise)",
+                "config": {"workload": "ensemble32", "runs": len(runs),
+                           "grids": sorted({r["nx"] for r in runs}),
+                           "nz": sorted({r["nz"] for r in runs}),
+                           "mu_range": [4.5, 8.0], "total_sites": total,
+                           "runs_per_rank": [len(a) for a in hqt.assign_runs(costs, ws)],
+                           "parallelism": f"runs bin-packed over {ws} GPU(s)",
+                           "launch": "one CUDA-graph launch per step per GPU",
+                           "l2": "no flush: the ensemble touches ~9 GB per step"},
+                "gpu_launches": launches, "roofline": None,
+                "step_hbm": {"alg_bytes_per_site": STEP_BYTES_FP64, "achieved_gbs": step_gbs,
+                             "frac": step_gbs / peak, "peak_source": peak_kind},
+                "e2e": None, "cpu_baseline": None, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="driven301", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="driven301",
+                    choices=sorted(WORKLOADS) + ["ensemble32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision variant")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))
+    if args.workload == "ensemble32":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the ensemble workload has no CPU reference arm; "
+                              "the reference runs one simulation per session"}))
+            return
+        ws, rank, local = dist_init()
+        try:
+            run_ensemble(args, ws, rank, local)
+        finally:
+            if ws > 1:
+                import torch.distributed as dist
+                dist.destroy_process_group()
+        return
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         # the CPU reference runs on rank 0 only; other ranks exit at once

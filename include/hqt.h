@@ -171,6 +171,30 @@ int hqt_count_vortices_field_noalloc(const void *dZ1, int32_t nx, int32_t ny,
                                      int32_t *nm, void *cuda_stream);
 const char *hqt_noalloc_last_error(void);
 
+/* Ensembles: independent runs advanced together (no counterpart in the
+ * reference, whose scripts run one simulation per MATLAB session; the
+ * members are the per-run contexts of hqt_create, each with its own grid,
+ * nz, mu, precision and initial state).  hqt_ensemble_create groups existing
+ * contexts of one device (the caller keeps owning them and destroys them
+ * after the ensemble).  hqt_ensemble_step_device advances every member
+ * `nsteps` RK4 steps on its DEVICE arrays (element i of each pointer array
+ * belongs to member i, same layout and in-place semantics as
+ * hqt_step_device) with one CUDA-graph launch per step for the whole
+ * ensemble.  `diags` is NULL or an array of one hqt_diag per member;
+ * vortex-count records are not taken (n_records = 0).  A non-finite member
+ * stops the whole ensemble at the next status poll (every 64 steps) with
+ * HQT_ENONFINITE and its diags[i].nonfinite_step set. */
+typedef struct hqt_ensemble hqt_ensemble;
+int hqt_ensemble_create(hqt_ctx *const *members, int32_t n, hqt_ensemble **out);
+void hqt_ensemble_destroy(hqt_ensemble *ens);
+/* Launch the ensemble graph on the caller's stream (NULL: its own). */
+int hqt_ensemble_set_stream(hqt_ensemble *ens, void *cuda_stream);
+const char *hqt_ensemble_last_error(const hqt_ensemble *ens);
+int hqt_ensemble_step_device(hqt_ensemble *ens, void *const *dZ1, void *const *dZ2,
+                             void *const *dZ3, void *const *dZ4,
+                             void *const *drhoi, int64_t nsteps,
+                             hqt_diag *diags);
+
 /* Instrumentation (no counterpart in the reference, which times its loop
  * with tic/toc every 50 steps, tevol_driven_cluster.m:116,144-146).
  * hqt_profile(ctx, 1) resets the counters and makes every following launch
