@@ -75,6 +75,7 @@ struct hqt_ctx {
     float *dxat32 = nullptr, *dyat32 = nullptr;
     double *f2x = nullptr, *f2y = nullptr, *f2 = nullptr;  // 2-D boundary terms
     double *slice_mean = nullptr;                           // 5 per z-slice
+    double *slice_partial = nullptr;                        // 5 per (z, chunk)
     double2 *O = nullptr;
     double *partial = nullptr;
     double *kxv = nullptr, *kyv = nullptr, *bins = nullptr;  // spectrum scratch
@@ -84,6 +85,7 @@ struct hqt_ctx {
     // launch geometry
     int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
     bool cx = false, cy = false;  // compile-time line transforms along x / y
+    bool px = false, py = false;  // prime-factor tensor-core transforms along x / y
     int smem_optin = 0;
     // state arrays the step acts on (internal buffers, or the caller's
     // device arrays for hqt_step_device)
@@ -243,6 +245,10 @@ int launch_x_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     a.dxxay = c->dxxay;
     const int grid = (a.nlines + a.NB - 1) / a.NB;
     Prof pr(c, K_X_RHS);
+    if (c->px) {
+        CK(pfa_launch_301(CT_X_RHS, &a, a.nlines, c->stream));
+        return HQT_OK;
+    }
     if (c->cx) {
         const int nb = ct_lines(c->nx, 3);
         RC(ct_dispatch(c, c->nx, CT_X_RHS, &a, dim3((a.nlines + nb - 1) / nb), smem_x(c->nx, 3, nb)));
@@ -607,9 +613,12 @@ int enqueue_stages_mixed(hqt_ctx *c) {
     double2 *psi = c->cpsi;
     double *at = c->cat, *ax = c->cax, *ay = c->cay;
     {
-        Prof pr(c, K_CONVERT, 2);
-        k_slice_means<<<c->nz, kRedThreads, 0, c->stream>>>(psi, at, ax, ay, c->plane,
-                                                            c->slice_mean);
+        Prof pr(c, K_CONVERT, 3);
+        k_slice_partials<<<dim3(kSliceChunks, c->nz), kRedThreads, 0, c->stream>>>(
+            psi, at, ax, ay, c->plane, c->slice_partial);
+        CK(cudaGetLastError());
+        k_slice_finalize<<<(5 * c->nz + 127) / 128, 128, 0, c->stream>>>(
+            c->slice_partial, c->nz, c->plane, c->slice_mean);
         CK(cudaGetLastError());
         k_state_to_f32<<<592, 256, 0, c->stream>>>(psi, at, ax, ay, c->plane, c->vol,
                                                   c->slice_mean, c->ypsi32[2], c->at32,
@@ -796,7 +805,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 2 + 4 * 3 : 0);
+    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 3 + 4 * 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -1123,6 +1132,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         A(&c->f2y, sizeof(double) * P2);
         A(&c->f2, sizeof(double) * P2);
         A(&c->slice_mean, sizeof(double) * 5 * p.nz);
+        A(&c->slice_partial, sizeof(double) * 5 * kSliceChunks * p.nz);
     }
     A(&c->rootsx32, sizeof(float2) * p.nx);
     A(&c->rootsy32, sizeof(float2) * p.ny);
@@ -1168,9 +1178,14 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     c->TXy_filt = pick_lines(p.ny, 6, 16);
     c->cx = ct_supported(p.nx);
     c->cy = ct_supported(p.ny);
+    c->px = pfa_length(p.nx);
+    c->py = pfa_length(p.ny);
     if (const char *env = std::getenv("HQT_LINE_ENGINE")) {
-        // "runtime" forces the runtime-plan engine (the tests cover both)
+        // "runtime" forces the runtime-plan engine, "stockham" the
+        // compile-time Stockham engine (the tests cover all three)
         if (std::string(env) == "runtime") c->cx = c->cy = false;
+        if (std::string(env) == "runtime" || std::string(env) == "stockham")
+            c->px = c->py = false;
     }
     {
         const size_t lim = 227 * 1024 - 1024;

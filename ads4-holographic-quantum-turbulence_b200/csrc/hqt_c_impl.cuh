@@ -4,6 +4,11 @@
 
 #include "hqt_cpasses.cuh"
 #include "hqt_launch.h"
+#if HQT_CN == 301
+#define HQT_PFA_P 7
+#define HQT_PFA_Q 43
+#include "hqt_pfa_passes.cuh"
+#endif
 
 #ifndef HQT_CN
 #error "define HQT_CN"
@@ -31,6 +36,13 @@ cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const 
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      max_smem - (int)fa.sharedSizeBytes);
     };
+#ifdef HQT_PFA_P
+    if (e == cudaSuccess) {
+        std::vector<double> frag(PfaDims<HQT_PFA_P, HQT_PFA_Q>::NFRAG * 32);
+        pfa_fragments<HQT_PFA_P, HQT_PFA_Q>(frag.data());
+        e = cudaMemcpyToSymbol(g_pfa_frag, frag.data(), sizeof(double) * frag.size());
+    }
+#endif
     opt((const void *)k_x_rhs_c<double, HQT_CN>);
     opt((const void *)k_y_rhs_c<double, HQT_CN>);
     opt((const void *)k_x_d1_c<double, HQT_CN>);
@@ -90,5 +102,21 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
     }
     return cudaGetLastError();
 }
+
+#ifdef HQT_PFA_P
+cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t s) {
+    constexpr int P = HQT_PFA_P, Q = HQT_PFA_Q;
+    const int grid = (nlines + kPfaLines - 1) / kPfaLines;
+    constexpr size_t smem = pfa_smem_bytes<P, Q>();
+    switch (kind) {
+        case CT_X_RHS:
+            k_x_rhs_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+#endif
 
 }  // namespace hqt

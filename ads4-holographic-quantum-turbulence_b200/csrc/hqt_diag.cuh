@@ -122,15 +122,21 @@ __global__ void k_phase_multiply(double2 *psi, int nx, int ny, long long vol,
     }
 }
 
-// Per z-slice plane means of (Re psi, Im psi, A_t, A_x, A_y): block z sums
-// the slice in a fixed tree (deterministic).
+// Per z-slice plane means of (Re psi, Im psi, A_t, A_x, A_y), in two
+// deterministic passes: block (chunk, z) sums chunk `chunk` of slice z in a
+// fixed tree into partial[z][chunk][5]; k_slice_finalize adds the chunks of
+// each slice in order.
+constexpr int kSliceChunks = 32;
 __global__ void __launch_bounds__(kRedThreads)
-    k_slice_means(const double2 *psi, const double *at, const double *ax, const double *ay,
-                  long long plane, double *mean) {
+    k_slice_partials(const double2 *psi, const double *at, const double *ax,
+                     const double *ay, long long plane, double *partial) {
     __shared__ double sh[5][kRedThreads];
-    const long long off = (long long)blockIdx.x * plane;
+    const long long off = (long long)blockIdx.y * plane;
+    const long long per = (plane + kSliceChunks - 1) / kSliceChunks;
+    const long long s0 = (long long)blockIdx.x * per;
+    const long long s1 = min(plane, s0 + per);
     double acc[5] = {0, 0, 0, 0, 0};
-    for (long long s = threadIdx.x; s < plane; s += blockDim.x) {
+    for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         const double2 p = psi[off + s];
         acc[0] += p.x;
         acc[1] += p.y;
@@ -145,7 +151,18 @@ __global__ void __launch_bounds__(kRedThreads)
             for (int f = 0; f < 5; ++f) sh[f][threadIdx.x] += sh[f][threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x < 5) mean[5 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0] / (double)plane;
+    if (threadIdx.x < 5)
+        partial[((long long)blockIdx.y * kSliceChunks + blockIdx.x) * 5 + threadIdx.x] =
+            sh[threadIdx.x][0];
+}
+
+__global__ void k_slice_finalize(const double *partial, int nz, long long plane, double *mean) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (z, field)
+    if (t >= 5 * nz) return;
+    const int z = t / 5, f = t % 5;
+    double s = 0.0;
+    for (int c = 0; c < kSliceChunks; ++c) s += partial[((long long)z * kSliceChunks + c) * 5 + f];
+    mean[t] = s / (double)plane;
 }
 
 // FP32 copies of the state minus the slice means, for the FP32 line passes

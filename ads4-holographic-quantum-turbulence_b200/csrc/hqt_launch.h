@@ -43,6 +43,11 @@ template <int N> cudaError_t ct_init(const double *tab_cos, const double *tab_si
 template <int N>
 cudaError_t ct_launch(int kind, const void *args, dim3 grid, size_t smem, cudaStream_t s);
 
+// Line lengths with a prime-factor tensor-core engine (hqt_pfa.cuh): 301 = 7*43.
+constexpr bool pfa_length(int n) { return n == 301; }
+// Launch pass `kind` (CT_X_RHS, ...) on it: lines of kPfaLines per one-warp block.
+cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t s);
+
 // Column kernels, one translation unit per compile-time column length N.
 // mode 0: right-hand side only, 1..4: RK stage.
 template <int N> cudaError_t z_init(int max_smem);

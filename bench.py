@@ -256,10 +256,18 @@ def run_ours(args, w, ws, rank, local):
             m1.record()
             torch.cuda.synchronize()
             mms = allreduce_max(m0.elapsed_time(m1), ws)
+            simm.profile(True)
+            simm.step_device(*Tm, nsteps=min(args.steps, 20))
+            mrep = simm.profile_report()
+            simm.profile(False)
         del Tm
+        mtot = sum(k["ms"] for k in mrep["kernels"])
+        mbreak = {k["kernel"]: {"launches": k["launches"], "ms": round(k["ms"], 4),
+                                "share": round(k["ms"] / mtot, 4)} for k in mrep["kernels"]}
         mixed = {"value": ws * sites * args.steps / (mms / 1e3), "unit": "site-updates/s",
                  "ms_per_step": mms / args.steps, "steps": args.steps,
-                 "dtype": "f32 line passes, f64 column contractions and state"}
+                 "dtype": "f32 line passes, f64 column contractions and state",
+                 "kernel_breakdown": mbreak}
 
     # per-kernel CUDA-event timing of the same step sequence (outside the graph)
     kp = min(args.steps, 20)

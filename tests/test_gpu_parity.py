@@ -46,7 +46,7 @@ def dev(cuda, hqt):
 
 
 GRIDS = [(33, 33, 10), (64, 64, 21), (48, 40, 17), (30, 22, 12), (53, 59, 8),
-         (128, 96, 25)]
+         (128, 96, 25), (301, 40, 8)]
 
 
 @pytest.mark.parametrize("nx,ny,nz", GRIDS)
@@ -232,11 +232,14 @@ def test_nonfinite_guard(hqt, cuda):
         assert np.all(np.isfinite(g1))
 
 
+@pytest.mark.parametrize("engine", ["runtime", "stockham"])
 @pytest.mark.parametrize("nx,ny,nz", [(64, 64, 21), (301, 301, 9), (53, 59, 8)])
-def test_runtime_line_engine_parity(hqt, oracle, dev, monkeypatch, nx, ny, nz):
-    """The runtime-plan line-transform engine (used for line lengths without a
-    compile-time transform) on the same RHS and filter checks."""
-    monkeypatch.setenv("HQT_LINE_ENGINE", "runtime")
+def test_runtime_line_engine_parity(hqt, oracle, dev, monkeypatch, nx, ny, nz, engine):
+    """The other line-transform engines on the same RHS and filter checks:
+    the runtime-plan engine (line lengths without a compile-time transform)
+    and the compile-time Stockham engine (which the prime-factor tensor-core
+    engine replaces for its lengths)."""
+    monkeypatch.setenv("HQT_LINE_ENGINE", engine)
     to_d, from_d = dev
     Lx, Ly = 0.5 * nx, 0.45 * ny
     Z1, Z2, Z3, Z4 = random_fields(nx, ny, nz, seed=nx + nz)
