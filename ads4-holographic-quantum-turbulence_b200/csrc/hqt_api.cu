@@ -281,6 +281,10 @@ int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     a.dyB = c->dyB;
     dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
     Prof pr(c, K_Y_RHS);
+    if (c->py) {
+        CK(pfa_launch_301(CT_Y_RHS, &a, c->nz, c->stream));
+        return HQT_OK;
+    }
     if (c->cy) {
         const int nb = ct_lines(c->ny, 3);
         RC(ct_dispatch(c, c->ny, CT_Y_RHS, &a, dim3((c->nx + nb - 1) / nb, c->nz),

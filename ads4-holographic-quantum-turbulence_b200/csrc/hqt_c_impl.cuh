@@ -106,12 +106,17 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
 #ifdef HQT_PFA_P
 cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t s) {
     constexpr int P = HQT_PFA_P, Q = HQT_PFA_Q;
-    const int grid = (nlines + kPfaLines - 1) / kPfaLines;
+    const int grid = (nlines + kPfaLines - 1) / kPfaLines;  // x passes
     constexpr size_t smem = pfa_smem_bytes<P, Q>();
     switch (kind) {
         case CT_X_RHS:
             k_x_rhs_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
             break;
+        case CT_Y_RHS: {
+            const YRhsArgs<double> &a = *(const YRhsArgs<double> *)args;
+            k_y_rhs_pfa<P, Q><<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines), 32, smem, s>>>(a);
+            break;
+        }
         default:
             return cudaErrorInvalidValue;
     }

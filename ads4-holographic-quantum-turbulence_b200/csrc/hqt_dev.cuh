@@ -10,4 +10,16 @@ template <typename T> __device__ __forceinline__ C2<T> *sptr(int off) {
     return reinterpret_cast<C2<T> *>(g_smem) + off;
 }
 
+// ---- cp.async (global -> shared, 4/8/16 bytes, completes per group) -------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem),
+                 "n"(BYTES));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 }  // namespace hqt

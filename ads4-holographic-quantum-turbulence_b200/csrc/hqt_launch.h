@@ -45,7 +45,8 @@ cudaError_t ct_launch(int kind, const void *args, dim3 grid, size_t smem, cudaSt
 
 // Line lengths with a prime-factor tensor-core engine (hqt_pfa.cuh): 301 = 7*43.
 constexpr bool pfa_length(int n) { return n == 301; }
-// Launch pass `kind` (CT_X_RHS, ...) on it: lines of kPfaLines per one-warp block.
+// Launch pass `kind` (CT_X_RHS, ...) on it: lines of kPfaLines per one-warp
+// block.  `nlines`: lines of an x pass; z slices of a y pass.
 cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t s);
 
 // Column kernels, one translation unit per compile-time column length N.

@@ -118,7 +118,10 @@ template <int P, int Q> struct PfaWarp {
                     pfa_mma(qa[m][0], qa[m][1], As[m][s], b);
                 }
             }
-            // lane holds rows k = 8m+g, column u = 4nt+q, parts re (0) and im (1)
+            // lane holds rows k = 8m+g, column u = 4nt+q, parts re (0) and im (1).
+            // A tile writes only its own columns, after all its reads: stage A
+            // may run in place.
+            __syncwarp();
             const int u = 4 * nt + q;
             if (u < D::U) {
 #pragma unroll

@@ -21,34 +21,49 @@ template <int P, int Q> struct PfaLines {
     using D = PfaDims<P, Q>;
     static constexpr int N = D::N, LN = kPfaLines * N;
     PfaBuf b0, b1;
-    int valid;
-    long long g0;
+    int valid;  // lines of this warp inside the grid
+    int lane;
 
-    __device__ __forceinline__ PfaLines(int nlines) {
+    __device__ __forceinline__ PfaLines(int valid_) : valid(valid_), lane(threadIdx.x & 31) {
         double *sm = reinterpret_cast<double *>(g_smem);
         b0 = PfaBuf{sm, sm + LN};
         b1 = PfaBuf{sm + 2 * LN, sm + 3 * LN};
-        const int L0 = blockIdx.x * kPfaLines;
-        valid = min(kPfaLines, nlines - L0);
-        g0 = (long long)L0 * N;
     }
-    // lines g0.. (contiguous in global memory) into b0 in the input order
-    template <typename Get> __device__ __forceinline__ void load(int lane, Get get) const {
+    // Position of element n of line ln in a buffer.  The input order of
+    // stage A and the output order of the inverse stage A coincide: n with
+    // n1 = n*QIP mod P, n2 = n*PIQ mod Q is the output (u = ln*P + n1, n2).
+    __device__ __forceinline__ static int pos(int ln, int n) {
+        return (ln * P + (n * D::QIP) % P) * Q + (n * D::PIQ) % Q;
+    }
+    // Element (ln, n), adjacent lanes on adjacent lines, for every element
+    // inside the grid: lines that are adjacent columns (y lines) are then
+    // touched a 32-byte sector at a time.
+    template <typename F> __device__ __forceinline__ void each(F f) const {
         for (int e = lane; e < LN; e += 32) {
-            const int ln = e / N, n = e - ln * N;
-            const int n1 = (n * D::QIP) % P, n2 = (n * D::PIQ) % Q;
-            const double2 v = ln < valid ? get(e) : make_double2(0.0, 0.0);
-            const int idx = (ln * P + n1) * Q + n2;
-            b0.re[idx] = v.x;
-            b0.im[idx] = v.y;
+            const int ln = e % kPfaLines, n = e / kPfaLines;
+            if (ln < valid) f(ln, n, pos(ln, n));
         }
-        __syncwarp();
     }
-    // global offset (from g0) of output element (u = line*P + n1, n2), or -1
-    __device__ __forceinline__ long long out_off(int u, int n2) const {
-        const int ln = u / P, n1 = u - ln * P;
-        if (ln >= valid) return -1;
-        return (long long)ln * N + (Q * n1 + P * n2) % N;
+    // cp.async of the doubles re(ln, n), im(ln, n) (pointers) into `dst`;
+    // elements of lines outside the grid are zeroed.  The caller commits.
+    template <typename Re, typename Im>
+    __device__ __forceinline__ void fetch(PfaBuf dst, Re re, Im im) const {
+        for (int e = lane; e < LN; e += 32) {
+            const int ln = e % kPfaLines, n = e / kPfaLines, i = pos(ln, n);
+            if (ln < valid) {
+                cp_async<8>(dst.re + i, re(ln, n));
+                cp_async<8>(dst.im + i, im(ln, n));
+            } else {
+                dst.re[i] = 0.0;
+                dst.im[i] = 0.0;
+            }
+        }
+    }
+    static __device__ __forceinline__ auto in_place(PfaBuf b) {
+        return [b](int u, int k, double re, double im) {
+            b.re[u * Q + k] = re;
+            b.im[u * Q + k] = im;
+        };
     }
 };
 
@@ -59,44 +74,218 @@ template <int P> __device__ __forceinline__ void pfa_twiddles(double (&cs)[2][P]
 }
 
 // x pass of one RK stage: d_x Psi, d_xx Psi, E = d_x(A_x + i A_y), d_xx A_y.
-// Per field: load (b0) -> stage A (b1) -> for each derivative: stage B with
-// the multiplier (b0) -> inverse stage A (global memory).
+// Per field: fetch (b0), stage A in place; per derivative: stage B with the
+// multiplier (b0 -> b1), inverse stage A in place, coalesced store.
 template <int P, int Q>
 __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsArgs<double> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<P, Q>;
     PfaWarp<P, Q> w;
     w.init(g_pfa_frag);
     double cs[2][P];
     pfa_twiddles<P>(cs);
-    const PfaLines<P, Q> L(a.nlines);
-    auto to_b1 = [&](int u, int k, double re, double im) {
-        L.b1.re[u * Q + k] = re;
-        L.b1.im[u * Q + k] = im;
-    };
-    // derivative ORDER of the field held (after stage A) in b1, to out()
-    auto deriv = [&](auto order, auto out) {
+    const int L0 = blockIdx.x * kPfaLines;
+    const long long g0 = (long long)L0 * N;
+    const L_t L(min(kPfaLines, a.nlines - L0));
+    auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
+    auto deriv = [&](auto order) {
         constexpr int ORDER = decltype(order)::value;
-        w.template stage_b_deriv<ORDER>(L.b1, L.b0, a.s1, a.s2, cs);
+        w.template stage_b_deriv<ORDER>(L.b0, L.b1, a.s1, a.s2, cs);
         __syncwarp();
-        w.template stage_a<+1>(L.b0, [&](int u, int n2, double re, double im) {
-            const long long o = L.out_off(u, n2);
-            if (o >= 0) out(L.g0 + o, re, im);
-        });
+    };
+    auto inverse = [&]() {
+        w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
         __syncwarp();
     };
     using O1 = std::integral_constant<int, 1>;
     using O2 = std::integral_constant<int, 2>;
     // Psi
-    L.load(w.lane, [&](int e) { return a.psi[L.g0 + e]; });
-    w.template stage_a<-1>(L.b0, to_b1);
+    L.fetch(L.b0, [&](int ln, int n) { return &a.psi[gi(ln, n)].x; },
+            [&](int ln, int n) { return &a.psi[gi(ln, n)].y; });
+    cp_commit();
+    cp_wait<0>();
     __syncwarp();
-    deriv(O1{}, [&](long long i, double re, double im) { a.dxpsi[i] = make_double2(re, im); });
-    deriv(O2{}, [&](long long i, double re, double im) { a.dxxpsi[i] = make_double2(re, im); });
-    // C = A_x + i A_y
-    L.load(w.lane, [&](int e) { return make_double2(a.ax[L.g0 + e], a.ay[L.g0 + e]); });
-    w.template stage_a<-1>(L.b0, to_b1);
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
     __syncwarp();
-    deriv(O1{}, [&](long long i, double re, double im) { a.E[i] = make_double2(re, im); });
-    deriv(O2{}, [&](long long i, double re, double im) { a.dxxay[i] = im; });
+    deriv(O1{});
+    inverse();
+    L.each([&](int ln, int n, int i) { a.dxpsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    __syncwarp();
+    deriv(O2{});
+    // C = A_x + i A_y loads while the inverse runs
+    L.fetch(L.b0, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
+            [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+    cp_commit();
+    inverse();
+    L.each([&](int ln, int n, int i) { a.dxxpsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    deriv(O1{});
+    inverse();
+    L.each([&](int ln, int n, int i) { a.E[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    __syncwarp();
+    deriv(O2{});
+    inverse();
+    L.each([&](int ln, int n, int i) { a.dxxay[gi(ln, n)] = L.b1.im[i]; });
+}
+
+// y pass of one RK stage (lines along y: kPfaLines adjacent x columns of one
+// z slice): d_y Psi, lap Psi = d_xx Psi + d_yy Psi, and from the spectra of
+// C = A_x + i A_y and E = d_x C the fields div A = d_x A_x + d_y A_y,
+// d_x B and d_y B (B = d_x A_y - d_y A_x).  The real fields are separated
+// from the pair spectra with the k <-> -k symmetry: in the prime-factor
+// order the partner of column k2 is column Q - k2, so one lane takes each
+// column pair and runs forward stage B, the combination and inverse stage
+// B in its registers.  Addends (d_xx Psi, d_x A_x, d_xx A_y) are fetched
+// into a freed buffer while an inverse stage runs.
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsArgs<double> a) {
+    using D = PfaDims<P, Q>;
+    using L_t = PfaLines<P, Q>;
+    constexpr int N = D::N, H = (P - 1) / 2;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int x0 = blockIdx.x * kPfaLines;
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    const L_t L(min(kPfaLines, a.nx - x0));
+    auto gi = [&](int ln, int n) { return zoff + (long long)n * a.nx + ln; };
+    auto inverse = [&](PfaBuf b) {
+        w.template stage_a<+1>(b, L_t::in_place(b));
+        __syncwarp();
+    };
+    // Psi: d_y and d_yy
+    L.fetch(L.b0, [&](int ln, int n) { return &a.psi[gi(ln, n)].x; },
+            [&](int ln, int n) { return &a.psi[gi(ln, n)].y; });
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, a.s2, cs);
+    __syncwarp();
+    inverse(L.b1);
+    L.each([&](int ln, int n, int i) { a.dypsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    __syncwarp();
+    w.template stage_b_deriv<2>(L.b0, L.b1, a.s1, a.s2, cs);
+    __syncwarp();
+    L.fetch(L.b0, [&](int ln, int n) { return &a.dxxpsi[gi(ln, n)].x; },
+            [&](int ln, int n) { return &a.dxxpsi[gi(ln, n)].y; });
+    cp_commit();
+    inverse(L.b1);
+    cp_wait<0>();
+    __syncwarp();
+    L.each([&](int ln, int n, int i) {
+        a.lap[gi(ln, n)] = make_double2(L.b0.re[i] + L.b1.re[i], L.b0.im[i] + L.b1.im[i]);
+    });
+    __syncwarp();
+    // C and E after stage A, in place
+    L.fetch(L.b0, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
+            [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+    L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+            [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    // column pairs (k2, Q - k2) of each line: spectra, combination, inverse
+    constexpr int NPAIR = (Q + 1) / 2;
+#pragma unroll 1
+    for (int task = w.lane; task < kPfaLines * NPAIR; task += 32) {
+        const int ln = task / NPAIR, k2a = task - ln * NPAIR;
+        const int k2b = (Q - k2a) % Q;
+        const int ncol = (k2b == k2a) ? 1 : 2;
+        double cr[2][P], ci[2][P], er[2][P], ei[2][P];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int k2 = c == 0 ? k2a : k2b;
+            double zr[P], zi[P];
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) {
+                const int e = (ln * P + n1) * Q + k2;
+                zr[n1] = L.b0.re[e];
+                zi[n1] = L.b0.im[e];
+            }
+            PfaWarp<P, Q>::template dft_real_pair<-1, H>(zr, zi, cr[c], ci[c], cs);
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) {
+                const int e = (ln * P + n1) * Q + k2;
+                zr[n1] = L.b1.re[e];
+                zi[n1] = L.b1.im[e];
+            }
+            PfaWarp<P, Q>::template dft_real_pair<-1, H>(zr, zi, er[c], ei[c], cs);
+        }
+        // entry (0, k1) pairs with (1, P - k1): combine both from the four
+        // spectra values and overwrite them in place (C <- the d_y A_y and
+        // -d_y d_x A_x pair spectrum, E <- the d_y B spectrum).  Column k2 = 0
+        // pairs with itself; both copies hold its spectra.
+        auto comb = [&](int k2, int k1, double c1x, double c1y, double c2x, double c2y,
+                        double e1x, double e1y, double e2x, double e2y, double &sr, double &si,
+                        double &tr, double &ti) {
+            const int k = (Q * D::QIP * k1 + P * D::PIQ * k2) % N;
+            const double kk = (double)(2 * k < N ? k : k - N);
+            const double m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = 0.5;
+            const double axr = h * (c1x + c2x), axi = h * (c1y - c2y);
+            const double ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
+            const double exr = h * (e1x + e2x), exi = h * (e1y - e2y);
+            const double eyr = h * (e1y + e2y), eyi = -h * (e1x - e2x);
+            const double q1r = -m1 * ayi, q1i = m1 * ayr;  // d_y A_y
+            const double q2r = m1 * exi, q2i = -m1 * exr;  // -d_y d_x A_x
+            sr = q1r - q2i;
+            si = q1i + q2r;
+            tr = -m1 * eyi - m2 * axr;  // d_y B
+            ti = m1 * eyr - m2 * axi;
+        };
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) {
+            const int k1p = (P - k1) % P;
+            const double c0x = cr[0][k1], c0y = ci[0][k1], c1x = cr[1][k1p], c1y = ci[1][k1p];
+            const double e0x = er[0][k1], e0y = ei[0][k1], e1x = er[1][k1p], e1y = ei[1][k1p];
+            comb(k2a, k1, c0x, c0y, c1x, c1y, e0x, e0y, e1x, e1y, cr[0][k1], ci[0][k1],
+                 er[0][k1], ei[0][k1]);
+            comb(k2b, k1p, c1x, c1y, c0x, c0y, e1x, e1y, e0x, e0y, cr[1][k1p], ci[1][k1p],
+                 er[1][k1p], ei[1][k1p]);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (c >= ncol) break;
+            const int k2 = c == 0 ? k2a : k2b;
+            double zr[P], zi[P];
+            PfaWarp<P, Q>::template dft_real_pair<+1, H>(cr[c], ci[c], zr, zi, cs);
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) {
+                const int e = (ln * P + n1) * Q + k2;
+                L.b0.re[e] = zr[n1];
+                L.b0.im[e] = zi[n1];
+            }
+            PfaWarp<P, Q>::template dft_real_pair<+1, H>(er[c], ei[c], zr, zi, cs);
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) {
+                const int e = (ln * P + n1) * Q + k2;
+                L.b1.re[e] = zr[n1];
+                L.b1.im[e] = zi[n1];
+            }
+        }
+    }
+    __syncwarp();
+    inverse(L.b1);
+    L.each([&](int ln, int n, int i) { a.dyB[gi(ln, n)] = L.b1.re[i]; });
+    __syncwarp();
+    L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+            [&](int ln, int n) { return &a.dxxay[gi(ln, n)]; });
+    cp_commit();
+    inverse(L.b0);
+    cp_wait<0>();
+    __syncwarp();
+    L.each([&](int ln, int n, int i) {
+        a.divA[gi(ln, n)] = L.b1.re[i] + L.b0.re[i];
+        a.dxB[gi(ln, n)] = L.b1.im[i] + L.b0.im[i];
+    });
 }
 
 }  // namespace hqt

@@ -43,18 +43,6 @@ namespace hqt {
 
 constexpr int kZCols = 8;  // columns per warp tile (the n extent of one mma)
 
-// ---- cp.async (global -> shared, 4/8/16 bytes, completes per group) -------
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem),
-                 "n"(BYTES));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N> __device__ __forceinline__ void cp_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // d += a * b on one 8x8x4 FP64 tensor-core tile
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
