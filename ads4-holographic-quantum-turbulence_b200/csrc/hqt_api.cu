@@ -306,6 +306,10 @@ int launch_x_d1(hqt_ctx *c, FieldIn<double> in, FieldOut<double> out, int nslice
     a.out = out;
     const int grid = (a.nlines + a.NB - 1) / a.NB;
     Prof pr(c, K_X_D1);
+    if (c->px) {
+        CK(pfa_launch_301(CT_X_D1, &a, a.nlines, c->stream));
+        return HQT_OK;
+    }
     if (c->cx) {
         const int nb = ct_lines(c->nx, 2);
         RC(ct_dispatch(c, c->nx, CT_X_D1, &a, dim3((a.nlines + nb - 1) / nb), smem_x(c->nx, 2, nb)));
@@ -330,6 +334,10 @@ int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<d
     a.out = out;
     dim3 grid((c->nx + a.TX - 1) / a.TX, nsl);
     Prof pr(c, K_Y_D1);
+    if (c->py) {
+        CK(pfa_launch_301(CT_Y_D1, &a, nsl, c->stream));
+        return HQT_OK;
+    }
     if (c->cy) {
         const int nb = ct_lines(c->ny, 2);
         RC(ct_dispatch(c, c->ny, CT_Y_D1, &a, dim3((c->nx + nb - 1) / nb, nsl),
@@ -465,7 +473,9 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.st = phase ? c->st : nullptr;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_FWD);
-        if (c->cx) {
+        if (c->px) {
+            CK(pfa_launch_301(CT_FX_FWD, &a, a.nlines, c->stream));
+        } else if (c->cx) {
             const int nb = ct_lines(c->nx, 2);
             RC(ct_dispatch(c, c->nx, CT_FX_FWD, &a, dim3((a.nlines + nb - 1) / nb),
                            smem_x(c->nx, 2, nb)));
@@ -487,7 +497,9 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.scale = 1.0 / ((double)c->nx * (double)c->ny);
         dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
         Prof pr(c, K_FILT_Y);
-        if (c->cy) {
+        if (c->py) {
+            CK(pfa_launch_301(CT_FY, &a, c->nz, c->stream));
+        } else if (c->cy) {
             const int tx = ct_lines(c->ny, 6);
             RC(ct_dispatch(c, c->ny, CT_FY, &a, dim3((c->nx + tx - 1) / tx, c->nz),
                            smem_x(c->ny, 2, 3 * tx)));
@@ -509,7 +521,9 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.st = check ? c->st : nullptr;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_INV);
-        if (c->cx) {
+        if (c->px) {
+            CK(pfa_launch_301(CT_FX_INV, &a, a.nlines, c->stream));
+        } else if (c->cx) {
             const int nb = ct_lines(c->nx, 2);
             RC(ct_dispatch(c, c->nx, CT_FX_INV, &a, dim3((a.nlines + nb - 1) / nb),
                            smem_x(c->nx, 2, nb)));

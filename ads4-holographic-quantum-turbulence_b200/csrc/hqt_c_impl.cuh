@@ -117,6 +117,26 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
             k_y_rhs_pfa<P, Q><<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines), 32, smem, s>>>(a);
             break;
         }
+        case CT_X_D1:
+            k_x_d1_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XD1Args<double> *)args);
+            break;
+        case CT_Y_D1: {
+            const YD1Args<double> &a = *(const YD1Args<double> *)args;
+            k_y_d1_pfa<P, Q><<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines), 32, smem, s>>>(a);
+            break;
+        }
+        case CT_FX_FWD:
+            k_x_filt_fwd_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XFiltFwdArgs<double> *)args);
+            break;
+        case CT_FY: {
+            const YFiltArgs<double> &a = *(const YFiltArgs<double> *)args;
+            k_y_filt_pfa<P, Q>
+                <<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines, a.nf), 32, smem, s>>>(a);
+            break;
+        }
+        case CT_FX_INV:
+            k_x_filt_inv_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XFiltInvArgs<double> *)args);
+            break;
         default:
             return cudaErrorInvalidValue;
     }

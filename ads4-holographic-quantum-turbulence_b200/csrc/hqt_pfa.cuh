@@ -143,43 +143,46 @@ template <int P, int Q> struct PfaWarp {
         }
     }
 
-    // Stage B on the CUDA cores, a lane per column (line, k2): Z(n1) of `in`
-    // (rows u = line*P + n1) -> forward P-point DFT -> times i*s1*kk
-    // (ORDER 1) or s2*kk^2 (ORDER 2), kk the signed wavenumber of
-    // k = CRT(k1, k2) -> inverse P-point DFT -> `out` (same rows).  The
-    // P-point DFTs use the real-pair form with cos/sin(2 pi j/P) in `cs`.
-    template <int ORDER>
-    __device__ __forceinline__ void stage_b_deriv(PfaBuf in, PfaBuf out, double s1, double s2,
-                                                  const double (&cs)[2][P]) const {
+    // Stage B on the CUDA cores, a lane per column (line, k2), in the
+    // real-pair form with cos/sin(2 pi j/P) in `cs`: values v(n1) of `in`
+    // (rows u = line*P + n1) -> forward P-point DFT if FWD -> mul(k1, k2,
+    // re, im) on every entry -> inverse P-point DFT if INV -> `out` (same
+    // rows).  mul gets (line, k1, k2, re, im).  The spectrum never goes to
+    // memory between the two DFTs.
+    template <bool FWD, bool INV, typename Mul>
+    __device__ __forceinline__ void stage_b(PfaBuf in, PfaBuf out, const double (&cs)[2][P],
+                                            Mul mul) const {
         constexpr int H = (P - 1) / 2;
 #pragma unroll 1
         for (int col = lane; col < D::CB; col += 32) {
             const int ln = col / Q, k2 = col - ln * Q;
-            double zr[P], zi[P];
+            double zr[P], zi[P], xr[P], xi[P];
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
                 zr[n1] = in.re[e];
                 zi[n1] = in.im[e];
             }
-            // forward: X_k = z0 + sum_t a_t cos - i b_t sin, X_{P-k} = ... + i ...
-            double xr[P], xi[P];
-            dft_real_pair<-1, H>(zr, zi, xr, xi, cs);
+            if (FWD) {
+                dft_real_pair<-1, H>(zr, zi, xr, xi, cs);
+            } else {
 #pragma unroll
-            for (int k1 = 0; k1 < P; ++k1) {
-                const int k = (Q * D::QIP * k1 + P * D::PIQ * k2) % N;
-                const double w = (double)(2 * k < N ? k : k - N);
-                if (ORDER == 1) {
-                    const double m = s1 * w, r = xr[k1];
-                    xr[k1] = -m * xi[k1];
-                    xi[k1] = m * r;
-                } else {
-                    const double m = s2 * w * w;
-                    xr[k1] *= m;
-                    xi[k1] *= m;
+                for (int k1 = 0; k1 < P; ++k1) {
+                    xr[k1] = zr[k1];
+                    xi[k1] = zi[k1];
                 }
             }
-            dft_real_pair<+1, H>(xr, xi, zr, zi, cs);
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) mul(ln, k1, k2, xr[k1], xi[k1]);
+            if (INV) {
+                dft_real_pair<+1, H>(xr, xi, zr, zi, cs);
+            } else {
+#pragma unroll
+                for (int k1 = 0; k1 < P; ++k1) {
+                    zr[k1] = xr[k1];
+                    zi[k1] = xi[k1];
+                }
+            }
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
@@ -187,6 +190,34 @@ template <int P, int Q> struct PfaWarp {
                 out.im[e] = zi[n1];
             }
         }
+    }
+
+    // natural index k of spectral entry (k1, k2): k = k1 mod P, k = k2 mod Q
+    __device__ __forceinline__ static int crt(int k1, int k2) {
+        return (Q * D::QIP * k1 + P * D::PIQ * k2) % N;
+    }
+    // its signed wavenumber (k or k - N)
+    __device__ __forceinline__ static double wavenumber(int k1, int k2) {
+        const int k = crt(k1, k2);
+        return (double)(2 * k < N ? k : k - N);
+    }
+
+    // derivative ORDER (1: i*s1*kk, 2: s2*kk^2) of a field after stage A
+    template <int ORDER>
+    __device__ __forceinline__ void stage_b_deriv(PfaBuf in, PfaBuf out, double s1, double s2,
+                                                  const double (&cs)[2][P]) const {
+        stage_b<true, true>(in, out, cs, [&](int, int k1, int k2, double &re, double &im) {
+            const double w = wavenumber(k1, k2);
+            if (ORDER == 1) {  // (i s1 w X): re = -s1 w X.im, im = s1 w X.re
+                const double m = s1 * w, r = re;
+                re = -m * im;
+                im = m * r;
+            } else {
+                const double m = s2 * w * w;
+                re *= m;
+                im *= m;
+            }
+        });
     }
 
     // P-point DFT of (xr, xi) into (yr, yi), sign SIGN, real-pair form.

@@ -48,11 +48,46 @@ template <int P, int Q> struct PfaLines {
     // elements of lines outside the grid are zeroed.  The caller commits.
     template <typename Re, typename Im>
     __device__ __forceinline__ void fetch(PfaBuf dst, Re re, Im im) const {
+        fetch(dst, re, im, [](int ln, int n) { return pos(ln, n); });
+    }
+    // ... at position at(ln, n) (spos for spectra in natural order)
+    template <typename Re, typename Im, typename At>
+    __device__ __forceinline__ void fetch(PfaBuf dst, Re re, Im im, At at) const {
         for (int e = lane; e < LN; e += 32) {
-            const int ln = e % kPfaLines, n = e / kPfaLines, i = pos(ln, n);
+            const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
             if (ln < valid) {
                 cp_async<8>(dst.re + i, re(ln, n));
                 cp_async<8>(dst.im + i, im(ln, n));
+            } else {
+                dst.re[i] = 0.0;
+                dst.im[i] = 0.0;
+            }
+        }
+    }
+    // position of spectral entry k (natural order) of line ln after stage B:
+    // row ln*P + k mod P, column k mod Q
+    __device__ __forceinline__ static int spos(int ln, int k) {
+        return (ln * P + k % P) * Q + k % Q;
+    }
+    // cp.async of a FieldIn (complex, or re with optional im) at element
+    // index gi(ln, n) into `dst` at position at(ln, n)
+    template <typename GI, typename At>
+    __device__ __forceinline__ void fetch_field(PfaBuf dst, const FieldIn<double> &f, GI gi,
+                                                At at) const {
+        for (int e = lane; e < LN; e += 32) {
+            const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
+            if (ln < valid) {
+                const long long g = gi(ln, n);
+                if (f.c) {
+                    cp_async<8>(dst.re + i, &f.c[g].x);
+                    cp_async<8>(dst.im + i, &f.c[g].y);
+                } else {
+                    cp_async<8>(dst.re + i, f.re + g);
+                    if (f.im)
+                        cp_async<8>(dst.im + i, f.im + g);
+                    else
+                        dst.im[i] = 0.0;
+                }
             } else {
                 dst.re[i] = 0.0;
                 dst.im[i] = 0.0;
@@ -227,8 +262,7 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         auto comb = [&](int k2, int k1, double c1x, double c1y, double c2x, double c2y,
                         double e1x, double e1y, double e2x, double e2y, double &sr, double &si,
                         double &tr, double &ti) {
-            const int k = (Q * D::QIP * k1 + P * D::PIQ * k2) % N;
-            const double kk = (double)(2 * k < N ? k : k - N);
+            const double kk = PfaWarp<P, Q>::wavenumber(k1, k2);
             const double m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = 0.5;
             const double axr = h * (c1x + c2x), axi = h * (c1y - c2y);
             const double ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
@@ -286,6 +320,200 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         a.divA[gi(ln, n)] = L.b1.re[i] + L.b0.re[i];
         a.dxB[gi(ln, n)] = L.b1.im[i] + L.b0.im[i];
     });
+}
+
+template <typename T>
+__device__ __forceinline__ void pfa_store_field(const FieldOut<T> &f, long long idx, double re,
+                                                double im) {
+    if (f.c) {
+        f.c[idx] = make_double2(re, im);
+        return;
+    }
+    if (f.re) f.re[idx] = re;
+    if (f.im) f.im[idx] = im;
+}
+
+// First x derivative of a field (x_d1 of hqt_cpasses.cuh).
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args<double> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<P, Q>;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int L0 = blockIdx.x * kPfaLines;
+    const long long g0 = (long long)L0 * N;
+    const L_t L(min(kPfaLines, a.nlines - L0));
+    auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
+    L.fetch_field(L.b0, a.in, gi, [](int ln, int n) { return L_t::pos(ln, n); });
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, 0.0, cs);
+    __syncwarp();
+    w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    L.each([&](int ln, int n, int i) { pfa_store_field(a.out, gi(ln, n), L.b1.re[i], L.b1.im[i]); });
+}
+
+// First y derivative of a field, optionally plus a real addend (y_d1).
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args<double> a) {
+    using L_t = PfaLines<P, Q>;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int x0 = blockIdx.x * kPfaLines;
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    const L_t L(min(kPfaLines, a.nx - x0));
+    auto gi = [&](int ln, int n) { return zoff + (long long)n * a.nx + ln; };
+    L.fetch_field(L.b0, a.in, gi, [](int ln, int n) { return L_t::pos(ln, n); });
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, 0.0, cs);
+    __syncwarp();
+    w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    L.each([&](int ln, int n, int i) {
+        const long long g = gi(ln, n);
+        const double re = L.b1.re[i] + (a.add_re ? a.add_re[g] : 0.0);
+        pfa_store_field(a.out, g, re, L.b1.im[i]);
+    });
+}
+
+// Filter, x forward: spectra along x of nf fields (field 0 times the winding
+// phase exp(-2 pi i y w / ny) when a status is given), natural order k.
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ XFiltFwdArgs<double> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<P, Q>;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int L0 = blockIdx.x * kPfaLines;
+    const long long g0 = (long long)L0 * N;
+    const L_t L(min(kPfaLines, a.nlines - L0));
+    auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
+    const int wnd = a.st ? a.st->winding : 0;
+#pragma unroll 1
+    for (int f = 0; f < a.nf; ++f) {
+        L.fetch_field(L.b0, a.in[f], gi, [](int ln, int n) { return L_t::pos(ln, n); });
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+        if (f == 0 && wnd != 0) {
+            // phase -2*pi*y*w/ny of line L0 + ln (tevol_driven_cluster.m:139)
+            L.each([&](int ln, int n, int i) {
+                const int y = (L0 + ln) % a.ny;
+                const long long qy = ((long long)y * wnd) % a.ny;
+                double sn, c;
+                sincospi(-2.0 * (double)qy / (double)a.ny, &sn, &c);
+                const double vr = L.b0.re[i], vi = L.b0.im[i];
+                L.b0.re[i] = vr * c - vi * sn;
+                L.b0.im[i] = vr * sn + vi * c;
+            });
+            __syncwarp();
+        }
+        w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+        __syncwarp();
+        w.template stage_b<true, false>(L.b0, L.b1, cs, [](int, int, int, double &, double &) {});
+        __syncwarp();
+        double2 *spec = a.spec[f];
+        for (int e = L.lane; e < L_t::LN; e += 32) {
+            const int ln = e % kPfaLines, k = e / kPfaLines;
+            if (ln < L.valid) {
+                const int i = L_t::spos(ln, k);
+                spec[gi(ln, k)] = make_double2(L.b1.re[i], L.b1.im[i]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Filter, y: along y of the x spectra, forward, weight
+// W = (M(kx,ky) + M(-kx,-ky))/2 * scale with M = mx(kx) my(ky), inverse.
+// blockIdx.y = z slice, blockIdx.z = field.
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFiltArgs<double> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<P, Q>;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int x0 = blockIdx.x * kPfaLines;
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    const L_t L(min(kPfaLines, a.nx - x0));
+    double2 *spec = a.spec[blockIdx.z];
+    auto gi = [&](int ln, int n) { return zoff + (long long)n * a.nx + ln; };
+    L.fetch(L.b0, [&](int ln, int n) { return &spec[gi(ln, n)].x; },
+            [&](int ln, int n) { return &spec[gi(ln, n)].y; });
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b<true, true>(L.b0, L.b1, cs,
+                                   [&](int ln, int k1, int k2, double &re, double &im) {
+        const int kx = x0 + min(ln, L.valid - 1);
+        const int kxm = (a.nx - kx) % a.nx;
+        const int ky = PfaWarp<P, Q>::crt(k1, k2), kym = (N - ky) % N;
+        const double wgt = 0.5 * (a.mx[kx] * a.my[ky] + a.mx[kxm] * a.my[kym]) * a.scale;
+        re *= wgt;
+        im *= wgt;
+    });
+    __syncwarp();
+    w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    L.each([&](int ln, int n, int i) { spec[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+}
+
+// Filter, x inverse: inverse transforms along x of nf spectra into the
+// fields; a non-finite value sets the status' first bad step.
+template <int P, int Q>
+__global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ XFiltInvArgs<double> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<P, Q>;
+    PfaWarp<P, Q> w;
+    w.init(g_pfa_frag);
+    double cs[2][P];
+    pfa_twiddles<P>(cs);
+    const int L0 = blockIdx.x * kPfaLines;
+    const long long g0 = (long long)L0 * N;
+    const L_t L(min(kPfaLines, a.nlines - L0));
+    auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
+    bool bad = false;
+#pragma unroll 1
+    for (int f = 0; f < a.nf; ++f) {
+        const double2 *spec = a.spec[f];
+        L.fetch(L.b0, [&](int ln, int k) { return &spec[gi(ln, k)].x; },
+                [&](int ln, int k) { return &spec[gi(ln, k)].y; },
+                [](int ln, int k) { return L_t::spos(ln, k); });
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+        w.template stage_b<false, true>(L.b0, L.b1, cs, [](int, int, int, double &, double &) {});
+        __syncwarp();
+        w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+        __syncwarp();
+        L.each([&](int ln, int n, int i) {
+            const double re = L.b1.re[i], im = L.b1.im[i];
+            if (!(isfinite(re) && isfinite(im))) bad = true;
+            pfa_store_field(a.out[f], gi(ln, n), re, im);
+        });
+        __syncwarp();
+    }
+    if (a.st && __any_sync(0xffffffffu, bad) && L.lane == 0)
+        atomicMin(reinterpret_cast<unsigned long long *>(&a.st->first_bad_step),
+                  (unsigned long long)(a.st->step + 1));
 }
 
 }  // namespace hqt
