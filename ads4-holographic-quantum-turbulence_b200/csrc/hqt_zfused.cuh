@@ -5,32 +5,37 @@
 // (:120-124,128).
 //
 // Every radial operator is an Nz x Nz matrix applied to all columns, i.e. a
-// product (Nz x Nz) x (Nz x columns).  A warp owns a tile of kZCols = 8
+// product (Nz x Nz) x (Nz x columns).  A warp owns a tile of kZCols = 4
 // adjacent (x, y) columns and runs each product on the FP64 tensor cores
-// (mma.sync m8n8k4 f64): the zero-padded Lz and Lz1 stay in the warp's
-// registers as A fragments for the life of the (persistent) warp, and the
-// column data is the B operand, read from the warp's own shared-memory tile.
-// The tile's inputs are staged there with cp.async in phase groups, so a
-// lane has tens of loads in flight, and buffers of finished phases are
-// refilled with the inputs of later ones while the current phase computes.
+// (mma.sync m8n8k4 f64).  The mma's 8 columns are (column, part) pairs: the
+// real and imaginary parts of Psi, or the x and y components of the gauge
+// field, so both gauge components share one product.  The zero-padded Lz and
+// Lz1 stay in the warp's registers as A fragments for the life of the
+// (persistent) warp; the column data is the B operand, read from the warp's
+// own shared-memory tile.  The tile's inputs are staged there with cp.async
+// in phase groups; buffers of finished phases are refilled with the inputs
+// of later ones (and of the next tile) while the current phase computes.
 // Warps share nothing, so there are no block barriers.
 //
 // Fragment layouts (g = lane/4, q = lane%4): A a0 = L[8m+g][4s+q];
-// B b0 = V[4s+q][col g]; C c_i = out[8m+g][col 2q+i].  Pointwise terms are
-// evaluated where the C fragments live: lane owns levels 8m+g, columns 2q
-// and 2q+1.
+// B b0 = V[level 4s+q][column g/2].part(g%2); C c_i = out[level 8m+g]
+// [column q].part(i).  A lane thus holds whole complex values (or both gauge
+// components) of levels 8m+g of column q, where the pointwise terms are
+// evaluated.  Each tile field is [level][4 columns]; operand reads, C-fragment
+// accesses and the cp.async fills are all contiguous runs of 32 lanes.
 //
 // Phases of a tile (MODE 1..4 = RK stage, MODE 0 = right-hand side only);
-// R, X1, X2 and V are the shared-memory regions of the warp:
-//   Gm  Psi, A_x, A_y, d_x Psi, d_y Psi -> R; A_x: d_x A_t, d_y B, state,
-//       accumulator -> X1 (issued while the previous tile finishes)
-//   Gy  A_y: d_y A_t, d_x B, state, accumulator -> X2
-//   Fx, Fy  g = d A_t + f Lz A, S = 1/2 Lz g +- 1/2 d B
-//       + Im(conj(Psi) d Psi) - A |Psi|^2 (:74-75), F = Lzr(S), RK update
-//   G2  A_t, d_z A_t, lap Psi, div A -> X1;  dp = Lz Psi -> V
-//   S1  d2 = Lz dp, S1 (:72-73), boundary row kb = Lz(nz,:) div A -> V
-//   G3  Psi state and accumulator -> X2, then Gm of the next tile
-//   F1  F1 = Lzr(S1), RK update of Psi (and of rhoi from kb)
+// R, G and V are the warp's shared-memory regions:
+//   Gm  Psi, (A_x, A_y), d_x Psi, d_y Psi -> R            (prefetched)
+//   Gg  (d_x A_t, d_y A_t), (d_y B, d_x B), state, accumulator -> G
+//   F3, F4  g = d A_t + f Lz A, S = 1/2 Lz g -+ 1/2 d B
+//           + Im(conj(Psi) d Psi) - A |Psi|^2 (:74-75), F = Lzr(S), RK update
+//   G2  A_t, d_z A_t, lap Psi, div A, Psi state and accumulator -> G;
+//       dp = Lz Psi -> V
+//   S1  d2 = Lz dp, S1 (:72-73), boundary row kb = Lz(nz,:) div A -> V;
+//       then Gm of the next tile
+//   F1  F1 = Lzr(S1), RK update of Psi (and of rhoi from kb); then Gg of the
+//       next tile
 // Reordering the stage's outputs this way is exact: they are disjoint and all
 // read the same stage inputs.
 #pragma once
@@ -41,7 +46,7 @@
 
 namespace hqt {
 
-constexpr int kZCols = 8;  // columns per warp tile (the n extent of one mma)
+constexpr int kZCols = 4;  // columns per warp tile (x 2 parts = the mma's n extent)
 
 // d += a * b on one 8x8x4 FP64 tensor-core tile
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
@@ -57,93 +62,100 @@ template <int NZP> struct ZmDims {
     static constexpr int LV = MP > KP ? MP : KP;  // levels stored per tile field
 };
 
-// Field of a tile in shared memory: element (level l, column c) at
-// l*8 + (c ^ ((l >> 1) & 7)).  Operand reads (4 levels x 8 columns) and the
-// fill stay permutations of whole rows; the swizzle makes the accesses at
-// the C-fragment positions (8 levels x 4 column pairs) conflict-free.
+// Field of a tile in shared memory: element (level l, column c) at l*4 + c.
 template <typename V> struct ZTileF {
     V *p;
-    __device__ __forceinline__ V &operator()(int l, int c) const {
-        return p[l * kZCols + (c ^ ((l >> 1) & 7))];
-    }
+    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZCols + c]; }
 };
 
-template <typename T, typename TS, typename TD, int NZP> struct ZfLayout {
+template <typename TD, int NZP> struct ZfLayout {
     static constexpr int L = ZmDims<NZP>::LV * kZCols;
-    static constexpr int c = L * (int)sizeof(C2<T>), r = L * (int)sizeof(T);
+    static constexpr int c = L * 16, r = L * 8;  // complex / pair, real (double)
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
-    static constexpr int sc = L * (int)sizeof(C2<TS>), sr = L * (int)sizeof(TS);
     static constexpr int mx(int a, int b) { return a > b ? a : b; }
-    // R: Psi, A_x, A_y, d_x Psi, d_y Psi
-    static constexpr int oPS = 0, oAX = oPS + c, oAY = oAX + r, oDXP = oAY + r,
-                         oDYP = oDXP + dc, oX1 = oDYP + dc;
-    // X1 (phase P2): A_t, d_z A_t, lap Psi, div A; later the A_x inputs
-    static constexpr int gsz = 2 * dr + 2 * sr;  // one gauge component's inputs
-    static constexpr int x1 = mx(2 * r + dc + dr, gsz);
-    static constexpr int oX2 = oX1 + x1;
-    // X2 (phase P3): Psi state and accumulator; later the A_y inputs
-    static constexpr int x2 = mx(2 * sc, gsz);
-    static constexpr int oV = oX2 + x2;
-    // V: dp then S1 (complex); later g and S of a gauge component (real)
-    static constexpr int v = mx(c, 2 * r);
-    static constexpr int bytes = oV + v;
+    // R: Psi, (A_x, A_y), d_x Psi, d_y Psi
+    static constexpr int oPS = 0, oAXY = c, oDXP = 2 * c, oDYP = 2 * c + dc, oG = 2 * c + 2 * dc;
+    // G, gauge phase: (d_x A_t, d_y A_t), (d_y B, d_x B), state, accumulator
+    static constexpr int gDT = 0, gBF = dc, gZA = 2 * dc, gKA = 2 * dc + c;
+    static constexpr int gsz = 2 * dc + 2 * c;
+    // G, Psi phase: A_t, d_z A_t, lap Psi, div A, Psi state and accumulator
+    static constexpr int pAT = 0, pDAT = r, pLAP = 2 * r, pDIV = 2 * r + dc;
+    static constexpr int pZP = ((pDIV + dr + 15) / 16) * 16, pKP = pZP + c;
+    static constexpr int psz = pKP + c;
+    static constexpr int oV = oG + mx(gsz, psz);
+    // V: dp then S1 (Psi phase); g and S of the gauge phase
+    static constexpr int oVG = oV, oVS = oV + c;
+    static constexpr int bytes = oV + 2 * c;
 };
 
 template <typename T, typename TS, typename TD, int NZP>
 __host__ __device__ constexpr int zf_smem_bytes() {
-    return ZfLayout<T, TS, TD, NZP>::bytes;
+    return ZfLayout<TD, NZP>::bytes;
 }
 
-// Stage levels 0..nz-1 of one field of the tile starting at site0.
-template <typename V>
-__device__ __forceinline__ void zf_stage(ZTileF<V> dst, const V *src, int nz, long long P,
-                                         long long site0, int lane) {
+// ---- staging of levels 0..nz-1 of the tile starting at site0 --------------
+// A compile-time trip count (NZP levels) with predicated copies: every lane
+// runs the same instructions, so the loops do not diverge.
+template <int NZP, typename V>
+__device__ __forceinline__ void zf_real(ZTileF<V> dst, const V *src, int nz, long long P,
+                                        long long site0, int lane) {
     if (!src) return;
-    for (int e = lane; e < nz * kZCols; e += 32) {
-        const int l = e >> 3, c = e & 7;
-        if (site0 + c < P) cp_async<sizeof(V)>(&dst(l, c), src + l * P + site0 + c);
+#pragma unroll
+    for (int it = 0; it < (NZP * kZCols + 31) / 32; ++it) {
+        const int e = lane + 32 * it, l = e >> 2, c = e & 3;
+        if (l < nz && site0 + c < P) cp_async<sizeof(V)>(&dst(l, c), src + l * P + site0 + c);
+    }
+}
+template <int NZP, typename V>
+__device__ __forceinline__ void zf_pair(ZTileF<C2<V>> dst, const V *sx, const V *sy, int nz,
+                                        long long P, long long site0, int lane) {
+    if (!sx || !sy) return;
+#pragma unroll
+    for (int it = 0; it < (NZP * kZCols + 31) / 32; ++it) {
+        const int e = lane + 32 * it, l = e >> 2, c = e & 3;
+        if (l < nz && site0 + c < P) {
+            const long long gi = l * P + site0 + c;
+            cp_async<sizeof(V)>(&dst(l, c).x, sx + gi);
+            cp_async<sizeof(V)>(&dst(l, c).y, sy + gi);
+        }
     }
 }
 
-// out = L V for a real tile field V (levels >= nz hold zero)
+// Sum over the 8 lane groups g = lane/4 (same column q): after the shuffles
+// every lane holds the total of its column.
+__device__ __forceinline__ double zf_colsum(double v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    return v;
+}
+
+// out = L V for a pair tile V (levels >= nz hold zero): C[m][i] is part i of
+// level 8m+g, column q
 template <int MT, int KS>
-__device__ __forceinline__ void zm_real(const double (&A)[MT][KS], ZTileF<double> V,
-                                        double (&C)[MT][2], int g, int q) {
+__device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double2> V,
+                                        double (&C)[MT][2], int lane) {
+    const double *v = reinterpret_cast<const double *>(V.p);
+    const int g = lane >> 2, q = lane & 3;
 #pragma unroll
     for (int m = 0; m < MT; ++m) C[m][0] = C[m][1] = 0.0;
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
-        const double b = V(4 * s + q, g);
+        const double b = v[(4 * s + q) * 8 + g];
 #pragma unroll
         for (int m = 0; m < MT; ++m) dmma(C[m][0], C[m][1], A[m][s], b);
-    }
-}
-// re/im of out = L V for a complex tile field
-template <int MT, int KS>
-__device__ __forceinline__ void zm_cplx(const double (&A)[MT][KS], ZTileF<double2> V,
-                                        double (&Cr)[MT][2], double (&Ci)[MT][2], int g, int q) {
-#pragma unroll
-    for (int m = 0; m < MT; ++m) Cr[m][0] = Cr[m][1] = Ci[m][0] = Ci[m][1] = 0.0;
-#pragma unroll
-    for (int s = 0; s < KS; ++s) {
-        const double2 b = V(4 * s + q, g);
-#pragma unroll
-        for (int m = 0; m < MT; ++m) {
-            dmma(Cr[m][0], Cr[m][1], A[m][s], b.x);
-            dmma(Ci[m][0], Ci[m][1], A[m][s], b.y);
-        }
     }
 }
 
 // T = TS = double (state and arithmetic); TD = double or float (derivative
 // fields of the line passes).
 template <typename T, typename TS, typename TD, int NZP, int MODE>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(32, 12)
     k_zstage(const __grid_constant__ ZStageArgs<T, TS, TD> a,
              const __grid_constant__ ZOps<T, NZP> op) {
     static_assert(std::is_same<T, double>::value && std::is_same<TS, double>::value,
                   "FP64 columns");
-    using Lay = ZfLayout<T, TS, TD, NZP>;
+    using Lay = ZfLayout<TD, NZP>;
     using D = ZmDims<NZP>;
     constexpr int MT = D::MT, KS = D::KS;
     const int lane = threadIdx.x, g = lane >> 2, q = lane & 3;
@@ -164,295 +176,271 @@ __global__ void __launch_bounds__(32)
             ALz[m][s] = in ? op.Lz[in ? i : 0][in ? j : 0] : 0.0;
             ALz1[m][s] = in ? op.Lz1[in ? i : 0][in ? j : 0] : 0.0;
         }
-    double zr[MT], fzr[MT];  // z and f = 1 - z^3 at this lane's levels
+    // z, f = 1 - z^3 and the boundary row Lz(nz, i) at this lane's levels
+    // i = 8m + g (zero past nz: the padded entries of op are zero)
+    double zr[MT], fzr[MT], lzr[MT];
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
         const int i = 8 * m + g;
         zr[m] = i < NZP ? op.zz[i < NZP ? i : 0] : 0.0;
         fzr[m] = i < NZP ? op.fz[i < NZP ? i : 0] : 0.0;
+        lzr[m] = i < NZP ? op.lzb[i < NZP ? i : 0] : 0.0;
     }
     __syncwarp();
 
-    const ZTileF<C2<T>> PS{reinterpret_cast<C2<T> *>(sm + Lay::oPS)};
-    const ZTileF<T> AX{reinterpret_cast<T *>(sm + Lay::oAX)};
-    const ZTileF<T> AY{reinterpret_cast<T *>(sm + Lay::oAY)};
+    const ZTileF<double2> PS{reinterpret_cast<double2 *>(sm + Lay::oPS)};
+    const ZTileF<double2> AXY{reinterpret_cast<double2 *>(sm + Lay::oAXY)};
     const ZTileF<C2<TD>> DXP{reinterpret_cast<C2<TD> *>(sm + Lay::oDXP)};
     const ZTileF<C2<TD>> DYP{reinterpret_cast<C2<TD> *>(sm + Lay::oDYP)};
-    const ZTileF<T> AT{reinterpret_cast<T *>(sm + Lay::oX1)};
-    const ZTileF<T> DAT{reinterpret_cast<T *>(sm + Lay::oX1 + Lay::r)};
-    const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(sm + Lay::oX1 + 2 * Lay::r)};
-    const ZTileF<TD> DIV{reinterpret_cast<TD *>(sm + Lay::oX1 + 2 * Lay::r + Lay::dc)};
-    const ZTileF<C2<TS>> ZP{reinterpret_cast<C2<TS> *>(sm + Lay::oX2)};
-    const ZTileF<C2<TS>> KP{reinterpret_cast<C2<TS> *>(sm + Lay::oX2 + Lay::sc)};
-    const ZTileF<C2<T>> VC{reinterpret_cast<C2<T> *>(sm + Lay::oV)};
-    const ZTileF<T> VG{reinterpret_cast<T *>(sm + Lay::oV)};
-    const ZTileF<T> VS{reinterpret_cast<T *>(sm + Lay::oV + Lay::r)};
-    auto gauge_tiles = [&](int off, ZTileF<TD> &dt, ZTileF<TD> &bf, ZTileF<TS> &za,
-                           ZTileF<TS> &ka) {
-        dt.p = reinterpret_cast<TD *>(sm + off);
-        bf.p = reinterpret_cast<TD *>(sm + off + Lay::dr);
-        za.p = reinterpret_cast<TS *>(sm + off + 2 * Lay::dr);
-        ka.p = reinterpret_cast<TS *>(sm + off + 2 * Lay::dr + Lay::sr);
-    };
+    unsigned char *gr = sm + Lay::oG;
+    const ZTileF<C2<TD>> DT{reinterpret_cast<C2<TD> *>(gr + Lay::gDT)};
+    const ZTileF<C2<TD>> BF{reinterpret_cast<C2<TD> *>(gr + Lay::gBF)};
+    const ZTileF<double2> ZA{reinterpret_cast<double2 *>(gr + Lay::gZA)};
+    const ZTileF<double2> KA{reinterpret_cast<double2 *>(gr + Lay::gKA)};
+    const ZTileF<T> AT{reinterpret_cast<T *>(gr + Lay::pAT)};
+    const ZTileF<T> DAT{reinterpret_cast<T *>(gr + Lay::pDAT)};
+    const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(gr + Lay::pLAP)};
+    const ZTileF<TD> DIV{reinterpret_cast<TD *>(gr + Lay::pDIV)};
+    const ZTileF<double2> ZP{reinterpret_cast<double2 *>(gr + Lay::pZP)};
+    const ZTileF<double2> KP{reinterpret_cast<double2 *>(gr + Lay::pKP)};
+    const ZTileF<double2> VC{reinterpret_cast<double2 *>(sm + Lay::oV)};
+    const ZTileF<double2> VG{reinterpret_cast<double2 *>(sm + Lay::oVG)};
+    const ZTileF<double2> VS{reinterpret_cast<double2 *>(sm + Lay::oVS)};
     constexpr bool kReadK = (MODE >= 2);
-    // inputs of one gauge component: d A_t, d B, state, accumulator
-    auto stage_gauge = [&](int comp, int off, long long site0) {
-        ZTileF<TD> dt, bf;
-        ZTileF<TS> za, ka;
-        gauge_tiles(off, dt, bf, za, ka);
-        zf_stage<TD>(dt, comp == 0 ? a.dxat : a.dyat, nz, P, site0, lane);
-        zf_stage<TD>(bf, comp == 0 ? a.dyB : a.dxB, nz, P, site0, lane);
+
+    auto stage_main = [&](long long site0) {
+        zf_real<NZP, double2>(PS, a.ypsi, nz, P, site0, lane);
+        zf_pair<NZP, double>(AXY, a.yax, a.yay, nz, P, site0, lane);
+        zf_real<NZP, C2<TD>>(DXP, a.dxpsi, nz, P, site0, lane);
+        zf_real<NZP, C2<TD>>(DYP, a.dypsi, nz, P, site0, lane);
+    };
+    auto stage_gauge = [&](long long site0) {
+        zf_pair<NZP, TD>(DT, a.dxat, a.dyat, nz, P, site0, lane);
+        // F3 takes -d_y B, F4 takes +d_x B: stored as (d_y B, d_x B)
+        zf_pair<NZP, TD>(BF, a.dyB, a.dxB, nz, P, site0, lane);
         if (MODE >= 1) {
-            zf_stage<TS>(za, comp == 0 ? a.zax : a.zay, nz, P, site0, lane);
-            if (kReadK) zf_stage<TS>(ka, comp == 0 ? a.kax : a.kay, nz, P, site0, lane);
+            zf_pair<NZP, double>(ZA, a.zax, a.zay, nz, P, site0, lane);
+            if (kReadK) zf_pair<NZP, double>(KA, a.kax, a.kay, nz, P, site0, lane);
         }
     };
+
     const long long ntiles = (P + kZCols - 1) / kZCols;
-    // G_main: Psi, A_x, A_y, d_x Psi, d_y Psi (R) and the A_x inputs (X1)
-    auto stage_main = [&](long long site0) {
-        zf_stage<C2<T>>(PS, a.ypsi, nz, P, site0, lane);
-        zf_stage<T>(AX, a.yax, nz, P, site0, lane);
-        zf_stage<T>(AY, a.yay, nz, P, site0, lane);
-        zf_stage<C2<TD>>(DXP, a.dxpsi, nz, P, site0, lane);
-        zf_stage<C2<TD>>(DYP, a.dypsi, nz, P, site0, lane);
-        stage_gauge(0, Lay::oX1, site0);
-    };
-    if ((long long)blockIdx.x < ntiles) stage_main((long long)blockIdx.x * kZCols);
+    if ((long long)blockIdx.x < ntiles) {
+        stage_main((long long)blockIdx.x * kZCols);
+        stage_gauge((long long)blockIdx.x * kZCols);
+    }
     cp_commit();
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long site0 = tile * kZCols;
-        stage_gauge(1, Lay::oX2, site0);  // G_y
-        cp_commit();
-
-        // ---- F3 (A_x), then F4 (A_y) --------------------------------------
-#pragma unroll 1
-        for (int comp = 0; comp < 2; ++comp) {
-            if (comp == 0)
-                cp_wait<1>();  // G_main
-            else
-                cp_wait<0>();  // G_y
-            __syncwarp();
-            ZTileF<TD> DT, BF;
-            ZTileF<TS> ZA, KA;
-            gauge_tiles(comp == 0 ? Lay::oX1 : Lay::oX2, DT, BF, ZA, KA);
-            const ZTileF<T> A = comp == 0 ? AX : AY;
-            const ZTileF<C2<TD>> DPS = comp == 0 ? DXP : DYP;
-            // boundary-row contraction Lz(nz,:) A (mixed precision forms F2 from it)
-            if (a.f2x && lane < kZCols && site0 + lane < P) {
-                T bnd = T(0);
-#pragma unroll
-                for (int j = 0; j < NZP; ++j)
-                    if (j < nz) bnd = fma(op.lzb[j], A(j, lane), bnd);
-                (comp == 0 ? a.f2x : a.f2y)[site0 + lane] = bnd;
-            }
-            // g = d A_t + f Lz A
-            {
-                double c[MT][2];
-                zm_real<MT, KS>(ALz, A, c, g, q);
-#pragma unroll
-                for (int m = 0; m < MT; ++m) {
-                    const int i = 8 * m + g;
-#pragma unroll
-                    for (int h = 0; h < 2; ++h)
-                        VG(i, 2 * q + h) = (i < nz) ? T(DT(i, 2 * q + h)) + fzr[m] * c[m][h] : T(0);
-                }
-            }
-            __syncwarp();
-            // S = 1/2 Lz g -/+ 1/2 d B + Im(conj(Psi) d Psi) - A |Psi|^2
-            {
-                double d[MT][2];
-                zm_real<MT, KS>(ALz, VG, d, g, q);
-#pragma unroll
-                for (int m = 0; m < MT; ++m) {
-                    const int i = 8 * m + g;
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int cc = 2 * q + h;
-                        T s = T(0);
-                        if (i < nz) {
-                            const C2<T> ps = PS(i, cc);
-                            const C2<TD> ddd = DPS(i, cc);
-                            const T bf = comp == 0 ? -T(BF(i, cc)) : T(BF(i, cc));
-                            const T av = A(i, cc);
-                            s = T(0.5) * d[m][h] + T(0.5) * bf +
-                                (ps.x * T(ddd.y) - ps.y * T(ddd.x)) -
-                                av * (ps.x * ps.x + ps.y * ps.y);
-                        }
-                        VS(i, cc) = s;
-                    }
-                }
-            }
-            __syncwarp();
-            // F = Lzr(S) (rows < nz-1 of Lz1, zero on the boundary row) and the update
-            {
-                double fr[MT][2];
-                zm_real<MT, KS>(ALz1, VS, fr, g, q);
-#pragma unroll
-                for (int m = 0; m < MT; ++m) {
-                    const int i = 8 * m + g;
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int cc = 2 * q + h;
-                        const long long site = site0 + cc;
-                        if (i >= nz || site >= P) continue;
-                        const long long gi = (long long)i * P + site;
-                        if (MODE == 0) {
-                            (comp == 0 ? a.f3 : a.f4)[gi] = fr[m][h];
-                            continue;
-                        }
-                        const TS k = a.h * TS(fr[m][h]);
-                        const TS z = ZA(i, cc);
-                        if (MODE == 4) {
-                            (comp == 0 ? a.wax : a.way)[gi] = z + (TS(1) / TS(6)) * (KA(i, cc) + k);
-                            continue;
-                        }
-                        TS *kacc = comp == 0 ? a.kax : a.kay;
-                        kacc[gi] = (MODE == 1) ? k : KA(i, cc) + 2 * k;
-                        const TS nv = (MODE == 3) ? z + k : z + k / 2;
-                        (comp == 0 ? a.nax : a.nay)[gi] = T(nv);
-                        TD *nd = comp == 0 ? a.nax_d : a.nay_d;
-                        if (nd) {
-                            const TS mean =
-                                a.slice_mean ? a.slice_mean[5 * i + 3 + comp] : TS(0);
-                            nd[gi] = TD(nv - mean);
-                        }
-                    }
-                }
-            }
-            __syncwarp();  // V (and, after A_x, the X1 inputs) are free
-        }
-
-        // ---- Psi: A_t, d_z A_t, lap Psi, div A into X1 -----------------------
-        zf_stage<T>(AT, a.at, nz, P, site0, lane);
-        zf_stage<T>(DAT, a.dat, nz, P, site0, lane);
-        zf_stage<C2<TD>>(LAP, a.lap, nz, P, site0, lane);
-        zf_stage<TD>(DIV, a.divA, nz, P, site0, lane);
-        cp_commit();
-
-        // dp = Lz Psi
-        {
-            double cr[MT][2], ci[MT][2];
-            zm_cplx<MT, KS>(ALz, PS, cr, ci, g, q);
-#pragma unroll
-            for (int m = 0; m < MT; ++m)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(cr[m][h], ci[m][h]);
-        }
+        const long long next = tile + gridDim.x;
+        const long long site = site0 + q;  // this lane's column in C layout
         cp_wait<0>();
         __syncwarp();
 
-        // d2 = Lz dp, S1, and the boundary row of F2
-        T kb = T(0);  // lanes 0..7: column `lane`
-        if (lane < kZCols) {
-#pragma unroll
-            for (int i = 0; i < NZP; ++i)
-                if (i < nz) kb = fma(op.lzb[i], T(DIV(i, lane)), kb);
-        }
-        double s1r[MT][2], s1i[MT][2];
-        {
-            double d2r[MT][2], d2i[MT][2];
-            zm_cplx<MT, KS>(ALz, VC, d2r, d2i, g, q);
+        // ---- F3, F4: both gauge components at once -------------------------
+        if (a.f2x) {
+            // boundary-row contractions Lz(nz,:) A (mixed precision forms F2)
+            double bx = 0.0, by = 0.0;
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
-                const int i = 8 * m + g;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int cc = 2 * q + h;
-                    s1r[m][h] = s1i[m][h] = 0.0;
-                    if (i < nz - 1) {
-                        const C2<T> ps = PS(i, cc);
-                        const T at = AT(i, cc), dat = DAT(i, cc), ax = AX(i, cc), ay = AY(i, cc);
-                        const C2<TD> lpd = LAP(i, cc), dxd = DXP(i, cc), dyd = DYP(i, cc);
-                        const T dv = T(DIV(i, cc));
-                        const C2<T> d1 = VC(i, cc);
-                        const T z = zr[m], f = fzr[m], hh = T(0.5);
-                        const T a2 = ax * ax + ay * ay;
-                        const T u = ax * T(dxd.x) + ay * T(dyd.x);
-                        const T w = ax * T(dxd.y) + ay * T(dyd.y);
-                        s1r[m][h] = -at * d1.y - hh * dat * ps.y + hh * f * d2r[m][h] -
-                                    T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
-                                    hh * T(lpd.x) + hh * dv * ps.y + w;
-                        s1i[m][h] = at * d1.x + hh * dat * ps.x + hh * f * d2i[m][h] -
-                                    T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
-                                    hh * T(lpd.y) - hh * dv * ps.x - u;
-                    }
-                }
+                const double2 v = AXY(8 * m + g, q);
+                bx = fma(lzr[m], v.x, bx);
+                by = fma(lzr[m], v.y, by);
+            }
+            bx = zf_colsum(bx);
+            by = zf_colsum(by);
+            if (g == 0 && site < P) {
+                a.f2x[site] = bx;
+                a.f2y[site] = by;
             }
         }
-        __syncwarp();  // every read of dp, R and X1 is done
+        {  // g = d A_t + f Lz A
+            double c[MT][2];
+            zm_pair<MT, KS>(ALz, AXY, c, lane);
 #pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) VC(8 * m + g, 2 * q + h) = mk2<T>(s1r[m][h], s1i[m][h]);
-        if (MODE >= 1) {  // Psi state and accumulator into X2
-            zf_stage<C2<TS>>(ZP, a.zpsi, nz, P, site0, lane);
-            if (kReadK) zf_stage<C2<TS>>(KP, a.kpsi, nz, P, site0, lane);
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g, ic = i < nz ? i : nz - 1;
+                const C2<TD> dt = DT(ic, q);
+                const bool in = i < nz;
+                VG(i, q) = make_double2(in ? T(dt.x) + fzr[m] * c[m][0] : 0.0,
+                                        in ? T(dt.y) + fzr[m] * c[m][1] : 0.0);
+            }
         }
-        cp_commit();
-        // the next tile's main inputs load while this tile finishes
-        if (tile + gridDim.x < ntiles) stage_main((tile + gridDim.x) * kZCols);
-        cp_commit();
-        cp_wait<1>();
         __syncwarp();
-
-        // ---- F1 = Lzr(S1) and the RK update of Psi ------------------------------
-        {
-            double fr[MT][2], fi[MT][2];
-            zm_cplx<MT, KS>(ALz1, VC, fr, fi, g, q);
+        {  // S = 1/2 Lz g -+ 1/2 d B + Im(conj(Psi) d Psi) - A |Psi|^2
+            double d[MT][2];
+            zm_pair<MT, KS>(ALz, VG, d, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g, ic = i < nz ? i : nz - 1;
+                const double2 ps = PS(ic, q), av = AXY(ic, q);
+                const C2<TD> dx = DXP(ic, q), dy = DYP(ic, q), bf = BF(ic, q);
+                const double p2 = ps.x * ps.x + ps.y * ps.y;
+                const double vx = T(0.5) * d[m][0] + T(0.5) * -T(bf.x) +
+                                  (ps.x * T(dx.y) - ps.y * T(dx.x)) - av.x * p2;
+                const double vy = T(0.5) * d[m][1] + T(0.5) * T(bf.y) +
+                                  (ps.x * T(dy.y) - ps.y * T(dy.x)) - av.y * p2;
+                const bool in = i < nz;
+                VS(i, q) = make_double2(in ? vx : 0.0, in ? vy : 0.0);
+            }
+        }
+        __syncwarp();
+        {  // F = Lzr(S) (rows < nz-1 of Lz1, zero on the boundary row), update
+            double f[MT][2];
+            zm_pair<MT, KS>(ALz1, VS, f, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int cc = 2 * q + h;
-                    const long long site = site0 + cc;
-                    if (i >= nz || site >= P) continue;
-                    const long long gi = (long long)i * P + site;
-                    if (MODE == 0) {
-                        a.f1[gi] = mk2<T>(fr[m][h], fi[m][h]);
-                        continue;
-                    }
-                    const C2<TS> k = mk2<TS>(a.h * TS(fr[m][h]), a.h * TS(fi[m][h]));
-                    const C2<TS> z = ZP(i, cc);
-                    if (MODE == 4) {
-                        const C2<TS> K = KP(i, cc);
-                        const TS s = TS(1) / TS(6);
-                        a.wpsi[gi] = mk2<TS>(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
-                        continue;
-                    }
-                    if (MODE == 1) {
-                        a.kpsi[gi] = k;
-                    } else {
-                        const C2<TS> K = KP(i, cc);
-                        a.kpsi[gi] = mk2<TS>(K.x + 2 * k.x, K.y + 2 * k.y);
-                    }
-                    const C2<TS> nv = (MODE == 3) ? mk2<TS>(z.x + k.x, z.y + k.y)
-                                                  : mk2<TS>(z.x + k.x / 2, z.y + k.y / 2);
-                    a.npsi[gi] = mk2<T>(T(nv.x), T(nv.y));
-                    if (a.npsi_d) {
-                        const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
-                        const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
-                        a.npsi_d[gi] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
-                    }
+                if (i >= nz || site >= P) continue;
+                const long long gi = (long long)i * P + site;
+                if (MODE == 0) {
+                    a.f3[gi] = f[m][0];
+                    a.f4[gi] = f[m][1];
+                    continue;
+                }
+                const TS kx = a.h * TS(f[m][0]), ky = a.h * TS(f[m][1]);
+                const double2 z = ZA(i, q);
+                if (MODE == 4) {
+                    const double2 K = KA(i, q);
+                    a.wax[gi] = z.x + (TS(1) / TS(6)) * (K.x + kx);
+                    a.way[gi] = z.y + (TS(1) / TS(6)) * (K.y + ky);
+                    continue;
+                }
+                if (MODE == 1) {
+                    a.kax[gi] = kx;
+                    a.kay[gi] = ky;
+                } else {
+                    const double2 K = KA(i, q);
+                    a.kax[gi] = K.x + 2 * kx;
+                    a.kay[gi] = K.y + 2 * ky;
+                }
+                const TS nx = (MODE == 3) ? z.x + kx : z.x + kx / 2;
+                const TS ny = (MODE == 3) ? z.y + ky : z.y + ky / 2;
+                a.nax[gi] = T(nx);
+                a.nay[gi] = T(ny);
+                if (a.nax_d) {
+                    const TS mx = a.slice_mean ? a.slice_mean[5 * i + 3] : TS(0);
+                    const TS my = a.slice_mean ? a.slice_mean[5 * i + 4] : TS(0);
+                    a.nax_d[gi] = TD(nx - mx);
+                    a.nay_d[gi] = TD(ny - my);
                 }
             }
         }
-        if (lane < kZCols && site0 + lane < P) {
-            const long long site = site0 + lane;
+        __syncwarp();  // G and V are free
+
+        // ---- Psi ---------------------------------------------------------------
+        zf_real<NZP, T>(AT, a.at, nz, P, site0, lane);
+        zf_real<NZP, T>(DAT, a.dat, nz, P, site0, lane);
+        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, lane);
+        zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, lane);
+        if (MODE >= 1) {
+            zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, lane);
+            if (kReadK) zf_real<NZP, double2>(KP, a.kpsi, nz, P, site0, lane);
+        }
+        cp_commit();
+        {  // dp = Lz Psi
+            double c[MT][2];
+            zm_pair<MT, KS>(ALz, PS, c, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) VC(8 * m + g, q) = make_double2(c[m][0], c[m][1]);
+        }
+        cp_wait<0>();
+        __syncwarp();
+        // boundary row of F2: kb = Lz(nz,:) div A of column q, in every lane
+        T kb = T(0);
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            const int i = 8 * m + g;
+            kb = fma(lzr[m], (i < nz) ? T(DIV(i < nz ? i : 0, q)) : T(0), kb);
+        }
+        kb = zf_colsum(kb);
+        double s1[MT][2];
+        {  // d2 = Lz dp and S1
+            double d2[MT][2];
+            zm_pair<MT, KS>(ALz, VC, d2, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                const int ic = i < nz - 1 ? i : 0;
+                const double2 ps = PS(ic, q), av = AXY(ic, q), d1 = VC(ic, q);
+                const T at = AT(ic, q), dat = DAT(ic, q);
+                const C2<TD> lp = LAP(ic, q), dx = DXP(ic, q), dy = DYP(ic, q);
+                const T dv = T(DIV(ic, q));
+                const T z = zr[m], f = fzr[m], hh = T(0.5);
+                const T a2 = av.x * av.x + av.y * av.y;
+                const T u = av.x * T(dx.x) + av.y * T(dy.x);
+                const T w = av.x * T(dx.y) + av.y * T(dy.y);
+                const T r0 = -at * d1.y - hh * dat * ps.y + hh * f * d2[m][0] -
+                             T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
+                             hh * T(lp.x) + hh * dv * ps.y + w;
+                const T r1 = at * d1.x + hh * dat * ps.x + hh * f * d2[m][1] -
+                             T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
+                             hh * T(lp.y) - hh * dv * ps.x - u;
+                const bool in = i < nz - 1;
+                s1[m][0] = in ? r0 : 0.0;
+                s1[m][1] = in ? r1 : 0.0;
+            }
+        }
+        __syncwarp();  // every read of dp and of R is done
+#pragma unroll
+        for (int m = 0; m < MT; ++m) VC(8 * m + g, q) = make_double2(s1[m][0], s1[m][1]);
+        if (next < ntiles) stage_main(next * kZCols);  // the next tile's R loads now
+        cp_commit();
+        __syncwarp();
+        {  // F1 = Lzr(S1) and the RK update of Psi
+            double f[MT][2];
+            zm_pair<MT, KS>(ALz1, VC, f, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                if (i >= nz || site >= P) continue;
+                const long long gi = (long long)i * P + site;
+                if (MODE == 0) {
+                    a.f1[gi] = make_double2(f[m][0], f[m][1]);
+                    continue;
+                }
+                const double2 k = make_double2(a.h * f[m][0], a.h * f[m][1]);
+                const double2 z = ZP(i, q);
+                if (MODE == 4) {
+                    const double2 K = KP(i, q);
+                    const TS s = TS(1) / TS(6);
+                    a.wpsi[gi] = make_double2(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
+                    continue;
+                }
+                if (MODE == 1) {
+                    a.kpsi[gi] = k;
+                } else {
+                    const double2 K = KP(i, q);
+                    a.kpsi[gi] = make_double2(K.x + 2 * k.x, K.y + 2 * k.y);
+                }
+                const double2 nv = (MODE == 3) ? make_double2(z.x + k.x, z.y + k.y)
+                                               : make_double2(z.x + k.x / 2, z.y + k.y / 2);
+                a.npsi[gi] = nv;
+                if (a.npsi_d) {
+                    const TS mr = a.slice_mean ? a.slice_mean[5 * i] : TS(0);
+                    const TS mi = a.slice_mean ? a.slice_mean[5 * i + 1] : TS(0);
+                    a.npsi_d[gi] = mk2<TD>(TD(nv.x - mr), TD(nv.y - mi));
+                }
+            }
+        }
+        if (g == 0 && site < P) {
+            const long long sl = site;
             if (MODE == 0) {
-                a.f2b[site] = kb;
+                a.f2b[sl] = kb;
             } else if (!a.f2x) {
                 const TS k = a.h * TS(kb);
                 if (MODE == 1)
-                    a.krho[site] = k;
+                    a.krho[sl] = k;
                 else if (MODE == 2 || MODE == 3)
-                    a.krho[site] = a.krho[site] + 2 * k;
+                    a.krho[sl] = a.krho[sl] + 2 * k;
                 else  // rhoi = rhoi - k2(:,:,nz), k2 = (1/6)(k21+2k22+2k23+k24)
-                    a.wrho[site] = a.zrho[site] - (TS(1) / TS(6)) * (a.krho[site] + k);
+                    a.wrho[sl] = a.zrho[sl] - (TS(1) / TS(6)) * (a.krho[sl] + k);
             }
         }
-        __syncwarp();  // X2 and V are free for the next tile
+        __syncwarp();  // G and V are free for the next tile
+        if (next < ntiles) stage_gauge(next * kZCols);
+        cp_commit();
     }
     cp_wait<0>();
 }
