@@ -367,6 +367,10 @@ int launch_x_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *
     a.E = c->E32;
     a.dxxay = c->dxxay32;
     Prof pr(c, K_X_RHS);
+    if (c->px) {
+        CK(pfa_launch_301(CT_X_RHS_F, &a, a.nlines, c->stream));
+        return HQT_OK;
+    }
     if (c->cx) {
         const int nb = ct_lines(c->nx, 3, sizeof(float2));
         RC(ct_dispatch(c, c->nx, CT_X_RHS_F, &a, dim3((a.nlines + nb - 1) / nb),
@@ -400,6 +404,10 @@ int launch_y_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *
     a.dxB = c->dxB32;
     a.dyB = c->dyB32;
     Prof pr(c, K_Y_RHS);
+    if (c->py) {
+        CK(pfa_launch_301(CT_Y_RHS_F, &a, c->nz, c->stream));
+        return HQT_OK;
+    }
     if (c->cy) {
         const int nb = ct_lines(c->ny, 3, sizeof(float2));
         RC(ct_dispatch(c, c->ny, CT_Y_RHS_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),
@@ -423,6 +431,10 @@ int launch_d1_32(hqt_ctx *c, bool along_x, const float *in, float *out) {
         a.in = FieldIn<float>{nullptr, in, nullptr};
         a.out = FieldOut<float>{nullptr, out, nullptr};
         Prof pr(c, K_X_D1);
+        if (c->px) {
+            CK(pfa_launch_301(CT_X_D1_F, &a, a.nlines, c->stream));
+            return HQT_OK;
+        }
         if (c->cx) {
             const int nb = ct_lines(c->nx, 2, sizeof(float2));
             RC(ct_dispatch(c, c->nx, CT_X_D1_F, &a, dim3((a.nlines + nb - 1) / nb),
@@ -443,6 +455,10 @@ int launch_d1_32(hqt_ctx *c, bool along_x, const float *in, float *out) {
     a.in = FieldIn<float>{nullptr, in, nullptr};
     a.out = FieldOut<float>{nullptr, out, nullptr};
     Prof pr(c, K_Y_D1);
+    if (c->py) {
+        CK(pfa_launch_301(CT_Y_D1_F, &a, c->nz, c->stream));
+        return HQT_OK;
+    }
     if (c->cy) {
         const int nb = ct_lines(c->ny, 2, sizeof(float2));
         RC(ct_dispatch(c, c->ny, CT_Y_D1_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),

@@ -41,6 +41,10 @@ cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const 
         std::vector<double> frag(PfaDims<HQT_PFA_P, HQT_PFA_Q>::NFRAG * 32);
         pfa_fragments<HQT_PFA_P, HQT_PFA_Q>(frag.data());
         e = cudaMemcpyToSymbol(g_pfa_frag, frag.data(), sizeof(double) * frag.size());
+        std::vector<float> frag32(PfaDims<HQT_PFA_P, HQT_PFA_Q>::NFRAG32 * 32);
+        pfa_fragments32<HQT_PFA_P, HQT_PFA_Q>(frag32.data());
+        if (e == cudaSuccess)
+            e = cudaMemcpyToSymbol(g_pfa_frag32, frag32.data(), sizeof(float) * frag32.size());
     }
 #endif
     opt((const void *)k_x_rhs_c<double, HQT_CN>);
@@ -107,22 +111,42 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
 cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t s) {
     constexpr int P = HQT_PFA_P, Q = HQT_PFA_Q;
     const int grid = (nlines + kPfaLines - 1) / kPfaLines;  // x passes
-    constexpr size_t smem = pfa_smem_bytes<P, Q>();
+    constexpr size_t smem = pfa_smem_bytes<double, P, Q>();
+    constexpr size_t smem32 = pfa_smem_bytes<float, P, Q>();
+    auto ygrid = [&](int nx, int nz_) {
+        return dim3((nx + kPfaLines - 1) / kPfaLines, nz_);
+    };
     switch (kind) {
         case CT_X_RHS:
-            k_x_rhs_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
+            k_x_rhs_pfa<double, P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
             break;
         case CT_Y_RHS: {
             const YRhsArgs<double> &a = *(const YRhsArgs<double> *)args;
-            k_y_rhs_pfa<P, Q><<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines), 32, smem, s>>>(a);
+            k_y_rhs_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
             break;
         }
         case CT_X_D1:
-            k_x_d1_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XD1Args<double> *)args);
+            k_x_d1_pfa<double, P, Q><<<grid, 32, smem, s>>>(*(const XD1Args<double> *)args);
             break;
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
-            k_y_d1_pfa<P, Q><<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines), 32, smem, s>>>(a);
+            k_y_d1_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
+            break;
+        }
+        case CT_X_RHS_F:
+            k_x_rhs_pfa<float, P, Q><<<grid, 32, smem32, s>>>(*(const XRhsArgs<float> *)args);
+            break;
+        case CT_Y_RHS_F: {
+            const YRhsArgs<float> &a = *(const YRhsArgs<float> *)args;
+            k_y_rhs_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
+            break;
+        }
+        case CT_X_D1_F:
+            k_x_d1_pfa<float, P, Q><<<grid, 32, smem32, s>>>(*(const XD1Args<float> *)args);
+            break;
+        case CT_Y_D1_F: {
+            const YD1Args<float> &a = *(const YD1Args<float> *)args;
+            k_y_d1_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
             break;
         }
         case CT_FX_FWD:

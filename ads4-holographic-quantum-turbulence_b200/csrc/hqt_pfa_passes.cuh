@@ -8,26 +8,31 @@
 
 namespace hqt {
 namespace {
-// per-lane fragment table of PfaWarp<P, Q> (pfa_fragments), uploaded by ct_init
+// per-lane fragment tables of PfaWarp<T, P, Q> (pfa_fragments,
+// pfa_fragments32), uploaded by ct_init
 __device__ double g_pfa_frag[PfaDims<HQT_PFA_P, HQT_PFA_Q>::NFRAG * 32];
+__device__ float g_pfa_frag32[PfaDims<HQT_PFA_P, HQT_PFA_Q>::NFRAG32 * 32];
 }  // namespace
+template <typename T> __device__ __forceinline__ const T *pfa_frag();
+template <> __device__ __forceinline__ const double *pfa_frag<double>() { return g_pfa_frag; }
+template <> __device__ __forceinline__ const float *pfa_frag<float>() { return g_pfa_frag32; }
 
-template <int P, int Q>
+template <typename T, int P, int Q>
 __host__ __device__ constexpr size_t pfa_smem_bytes() {
-    return sizeof(double) * 4 * kPfaLines * P * Q;  // two buffers, re/im planes
+    return sizeof(T) * 4 * kPfaLines * P * Q;  // two buffers, re/im planes
 }
 
-template <int P, int Q> struct PfaLines {
+template <typename T, int P, int Q> struct PfaLines {
     using D = PfaDims<P, Q>;
     static constexpr int N = D::N, LN = kPfaLines * N;
-    PfaBuf b0, b1;
+    PfaBuf<T> b0, b1;
     int valid;  // lines of this warp inside the grid
     int lane;
 
     __device__ __forceinline__ PfaLines(int valid_) : valid(valid_), lane(threadIdx.x & 31) {
-        double *sm = reinterpret_cast<double *>(g_smem);
-        b0 = PfaBuf{sm, sm + LN};
-        b1 = PfaBuf{sm + 2 * LN, sm + 3 * LN};
+        T *sm = reinterpret_cast<T *>(g_smem);
+        b0 = PfaBuf<T>{sm, sm + LN};
+        b1 = PfaBuf<T>{sm + 2 * LN, sm + 3 * LN};
     }
     // Position of element n of line ln in a buffer.  The input order of
     // stage A and the output order of the inverse stage A coincide: n with
@@ -44,23 +49,23 @@ template <int P, int Q> struct PfaLines {
             if (ln < valid) f(ln, n, pos(ln, n));
         }
     }
-    // cp.async of the doubles re(ln, n), im(ln, n) (pointers) into `dst`;
+    // cp.async of the values re(ln, n), im(ln, n) (pointers) into `dst`;
     // elements of lines outside the grid are zeroed.  The caller commits.
     template <typename Re, typename Im>
-    __device__ __forceinline__ void fetch(PfaBuf dst, Re re, Im im) const {
+    __device__ __forceinline__ void fetch(PfaBuf<T> dst, Re re, Im im) const {
         fetch(dst, re, im, [](int ln, int n) { return pos(ln, n); });
     }
     // ... at position at(ln, n) (spos for spectra in natural order)
     template <typename Re, typename Im, typename At>
-    __device__ __forceinline__ void fetch(PfaBuf dst, Re re, Im im, At at) const {
+    __device__ __forceinline__ void fetch(PfaBuf<T> dst, Re re, Im im, At at) const {
         for (int e = lane; e < LN; e += 32) {
             const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
             if (ln < valid) {
-                cp_async<8>(dst.re + i, re(ln, n));
-                cp_async<8>(dst.im + i, im(ln, n));
+                cp_async<sizeof(T)>(dst.re + i, re(ln, n));
+                cp_async<sizeof(T)>(dst.im + i, im(ln, n));
             } else {
-                dst.re[i] = 0.0;
-                dst.im[i] = 0.0;
+                dst.re[i] = T(0);
+                dst.im[i] = T(0);
             }
         }
     }
@@ -72,30 +77,30 @@ template <int P, int Q> struct PfaLines {
     // cp.async of a FieldIn (complex, or re with optional im) at element
     // index gi(ln, n) into `dst` at position at(ln, n)
     template <typename GI, typename At>
-    __device__ __forceinline__ void fetch_field(PfaBuf dst, const FieldIn<double> &f, GI gi,
+    __device__ __forceinline__ void fetch_field(PfaBuf<T> dst, const FieldIn<T> &f, GI gi,
                                                 At at) const {
         for (int e = lane; e < LN; e += 32) {
             const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
             if (ln < valid) {
                 const long long g = gi(ln, n);
                 if (f.c) {
-                    cp_async<8>(dst.re + i, &f.c[g].x);
-                    cp_async<8>(dst.im + i, &f.c[g].y);
+                    cp_async<sizeof(T)>(dst.re + i, &f.c[g].x);
+                    cp_async<sizeof(T)>(dst.im + i, &f.c[g].y);
                 } else {
-                    cp_async<8>(dst.re + i, f.re + g);
+                    cp_async<sizeof(T)>(dst.re + i, f.re + g);
                     if (f.im)
-                        cp_async<8>(dst.im + i, f.im + g);
+                        cp_async<sizeof(T)>(dst.im + i, f.im + g);
                     else
-                        dst.im[i] = 0.0;
+                        dst.im[i] = T(0);
                 }
             } else {
-                dst.re[i] = 0.0;
-                dst.im[i] = 0.0;
+                dst.re[i] = T(0);
+                dst.im[i] = T(0);
             }
         }
     }
-    static __device__ __forceinline__ auto in_place(PfaBuf b) {
-        return [b](int u, int k, double re, double im) {
+    static __device__ __forceinline__ auto in_place(PfaBuf<T> b) {
+        return [b](int u, int k, T re, T im) {
             b.re[u * Q + k] = re;
             b.im[u * Q + k] = im;
         };
@@ -103,22 +108,27 @@ template <int P, int Q> struct PfaLines {
 };
 
 // cos/sin(2 pi j/P), j = 0..P-1, for the CUDA-core stage B
-template <int P> __device__ __forceinline__ void pfa_twiddles(double (&cs)[2][P]) {
+template <typename T, int P> __device__ __forceinline__ void pfa_twiddles(T (&cs)[2][P]) {
 #pragma unroll
-    for (int j = 0; j < P; ++j) sincospi(2.0 * j / P, &cs[1][j], &cs[0][j]);
+    for (int j = 0; j < P; ++j) {
+        double sn, c;
+        sincospi(2.0 * j / P, &sn, &c);
+        cs[0][j] = (T)c;
+        cs[1][j] = (T)sn;
+    }
 }
 
 // x pass of one RK stage: d_x Psi, d_xx Psi, E = d_x(A_x + i A_y), d_xx A_y.
 // Per field: fetch (b0), stage A in place; per derivative: stage B with the
 // multiplier (b0 -> b1), inverse stage A in place, coalesced store.
-template <int P, int Q>
-__global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsArgs<double> a) {
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsArgs<T> a) {
     constexpr int N = P * Q;
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -144,7 +154,7 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
     __syncwarp();
     deriv(O1{});
     inverse();
-    L.each([&](int ln, int n, int i) { a.dxpsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    L.each([&](int ln, int n, int i) { a.dxpsi[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
     __syncwarp();
     deriv(O2{});
     // C = A_x + i A_y loads while the inverse runs
@@ -152,14 +162,14 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
             [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
     cp_commit();
     inverse();
-    L.each([&](int ln, int n, int i) { a.dxxpsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    L.each([&](int ln, int n, int i) { a.dxxpsi[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
     cp_wait<0>();
     __syncwarp();
     w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
     __syncwarp();
     deriv(O1{});
     inverse();
-    L.each([&](int ln, int n, int i) { a.E[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    L.each([&](int ln, int n, int i) { a.E[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
     __syncwarp();
     deriv(O2{});
     inverse();
@@ -175,20 +185,20 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
 // column pair and runs forward stage B, the combination and inverse stage
 // B in its registers.  Addends (d_xx Psi, d_x A_x, d_xx A_y) are fetched
 // into a freed buffer while an inverse stage runs.
-template <int P, int Q>
-__global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsArgs<double> a) {
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsArgs<T> a) {
     using D = PfaDims<P, Q>;
-    using L_t = PfaLines<P, Q>;
+    using L_t = PfaLines<T, P, Q>;
     constexpr int N = D::N, H = (P - 1) / 2;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const L_t L(min(kPfaLines, a.nx - x0));
     auto gi = [&](int ln, int n) { return zoff + (long long)n * a.nx + ln; };
-    auto inverse = [&](PfaBuf b) {
+    auto inverse = [&](PfaBuf<T> b) {
         w.template stage_a<+1>(b, L_t::in_place(b));
         __syncwarp();
     };
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, a.s2, cs);
     __syncwarp();
     inverse(L.b1);
-    L.each([&](int ln, int n, int i) { a.dypsi[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    L.each([&](int ln, int n, int i) { a.dypsi[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
     __syncwarp();
     w.template stage_b_deriv<2>(L.b0, L.b1, a.s1, a.s2, cs);
     __syncwarp();
@@ -214,7 +224,7 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     cp_wait<0>();
     __syncwarp();
     L.each([&](int ln, int n, int i) {
-        a.lap[gi(ln, n)] = make_double2(L.b0.re[i] + L.b1.re[i], L.b0.im[i] + L.b1.im[i]);
+        a.lap[gi(ln, n)] = mk2<T>(L.b0.re[i] + L.b1.re[i], L.b0.im[i] + L.b1.im[i]);
     });
     __syncwarp();
     // C and E after stage A, in place
@@ -235,41 +245,41 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         const int ln = task / NPAIR, k2a = task - ln * NPAIR;
         const int k2b = (Q - k2a) % Q;
         const int ncol = (k2b == k2a) ? 1 : 2;
-        double cr[2][P], ci[2][P], er[2][P], ei[2][P];
+        T cr[2][P], ci[2][P], er[2][P], ei[2][P];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const int k2 = c == 0 ? k2a : k2b;
-            double zr[P], zi[P];
+            T zr[P], zi[P];
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
                 zr[n1] = L.b0.re[e];
                 zi[n1] = L.b0.im[e];
             }
-            PfaWarp<P, Q>::template dft_real_pair<-1, H>(zr, zi, cr[c], ci[c], cs);
+            PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, cr[c], ci[c], cs);
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
                 zr[n1] = L.b1.re[e];
                 zi[n1] = L.b1.im[e];
             }
-            PfaWarp<P, Q>::template dft_real_pair<-1, H>(zr, zi, er[c], ei[c], cs);
+            PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, er[c], ei[c], cs);
         }
         // entry (0, k1) pairs with (1, P - k1): combine both from the four
         // spectra values and overwrite them in place (C <- the d_y A_y and
         // -d_y d_x A_x pair spectrum, E <- the d_y B spectrum).  Column k2 = 0
         // pairs with itself; both copies hold its spectra.
-        auto comb = [&](int k2, int k1, double c1x, double c1y, double c2x, double c2y,
-                        double e1x, double e1y, double e2x, double e2y, double &sr, double &si,
-                        double &tr, double &ti) {
-            const double kk = PfaWarp<P, Q>::wavenumber(k1, k2);
-            const double m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = 0.5;
-            const double axr = h * (c1x + c2x), axi = h * (c1y - c2y);
-            const double ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
-            const double exr = h * (e1x + e2x), exi = h * (e1y - e2y);
-            const double eyr = h * (e1y + e2y), eyi = -h * (e1x - e2x);
-            const double q1r = -m1 * ayi, q1i = m1 * ayr;  // d_y A_y
-            const double q2r = m1 * exi, q2i = -m1 * exr;  // -d_y d_x A_x
+        auto comb = [&](int k2, int k1, T c1x, T c1y, T c2x, T c2y,
+                        T e1x, T e1y, T e2x, T e2y, T &sr, T &si,
+                        T &tr, T &ti) {
+            const T kk = PfaWarp<T, P, Q>::wavenumber(k1, k2);
+            const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = T(0.5);
+            const T axr = h * (c1x + c2x), axi = h * (c1y - c2y);
+            const T ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
+            const T exr = h * (e1x + e2x), exi = h * (e1y - e2y);
+            const T eyr = h * (e1y + e2y), eyi = -h * (e1x - e2x);
+            const T q1r = -m1 * ayi, q1i = m1 * ayr;  // d_y A_y
+            const T q2r = m1 * exi, q2i = -m1 * exr;  // -d_y d_x A_x
             sr = q1r - q2i;
             si = q1i + q2r;
             tr = -m1 * eyi - m2 * axr;  // d_y B
@@ -278,8 +288,8 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
 #pragma unroll
         for (int k1 = 0; k1 < P; ++k1) {
             const int k1p = (P - k1) % P;
-            const double c0x = cr[0][k1], c0y = ci[0][k1], c1x = cr[1][k1p], c1y = ci[1][k1p];
-            const double e0x = er[0][k1], e0y = ei[0][k1], e1x = er[1][k1p], e1y = ei[1][k1p];
+            const T c0x = cr[0][k1], c0y = ci[0][k1], c1x = cr[1][k1p], c1y = ci[1][k1p];
+            const T e0x = er[0][k1], e0y = ei[0][k1], e1x = er[1][k1p], e1y = ei[1][k1p];
             comb(k2a, k1, c0x, c0y, c1x, c1y, e0x, e0y, e1x, e1y, cr[0][k1], ci[0][k1],
                  er[0][k1], ei[0][k1]);
             comb(k2b, k1p, c1x, c1y, c0x, c0y, e1x, e1y, e0x, e0y, cr[1][k1p], ci[1][k1p],
@@ -289,15 +299,15 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         for (int c = 0; c < 2; ++c) {
             if (c >= ncol) break;
             const int k2 = c == 0 ? k2a : k2b;
-            double zr[P], zi[P];
-            PfaWarp<P, Q>::template dft_real_pair<+1, H>(cr[c], ci[c], zr, zi, cs);
+            T zr[P], zi[P];
+            PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(cr[c], ci[c], zr, zi, cs);
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
                 L.b0.re[e] = zr[n1];
                 L.b0.im[e] = zi[n1];
             }
-            PfaWarp<P, Q>::template dft_real_pair<+1, H>(er[c], ei[c], zr, zi, cs);
+            PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(er[c], ei[c], zr, zi, cs);
 #pragma unroll
             for (int n1 = 0; n1 < P; ++n1) {
                 const int e = (ln * P + n1) * Q + k2;
@@ -323,10 +333,9 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
 }
 
 template <typename T>
-__device__ __forceinline__ void pfa_store_field(const FieldOut<T> &f, long long idx, double re,
-                                                double im) {
+__device__ __forceinline__ void pfa_store_field(const FieldOut<T> &f, long long idx, T re, T im) {
     if (f.c) {
-        f.c[idx] = make_double2(re, im);
+        f.c[idx] = mk2<T>(re, im);
         return;
     }
     if (f.re) f.re[idx] = re;
@@ -334,14 +343,14 @@ __device__ __forceinline__ void pfa_store_field(const FieldOut<T> &f, long long 
 }
 
 // First x derivative of a field (x_d1 of hqt_cpasses.cuh).
-template <int P, int Q>
-__global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args<double> a) {
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args<T> a) {
     constexpr int N = P * Q;
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args
     __syncwarp();
     w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
     __syncwarp();
-    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, 0.0, cs);
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, T(0), cs);
     __syncwarp();
     w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
     __syncwarp();
@@ -360,13 +369,13 @@ __global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args
 }
 
 // First y derivative of a field, optionally plus a real addend (y_d1).
-template <int P, int Q>
-__global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args<double> a) {
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args<T> a) {
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const L_t L(min(kPfaLines, a.nx - x0));
@@ -377,13 +386,13 @@ __global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args
     __syncwarp();
     w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
     __syncwarp();
-    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, 0.0, cs);
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, T(0), cs);
     __syncwarp();
     w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
     __syncwarp();
     L.each([&](int ln, int n, int i) {
         const long long g = gi(ln, n);
-        const double re = L.b1.re[i] + (a.add_re ? a.add_re[g] : 0.0);
+        const T re = L.b1.re[i] + (a.add_re ? a.add_re[g] : T(0));
         pfa_store_field(a.out, g, re, L.b1.im[i]);
     });
 }
@@ -392,12 +401,13 @@ __global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args
 // phase exp(-2 pi i y w / ny) when a status is given), natural order k.
 template <int P, int Q>
 __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ XFiltFwdArgs<double> a) {
+    using T = double;
     constexpr int N = P * Q;
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -431,7 +441,7 @@ __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ X
             const int ln = e % kPfaLines, k = e / kPfaLines;
             if (ln < L.valid) {
                 const int i = L_t::spos(ln, k);
-                spec[gi(ln, k)] = make_double2(L.b1.re[i], L.b1.im[i]);
+                spec[gi(ln, k)] = mk2<T>(L.b1.re[i], L.b1.im[i]);
             }
         }
         __syncwarp();
@@ -443,12 +453,13 @@ __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ X
 // blockIdx.y = z slice, blockIdx.z = field.
 template <int P, int Q>
 __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFiltArgs<double> a) {
+    using T = double;
     constexpr int N = P * Q;
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const L_t L(min(kPfaLines, a.nx - x0));
@@ -465,7 +476,7 @@ __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFilt
                                    [&](int ln, int k1, int k2, double &re, double &im) {
         const int kx = x0 + min(ln, L.valid - 1);
         const int kxm = (a.nx - kx) % a.nx;
-        const int ky = PfaWarp<P, Q>::crt(k1, k2), kym = (N - ky) % N;
+        const int ky = PfaWarp<T, P, Q>::crt(k1, k2), kym = (N - ky) % N;
         const double wgt = 0.5 * (a.mx[kx] * a.my[ky] + a.mx[kxm] * a.my[kym]) * a.scale;
         re *= wgt;
         im *= wgt;
@@ -473,19 +484,20 @@ __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFilt
     __syncwarp();
     w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
     __syncwarp();
-    L.each([&](int ln, int n, int i) { spec[gi(ln, n)] = make_double2(L.b1.re[i], L.b1.im[i]); });
+    L.each([&](int ln, int n, int i) { spec[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
 }
 
 // Filter, x inverse: inverse transforms along x of nf spectra into the
 // fields; a non-finite value sets the status' first bad step.
 template <int P, int Q>
 __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ XFiltInvArgs<double> a) {
+    using T = double;
     constexpr int N = P * Q;
-    using L_t = PfaLines<P, Q>;
-    PfaWarp<P, Q> w;
-    w.init(g_pfa_frag);
-    double cs[2][P];
-    pfa_twiddles<P>(cs);
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
