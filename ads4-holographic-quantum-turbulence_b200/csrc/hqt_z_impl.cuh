@@ -50,8 +50,9 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     return e;
 }
 
-// One fused launch per stage (hqt_zfused.cuh): persistent one-warp blocks,
-// as many as fit on the device at once, each looping over column tiles.
+// One fused launch per stage (hqt_zfused.cuh): persistent blocks of kZWarps
+// warps, as many as fit on the device at once, each looping over tiles of
+// kZTile columns.
 template <typename TD, int M> static int z_stage_grid(long long plane) {
     static int per_sm = 0, nsm = 0;
     if (per_sm == 0) {
@@ -59,11 +60,11 @@ template <typename TD, int M> static int z_stage_grid(long long plane) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_zstage<double, double, TD, HQT_ZN, M>, 32,
+            &per_sm, k_zstage<double, double, TD, HQT_ZN, M>, kZThreads,
             zf_smem_bytes<double, double, TD, HQT_ZN>());
         if (per_sm < 1) per_sm = 1;
     }
-    const long long tiles = (plane + kZCols - 1) / kZCols;
+    const long long tiles = (plane + kZTile - 1) / kZTile;
     const long long full = (long long)per_sm * (nsm > 0 ? nsm : 1);
     return (int)(tiles < full ? tiles : full);
 }
@@ -77,7 +78,7 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
 #define HQT_ZS(M)                                                                            \
     case M:                                                                                  \
         k_zstage<double, double, TD, HQT_ZN, M>                                              \
-            <<<z_stage_grid<TD, M>(a.plane), 32, smem, s>>>(a, op);                          \
+            <<<z_stage_grid<TD, M>(a.plane), kZThreads, smem, s>>>(a, op);                          \
         break;
         HQT_ZS(1)
         HQT_ZS(2)
@@ -87,7 +88,7 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
         case 0:
             if constexpr (std::is_same<TD, double>::value) {
                 k_zstage<double, double, double, HQT_ZN, 0>
-                    <<<z_stage_grid<double, 0>(a.plane), 32, smem, s>>>(a, op);
+                    <<<z_stage_grid<double, 0>(a.plane), kZThreads, smem, s>>>(a, op);
                 break;
             }
             return cudaErrorInvalidValue;

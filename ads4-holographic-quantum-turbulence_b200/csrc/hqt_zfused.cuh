@@ -46,7 +46,9 @@
 
 namespace hqt {
 
-constexpr int kZCols = 4;  // columns per warp tile (x 2 parts = the mma's n extent)
+constexpr int kZCols = 4;   // columns per warp (x 2 parts = the mma's n extent)
+constexpr int kZWarps = 4;  // warps per block; a block stages kZTile columns
+constexpr int kZTile = kZCols * kZWarps;
 
 // d += a * b on one 8x8x4 FP64 tensor-core tile
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
@@ -62,14 +64,16 @@ template <int NZP> struct ZmDims {
     static constexpr int LV = MP > KP ? MP : KP;  // levels stored per tile field
 };
 
-// Field of a tile in shared memory: element (level l, column c) at l*4 + c.
+// Field of a tile in shared memory: element (level l, column c) at
+// l*kZTile + c.  A warp's view starts at its first column.
 template <typename V> struct ZTileF {
     V *p;
-    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZCols + c]; }
+    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZTile + c]; }
+    __device__ __forceinline__ ZTileF<V> cols(int c0) const { return ZTileF<V>{p + c0}; }
 };
 
 template <typename TD, int NZP> struct ZfLayout {
-    static constexpr int L = ZmDims<NZP>::LV * kZCols;
+    static constexpr int L = ZmDims<NZP>::LV * kZTile;
     static constexpr int c = L * 16, r = L * 8;  // complex / pair, real (double)
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
     static constexpr int mx(int a, int b) { return a > b ? a : b; }
@@ -94,25 +98,27 @@ __host__ __device__ constexpr int zf_smem_bytes() {
 }
 
 // ---- staging of levels 0..nz-1 of the tile starting at site0 --------------
-// A compile-time trip count (NZP levels) with predicated copies: every lane
-// runs the same instructions, so the loops do not diverge.
+// All threads of the block share the copies (tid = threadIdx.x); a
+// compile-time trip count with predicated copies, so the loops do not
+// diverge.  A level row of a tile is kZTile consecutive sites.
+constexpr int kZThreads = 32 * kZWarps;
 template <int NZP, typename V>
 __device__ __forceinline__ void zf_real(ZTileF<V> dst, const V *src, int nz, long long P,
-                                        long long site0, int lane) {
+                                        long long site0, int tid) {
     if (!src) return;
 #pragma unroll
-    for (int it = 0; it < (NZP * kZCols + 31) / 32; ++it) {
-        const int e = lane + 32 * it, l = e >> 2, c = e & 3;
+    for (int it = 0; it < (NZP * kZTile + kZThreads - 1) / kZThreads; ++it) {
+        const int e = tid + kZThreads * it, l = e / kZTile, c = e % kZTile;
         if (l < nz && site0 + c < P) cp_async<sizeof(V)>(&dst(l, c), src + l * P + site0 + c);
     }
 }
 template <int NZP, typename V>
 __device__ __forceinline__ void zf_pair(ZTileF<C2<V>> dst, const V *sx, const V *sy, int nz,
-                                        long long P, long long site0, int lane) {
+                                        long long P, long long site0, int tid) {
     if (!sx || !sy) return;
 #pragma unroll
-    for (int it = 0; it < (NZP * kZCols + 31) / 32; ++it) {
-        const int e = lane + 32 * it, l = e >> 2, c = e & 3;
+    for (int it = 0; it < (NZP * kZTile + kZThreads - 1) / kZThreads; ++it) {
+        const int e = tid + kZThreads * it, l = e / kZTile, c = e % kZTile;
         if (l < nz && site0 + c < P) {
             const long long gi = l * P + site0 + c;
             cp_async<sizeof(V)>(&dst(l, c).x, sx + gi);
@@ -141,7 +147,7 @@ __device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double
     for (int m = 0; m < MT; ++m) C[m][0] = C[m][1] = 0.0;
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
-        const double b = v[(4 * s + q) * 8 + g];
+        const double b = v[(4 * s + q) * 2 * kZTile + g];
 #pragma unroll
         for (int m = 0; m < MT; ++m) dmma(C[m][0], C[m][1], A[m][s], b);
     }
@@ -150,7 +156,7 @@ __device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double
 // T = TS = double (state and arithmetic); TD = double or float (derivative
 // fields of the line passes).
 template <typename T, typename TS, typename TD, int NZP, int MODE>
-__global__ void __launch_bounds__(32, 12)
+__global__ void __launch_bounds__(kZThreads, 3)
     k_zstage(const __grid_constant__ ZStageArgs<T, TS, TD> a,
              const __grid_constant__ ZOps<T, NZP> op) {
     static_assert(std::is_same<T, double>::value && std::is_same<TS, double>::value,
@@ -158,12 +164,13 @@ __global__ void __launch_bounds__(32, 12)
     using Lay = ZfLayout<TD, NZP>;
     using D = ZmDims<NZP>;
     constexpr int MT = D::MT, KS = D::KS;
-    const int lane = threadIdx.x, g = lane >> 2, q = lane & 3;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+    const int cw = kZCols * warp;  // this warp's first column in the tile
     const int nz = a.nz;
     const long long P = a.plane;
     unsigned char *sm = g_smem;
     // zero the tile once: padded levels must read as 0 in every product
-    for (int i = lane; i < Lay::bytes / 16; i += 32)
+    for (int i = tid; i < Lay::bytes / 16; i += kZThreads)
         reinterpret_cast<double2 *>(sm)[i] = make_double2(0.0, 0.0);
     // operator fragments (padded rows and columns of op are zero)
     double ALz[MT][KS], ALz1[MT][KS];
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(32, 12)
         fzr[m] = i < NZP ? op.fz[i < NZP ? i : 0] : 0.0;
         lzr[m] = i < NZP ? op.lzb[i < NZP ? i : 0] : 0.0;
     }
-    __syncwarp();
+    __syncthreads();
 
     const ZTileF<double2> PS{reinterpret_cast<double2 *>(sm + Lay::oPS)};
     const ZTileF<double2> AXY{reinterpret_cast<double2 *>(sm + Lay::oAXY)};
@@ -209,34 +216,38 @@ __global__ void __launch_bounds__(32, 12)
     constexpr bool kReadK = (MODE >= 2);
 
     auto stage_main = [&](long long site0) {
-        zf_real<NZP, double2>(PS, a.ypsi, nz, P, site0, lane);
-        zf_pair<NZP, double>(AXY, a.yax, a.yay, nz, P, site0, lane);
-        zf_real<NZP, C2<TD>>(DXP, a.dxpsi, nz, P, site0, lane);
-        zf_real<NZP, C2<TD>>(DYP, a.dypsi, nz, P, site0, lane);
+        zf_real<NZP, double2>(PS, a.ypsi, nz, P, site0, tid);
+        zf_pair<NZP, double>(AXY, a.yax, a.yay, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(DXP, a.dxpsi, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(DYP, a.dypsi, nz, P, site0, tid);
     };
     auto stage_gauge = [&](long long site0) {
-        zf_pair<NZP, TD>(DT, a.dxat, a.dyat, nz, P, site0, lane);
+        zf_pair<NZP, TD>(DT, a.dxat, a.dyat, nz, P, site0, tid);
         // F3 takes -d_y B, F4 takes +d_x B: stored as (d_y B, d_x B)
-        zf_pair<NZP, TD>(BF, a.dyB, a.dxB, nz, P, site0, lane);
+        zf_pair<NZP, TD>(BF, a.dyB, a.dxB, nz, P, site0, tid);
         if (MODE >= 1) {
-            zf_pair<NZP, double>(ZA, a.zax, a.zay, nz, P, site0, lane);
-            if (kReadK) zf_pair<NZP, double>(KA, a.kax, a.kay, nz, P, site0, lane);
+            zf_pair<NZP, double>(ZA, a.zax, a.zay, nz, P, site0, tid);
+            if (kReadK) zf_pair<NZP, double>(KA, a.kax, a.kay, nz, P, site0, tid);
         }
     };
 
-    const long long ntiles = (P + kZCols - 1) / kZCols;
+    // this warp's columns of every tile field
+    const auto PSw = PS.cols(cw), AXYw = AXY.cols(cw), VCw = VC.cols(cw), VGw = VG.cols(cw),
+               VSw = VS.cols(cw);
+    const long long ntiles = (P + kZTile - 1) / kZTile;
     if ((long long)blockIdx.x < ntiles) {
-        stage_main((long long)blockIdx.x * kZCols);
-        stage_gauge((long long)blockIdx.x * kZCols);
+        stage_main((long long)blockIdx.x * kZTile);
+        stage_gauge((long long)blockIdx.x * kZTile);
     }
     cp_commit();
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long site0 = tile * kZCols;
+        const long long site0 = tile * kZTile;
         const long long next = tile + gridDim.x;
-        const long long site = site0 + q;  // this lane's column in C layout
+        const long long sw0 = site0 + cw;   // this warp's first column
+        const long long site = sw0 + q;     // this lane's column in C layout
         cp_wait<0>();
-        __syncwarp();
+        __syncthreads();  // every thread's copies are in
 
         // ---- F3, F4: both gauge components at once -------------------------
         if (a.f2x) {
@@ -244,7 +255,7 @@ __global__ void __launch_bounds__(32, 12)
             double bx = 0.0, by = 0.0;
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
-                const double2 v = AXY(8 * m + g, q);
+                const double2 v = AXY(8 * m + g, cw + q);
                 bx = fma(lzr[m], v.x, bx);
                 by = fma(lzr[m], v.y, by);
             }
@@ -257,38 +268,38 @@ __global__ void __launch_bounds__(32, 12)
         }
         {  // g = d A_t + f Lz A
             double c[MT][2];
-            zm_pair<MT, KS>(ALz, AXY, c, lane);
+            zm_pair<MT, KS>(ALz, AXYw, c, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g, ic = i < nz ? i : nz - 1;
-                const C2<TD> dt = DT(ic, q);
+                const C2<TD> dt = DT(ic, cw + q);
                 const bool in = i < nz;
-                VG(i, q) = make_double2(in ? T(dt.x) + fzr[m] * c[m][0] : 0.0,
+                VG(i, cw + q) = make_double2(in ? T(dt.x) + fzr[m] * c[m][0] : 0.0,
                                         in ? T(dt.y) + fzr[m] * c[m][1] : 0.0);
             }
         }
         __syncwarp();
         {  // S = 1/2 Lz g -+ 1/2 d B + Im(conj(Psi) d Psi) - A |Psi|^2
             double d[MT][2];
-            zm_pair<MT, KS>(ALz, VG, d, lane);
+            zm_pair<MT, KS>(ALz, VGw, d, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g, ic = i < nz ? i : nz - 1;
-                const double2 ps = PS(ic, q), av = AXY(ic, q);
-                const C2<TD> dx = DXP(ic, q), dy = DYP(ic, q), bf = BF(ic, q);
+                const double2 ps = PS(ic, cw + q), av = AXY(ic, cw + q);
+                const C2<TD> dx = DXP(ic, cw + q), dy = DYP(ic, cw + q), bf = BF(ic, cw + q);
                 const double p2 = ps.x * ps.x + ps.y * ps.y;
                 const double vx = T(0.5) * d[m][0] + T(0.5) * -T(bf.x) +
                                   (ps.x * T(dx.y) - ps.y * T(dx.x)) - av.x * p2;
                 const double vy = T(0.5) * d[m][1] + T(0.5) * T(bf.y) +
                                   (ps.x * T(dy.y) - ps.y * T(dy.x)) - av.y * p2;
                 const bool in = i < nz;
-                VS(i, q) = make_double2(in ? vx : 0.0, in ? vy : 0.0);
+                VS(i, cw + q) = make_double2(in ? vx : 0.0, in ? vy : 0.0);
             }
         }
         __syncwarp();
         {  // F = Lzr(S) (rows < nz-1 of Lz1, zero on the boundary row), update
             double f[MT][2];
-            zm_pair<MT, KS>(ALz1, VS, f, lane);
+            zm_pair<MT, KS>(ALz1, VSw, f, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
@@ -300,9 +311,9 @@ __global__ void __launch_bounds__(32, 12)
                     continue;
                 }
                 const TS kx = a.h * TS(f[m][0]), ky = a.h * TS(f[m][1]);
-                const double2 z = ZA(i, q);
+                const double2 z = ZA(i, cw + q);
                 if (MODE == 4) {
-                    const double2 K = KA(i, q);
+                    const double2 K = KA(i, cw + q);
                     a.wax[gi] = z.x + (TS(1) / TS(6)) * (K.x + kx);
                     a.way[gi] = z.y + (TS(1) / TS(6)) * (K.y + ky);
                     continue;
@@ -311,7 +322,7 @@ __global__ void __launch_bounds__(32, 12)
                     a.kax[gi] = kx;
                     a.kay[gi] = ky;
                 } else {
-                    const double2 K = KA(i, q);
+                    const double2 K = KA(i, cw + q);
                     a.kax[gi] = K.x + 2 * kx;
                     a.kay[gi] = K.y + 2 * ky;
                 }
@@ -327,46 +338,46 @@ __global__ void __launch_bounds__(32, 12)
                 }
             }
         }
-        __syncwarp();  // G and V are free
+        __syncthreads();  // every warp is done with G: the Psi inputs refill it
 
         // ---- Psi ---------------------------------------------------------------
-        zf_real<NZP, T>(AT, a.at, nz, P, site0, lane);
-        zf_real<NZP, T>(DAT, a.dat, nz, P, site0, lane);
-        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, lane);
-        zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, lane);
+        zf_real<NZP, T>(AT, a.at, nz, P, site0, tid);
+        zf_real<NZP, T>(DAT, a.dat, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, tid);
+        zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, tid);
         if (MODE >= 1) {
-            zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, lane);
-            if (kReadK) zf_real<NZP, double2>(KP, a.kpsi, nz, P, site0, lane);
+            zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, tid);
+            if (kReadK) zf_real<NZP, double2>(KP, a.kpsi, nz, P, site0, tid);
         }
         cp_commit();
         {  // dp = Lz Psi
             double c[MT][2];
-            zm_pair<MT, KS>(ALz, PS, c, lane);
+            zm_pair<MT, KS>(ALz, PSw, c, lane);
 #pragma unroll
-            for (int m = 0; m < MT; ++m) VC(8 * m + g, q) = make_double2(c[m][0], c[m][1]);
+            for (int m = 0; m < MT; ++m) VC(8 * m + g, cw + q) = make_double2(c[m][0], c[m][1]);
         }
         cp_wait<0>();
-        __syncwarp();
+        __syncthreads();  // every thread's copies are in
         // boundary row of F2: kb = Lz(nz,:) div A of column q, in every lane
         T kb = T(0);
 #pragma unroll
         for (int m = 0; m < MT; ++m) {
             const int i = 8 * m + g;
-            kb = fma(lzr[m], (i < nz) ? T(DIV(i < nz ? i : 0, q)) : T(0), kb);
+            kb = fma(lzr[m], (i < nz) ? T(DIV(i < nz ? i : 0, cw + q)) : T(0), kb);
         }
         kb = zf_colsum(kb);
         double s1[MT][2];
         {  // d2 = Lz dp and S1
             double d2[MT][2];
-            zm_pair<MT, KS>(ALz, VC, d2, lane);
+            zm_pair<MT, KS>(ALz, VCw, d2, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
                 const int ic = i < nz - 1 ? i : 0;
-                const double2 ps = PS(ic, q), av = AXY(ic, q), d1 = VC(ic, q);
-                const T at = AT(ic, q), dat = DAT(ic, q);
-                const C2<TD> lp = LAP(ic, q), dx = DXP(ic, q), dy = DYP(ic, q);
-                const T dv = T(DIV(ic, q));
+                const double2 ps = PS(ic, cw + q), av = AXY(ic, cw + q), d1 = VC(ic, cw + q);
+                const T at = AT(ic, cw + q), dat = DAT(ic, cw + q);
+                const C2<TD> lp = LAP(ic, cw + q), dx = DXP(ic, cw + q), dy = DYP(ic, cw + q);
+                const T dv = T(DIV(ic, cw + q));
                 const T z = zr[m], f = fzr[m], hh = T(0.5);
                 const T a2 = av.x * av.x + av.y * av.y;
                 const T u = av.x * T(dx.x) + av.y * T(dy.x);
@@ -382,15 +393,15 @@ __global__ void __launch_bounds__(32, 12)
                 s1[m][1] = in ? r1 : 0.0;
             }
         }
-        __syncwarp();  // every read of dp and of R is done
+        __syncthreads();  // every warp is done with R: the next tile refills it
 #pragma unroll
-        for (int m = 0; m < MT; ++m) VC(8 * m + g, q) = make_double2(s1[m][0], s1[m][1]);
-        if (next < ntiles) stage_main(next * kZCols);  // the next tile's R loads now
+        for (int m = 0; m < MT; ++m) VC(8 * m + g, cw + q) = make_double2(s1[m][0], s1[m][1]);
+        if (next < ntiles) stage_main(next * kZTile);  // the next tile's R loads now
         cp_commit();
         __syncwarp();
         {  // F1 = Lzr(S1) and the RK update of Psi
             double f[MT][2];
-            zm_pair<MT, KS>(ALz1, VC, f, lane);
+            zm_pair<MT, KS>(ALz1, VCw, f, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
@@ -401,9 +412,9 @@ __global__ void __launch_bounds__(32, 12)
                     continue;
                 }
                 const double2 k = make_double2(a.h * f[m][0], a.h * f[m][1]);
-                const double2 z = ZP(i, q);
+                const double2 z = ZP(i, cw + q);
                 if (MODE == 4) {
-                    const double2 K = KP(i, q);
+                    const double2 K = KP(i, cw + q);
                     const TS s = TS(1) / TS(6);
                     a.wpsi[gi] = make_double2(z.x + s * (K.x + k.x), z.y + s * (K.y + k.y));
                     continue;
@@ -411,7 +422,7 @@ __global__ void __launch_bounds__(32, 12)
                 if (MODE == 1) {
                     a.kpsi[gi] = k;
                 } else {
-                    const double2 K = KP(i, q);
+                    const double2 K = KP(i, cw + q);
                     a.kpsi[gi] = make_double2(K.x + 2 * k.x, K.y + 2 * k.y);
                 }
                 const double2 nv = (MODE == 3) ? make_double2(z.x + k.x, z.y + k.y)
@@ -438,8 +449,8 @@ __global__ void __launch_bounds__(32, 12)
                     a.wrho[sl] = a.zrho[sl] - (TS(1) / TS(6)) * (a.krho[sl] + k);
             }
         }
-        __syncwarp();  // G and V are free for the next tile
-        if (next < ntiles) stage_gauge(next * kZCols);
+        __syncthreads();  // every warp is done with G: the next tile refills it
+        if (next < ntiles) stage_gauge(next * kZTile);
         cp_commit();
     }
     cp_wait<0>();
