@@ -177,19 +177,15 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
 }
 
 // y pass of one RK stage (lines along y: kPfaLines adjacent x columns of one
-// z slice): d_y Psi, lap Psi = d_xx Psi + d_yy Psi, and from the spectra of
-// C = A_x + i A_y and E = d_x C the fields div A = d_x A_x + d_y A_y,
-// d_x B and d_y B (B = d_x A_y - d_y A_x).  The real fields are separated
-// from the pair spectra with the k <-> -k symmetry: in the prime-factor
-// order the partner of column k2 is column Q - k2, so one lane takes each
-// column pair and runs forward stage B, the combination and inverse stage
-// B in its registers.  Addends (d_xx Psi, d_x A_x, d_xx A_y) are fetched
-// into a freed buffer while an inverse stage runs.
+// z slice): d_y Psi, lap Psi = d_xx Psi + d_yy Psi, and from A_x, A_y and
+// E = d_x(A_x + i A_y) the fields div A = d_x A_x + d_y A_y, d_x B and d_y B
+// (B = d_x A_y - d_y A_x).  Addends (d_xx Psi, d_x A_x, d_xx A_y) are
+// fetched into a freed buffer while an inverse stage runs.
 template <typename T, int P, int Q>
 __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsArgs<T> a) {
     using D = PfaDims<P, Q>;
     using L_t = PfaLines<T, P, Q>;
-    constexpr int N = D::N, H = (P - 1) / 2;
+    constexpr int H = (P - 1) / 2;
     PfaWarp<T, P, Q> w;
     w.init(pfa_frag<T>());
     T cs[2][P];
@@ -227,109 +223,152 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         a.lap[gi(ln, n)] = mk2<T>(L.b0.re[i] + L.b1.re[i], L.b0.im[i] + L.b1.im[i]);
     });
     __syncwarp();
-    // C and E after stage A, in place
-    L.fetch(L.b0, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
-            [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
-    L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
-            [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
-    cp_commit();
-    cp_wait<0>();
-    __syncwarp();
-    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
-    w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
-    __syncwarp();
-    // column pairs (k2, Q - k2) of each line: spectra, combination, inverse
-    constexpr int NPAIR = (Q + 1) / 2;
-#pragma unroll 1
-    for (int task = w.lane; task < kPfaLines * NPAIR; task += 32) {
-        const int ln = task / NPAIR, k2a = task - ln * NPAIR;
-        const int k2b = (Q - k2a) % Q;
-        const int ncol = (k2b == k2a) ? 1 : 2;
-        T cr[2][P], ci[2][P], er[2][P], ei[2][P];
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int k2 = c == 0 ? k2a : k2b;
-            T zr[P], zi[P];
-#pragma unroll
-            for (int n1 = 0; n1 < P; ++n1) {
-                const int e = (ln * P + n1) * Q + k2;
-                zr[n1] = L.b0.re[e];
-                zi[n1] = L.b0.im[e];
+    if constexpr (std::is_same<T, double>::value) {
+        // FP64: C = A_x + i A_y and E = d_x C after stage A, and the real
+        // fields separated from their pair spectra (measured faster in FP64
+        // than the two-field form below, which keeps fewer registers but
+        // loads the shared-memory pipe more)
+        L.fetch(L.b0, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
+                [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+        L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+                [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+        w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+        w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
+        __syncwarp();
+        // column pairs (k2, Q - k2) of each line: spectra, combination, inverse
+        constexpr int NPAIR = (Q + 1) / 2;
+    #pragma unroll 1
+        for (int task = w.lane; task < kPfaLines * NPAIR; task += 32) {
+            const int ln = task / NPAIR, k2a = task - ln * NPAIR;
+            const int k2b = (Q - k2a) % Q;
+            const int ncol = (k2b == k2a) ? 1 : 2;
+            T cr[2][P], ci[2][P], er[2][P], ei[2][P];
+    #pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int k2 = c == 0 ? k2a : k2b;
+                T zr[P], zi[P];
+    #pragma unroll
+                for (int n1 = 0; n1 < P; ++n1) {
+                    const int e = (ln * P + n1) * Q + k2;
+                    zr[n1] = L.b0.re[e];
+                    zi[n1] = L.b0.im[e];
+                }
+                PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, cr[c], ci[c], cs);
+    #pragma unroll
+                for (int n1 = 0; n1 < P; ++n1) {
+                    const int e = (ln * P + n1) * Q + k2;
+                    zr[n1] = L.b1.re[e];
+                    zi[n1] = L.b1.im[e];
+                }
+                PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, er[c], ei[c], cs);
             }
-            PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, cr[c], ci[c], cs);
-#pragma unroll
-            for (int n1 = 0; n1 < P; ++n1) {
-                const int e = (ln * P + n1) * Q + k2;
-                zr[n1] = L.b1.re[e];
-                zi[n1] = L.b1.im[e];
+            // entry (0, k1) pairs with (1, P - k1): combine both from the four
+            // spectra values and overwrite them in place (C <- the d_y A_y and
+            // -d_y d_x A_x pair spectrum, E <- the d_y B spectrum).  Column k2 = 0
+            // pairs with itself; both copies hold its spectra.
+            auto comb = [&](int k2, int k1, T c1x, T c1y, T c2x, T c2y,
+                            T e1x, T e1y, T e2x, T e2y, T &sr, T &si,
+                            T &tr, T &ti) {
+                const T kk = PfaWarp<T, P, Q>::wavenumber(k1, k2);
+                const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = T(0.5);
+                const T axr = h * (c1x + c2x), axi = h * (c1y - c2y);
+                const T ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
+                const T exr = h * (e1x + e2x), exi = h * (e1y - e2y);
+                const T eyr = h * (e1y + e2y), eyi = -h * (e1x - e2x);
+                const T q1r = -m1 * ayi, q1i = m1 * ayr;  // d_y A_y
+                const T q2r = m1 * exi, q2i = -m1 * exr;  // -d_y d_x A_x
+                sr = q1r - q2i;
+                si = q1i + q2r;
+                tr = -m1 * eyi - m2 * axr;  // d_y B
+                ti = m1 * eyr - m2 * axi;
+            };
+    #pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) {
+                const int k1p = (P - k1) % P;
+                const T c0x = cr[0][k1], c0y = ci[0][k1], c1x = cr[1][k1p], c1y = ci[1][k1p];
+                const T e0x = er[0][k1], e0y = ei[0][k1], e1x = er[1][k1p], e1y = ei[1][k1p];
+                comb(k2a, k1, c0x, c0y, c1x, c1y, e0x, e0y, e1x, e1y, cr[0][k1], ci[0][k1],
+                     er[0][k1], ei[0][k1]);
+                comb(k2b, k1p, c1x, c1y, c0x, c0y, e1x, e1y, e0x, e0y, cr[1][k1p], ci[1][k1p],
+                     er[1][k1p], ei[1][k1p]);
             }
-            PfaWarp<T, P, Q>::template dft_real_pair<-1, H>(zr, zi, er[c], ei[c], cs);
+    #pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (c >= ncol) break;
+                const int k2 = c == 0 ? k2a : k2b;
+                T zr[P], zi[P];
+                PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(cr[c], ci[c], zr, zi, cs);
+    #pragma unroll
+                for (int n1 = 0; n1 < P; ++n1) {
+                    const int e = (ln * P + n1) * Q + k2;
+                    L.b0.re[e] = zr[n1];
+                    L.b0.im[e] = zi[n1];
+                }
+                PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(er[c], ei[c], zr, zi, cs);
+    #pragma unroll
+                for (int n1 = 0; n1 < P; ++n1) {
+                    const int e = (ln * P + n1) * Q + k2;
+                    L.b1.re[e] = zr[n1];
+                    L.b1.im[e] = zi[n1];
+                }
+            }
         }
-        // entry (0, k1) pairs with (1, P - k1): combine both from the four
-        // spectra values and overwrite them in place (C <- the d_y A_y and
-        // -d_y d_x A_x pair spectrum, E <- the d_y B spectrum).  Column k2 = 0
-        // pairs with itself; both copies hold its spectra.
-        auto comb = [&](int k2, int k1, T c1x, T c1y, T c2x, T c2y,
-                        T e1x, T e1y, T e2x, T e2y, T &sr, T &si,
-                        T &tr, T &ti) {
+        __syncwarp();
+        inverse(L.b1);
+        L.each([&](int ln, int n, int i) { a.dyB[gi(ln, n)] = L.b1.re[i]; });
+        __syncwarp();
+        L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+                [&](int ln, int n) { return &a.dxxay[gi(ln, n)]; });
+        cp_commit();
+        inverse(L.b0);
+        cp_wait<0>();
+        __syncwarp();
+        L.each([&](int ln, int n, int i) {
+            a.divA[gi(ln, n)] = L.b1.re[i] + L.b0.re[i];
+            a.dxB[gi(ln, n)] = L.b1.im[i] + L.b0.im[i];
+        });
+    } else {
+        // The gauge fields as two complex lines whose y derivatives give the
+        // outputs directly (no k <-> -k split of pair spectra):
+        //   W1 = E_x + i A_y:  d_y W1 = d_y E_x + i d_y A_y, so
+        //     div A = E_x + Im(d_y W1),  d_x B = d_xx A_y - Re(d_y W1);
+        //   W2 = A_x + i E_y:  d_y B = d_y E_y - d_yy A_x = Im(d_y W2) - Re(d_yy W2)
+        //     = Re(IFFT((s1 k - s2 k^2) W2^)) (Im(z) = Re(-i z)), one real multiplier.
+        L.fetch(L.b0, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+                [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+        L.fetch(L.b1, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
+                [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+        w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+        w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
+        __syncwarp();
+        w.template stage_b_deriv<1>(L.b0, L.b0, a.s1, a.s2, cs);
+        w.template stage_b<true, true>(L.b1, L.b1, cs, [&](int, int k1, int k2, T &re, T &im) {
             const T kk = PfaWarp<T, P, Q>::wavenumber(k1, k2);
-            const T m1 = a.s1 * kk, m2 = a.s2 * kk * kk, h = T(0.5);
-            const T axr = h * (c1x + c2x), axi = h * (c1y - c2y);
-            const T ayr = h * (c1y + c2y), ayi = -h * (c1x - c2x);
-            const T exr = h * (e1x + e2x), exi = h * (e1y - e2y);
-            const T eyr = h * (e1y + e2y), eyi = -h * (e1x - e2x);
-            const T q1r = -m1 * ayi, q1i = m1 * ayr;  // d_y A_y
-            const T q2r = m1 * exi, q2i = -m1 * exr;  // -d_y d_x A_x
-            sr = q1r - q2i;
-            si = q1i + q2r;
-            tr = -m1 * eyi - m2 * axr;  // d_y B
-            ti = m1 * eyr - m2 * axi;
-        };
-#pragma unroll
-        for (int k1 = 0; k1 < P; ++k1) {
-            const int k1p = (P - k1) % P;
-            const T c0x = cr[0][k1], c0y = ci[0][k1], c1x = cr[1][k1p], c1y = ci[1][k1p];
-            const T e0x = er[0][k1], e0y = ei[0][k1], e1x = er[1][k1p], e1y = ei[1][k1p];
-            comb(k2a, k1, c0x, c0y, c1x, c1y, e0x, e0y, e1x, e1y, cr[0][k1], ci[0][k1],
-                 er[0][k1], ei[0][k1]);
-            comb(k2b, k1p, c1x, c1y, c0x, c0y, e1x, e1y, e0x, e0y, cr[1][k1p], ci[1][k1p],
-                 er[1][k1p], ei[1][k1p]);
-        }
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            if (c >= ncol) break;
-            const int k2 = c == 0 ? k2a : k2b;
-            T zr[P], zi[P];
-            PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(cr[c], ci[c], zr, zi, cs);
-#pragma unroll
-            for (int n1 = 0; n1 < P; ++n1) {
-                const int e = (ln * P + n1) * Q + k2;
-                L.b0.re[e] = zr[n1];
-                L.b0.im[e] = zi[n1];
-            }
-            PfaWarp<T, P, Q>::template dft_real_pair<+1, H>(er[c], ei[c], zr, zi, cs);
-#pragma unroll
-            for (int n1 = 0; n1 < P; ++n1) {
-                const int e = (ln * P + n1) * Q + k2;
-                L.b1.re[e] = zr[n1];
-                L.b1.im[e] = zi[n1];
-            }
-        }
+            const T m = a.s1 * kk - a.s2 * kk * kk;
+            re *= m;
+            im *= m;
+        });
+        __syncwarp();
+        inverse(L.b1);
+        L.each([&](int ln, int n, int i) { a.dyB[gi(ln, n)] = L.b1.re[i]; });
+        __syncwarp();
+        L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+                [&](int ln, int n) { return &a.dxxay[gi(ln, n)]; });
+        cp_commit();
+        inverse(L.b0);
+        cp_wait<0>();
+        __syncwarp();
+        L.each([&](int ln, int n, int i) {
+            a.divA[gi(ln, n)] = L.b1.re[i] + L.b0.im[i];
+            a.dxB[gi(ln, n)] = L.b1.im[i] - L.b0.re[i];
+        });
     }
-    __syncwarp();
-    inverse(L.b1);
-    L.each([&](int ln, int n, int i) { a.dyB[gi(ln, n)] = L.b1.re[i]; });
-    __syncwarp();
-    L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
-            [&](int ln, int n) { return &a.dxxay[gi(ln, n)]; });
-    cp_commit();
-    inverse(L.b0);
-    cp_wait<0>();
-    __syncwarp();
-    L.each([&](int ln, int n, int i) {
-        a.divA[gi(ln, n)] = L.b1.re[i] + L.b0.re[i];
-        a.dxB[gi(ln, n)] = L.b1.im[i] + L.b0.im[i];
-    });
 }
 
 template <typename T>
