@@ -73,7 +73,6 @@ struct hqt_ctx {
     float2 *dxpsi32 = nullptr, *lap32 = nullptr, *E32 = nullptr, *dypsi32 = nullptr;
     float *dxxay32 = nullptr, *divA32 = nullptr, *dxB32 = nullptr, *dyB32 = nullptr;
     float *dxat32 = nullptr, *dyat32 = nullptr;
-    double *f2x = nullptr, *f2y = nullptr, *f2 = nullptr;  // 2-D boundary terms
     double *slice_mean = nullptr;                           // 5 per z-slice
     double *slice_partial = nullptr;                        // 5 per (z, chunk)
     double2 *O = nullptr;
@@ -704,21 +703,8 @@ int enqueue_stages_mixed(hqt_ctx *c) {
         a.wax = ax;
         a.way = ay;
         a.wrho = c->rho;
-        a.f2x = c->f2x;
-        a.f2y = c->f2y;
         a.slice_mean = c->slice_mean;
         RC(launch_zstage_mixed(c, s, a));
-        // F2(z=0) = d_x(Lz(nz,:)A_x) + d_y(Lz(nz,:)A_y) in FP64 on one slice
-        RC(launch_x_d1(c, FieldIn<double>{nullptr, c->f2x, nullptr},
-                       FieldOut<double>{nullptr, c->f2x, nullptr}, 1));
-        RC(launch_y_d1(c, FieldIn<double>{nullptr, c->f2y, nullptr}, c->f2x,
-                       FieldOut<double>{nullptr, c->f2, nullptr}, 1));
-        {
-            Prof pr(c, K_RHO);
-            k_rho_stage<<<148, 256, 0, c->stream>>>(c->f2, c->p.dt, s, c->plane, c->rho, c->krho,
-                                                     c->rho);
-            CK(cudaGetLastError());
-        }
     }
     return HQT_OK;
 }
@@ -839,7 +825,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 3 + 4 * 3 : 0);
+    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -1162,9 +1148,6 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         A(&c->dyB32, sizeof(float) * V);
         A(&c->dxat32, sizeof(float) * V);
         A(&c->dyat32, sizeof(float) * V);
-        A(&c->f2x, sizeof(double) * P2);
-        A(&c->f2y, sizeof(double) * P2);
-        A(&c->f2, sizeof(double) * P2);
         A(&c->slice_mean, sizeof(double) * 5 * p.nz);
         A(&c->slice_partial, sizeof(double) * 5 * kSliceChunks * p.nz);
     }

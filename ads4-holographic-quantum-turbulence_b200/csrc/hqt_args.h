@@ -128,10 +128,6 @@ template <typename T, typename TS, typename TD = T> struct ZStageArgs {
     const TS *slice_mean;
     C2<TS> *wpsi;  // new state (stage 4)
     TS *wax, *way, *wrho;
-    // When set (mixed precision), k_zgauge writes the boundary-row contractions
-    // Lz(nz,:)*A_x and Lz(nz,:)*A_y (2-D, type T) and k_zpsi leaves rhoi alone:
-    // F2 = d_x(Lz(nz,:)A_x) + d_y(Lz(nz,:)A_y) is then formed in T precision.
-    T *f2x, *f2y;
     // right-hand-side outputs (MODE 0)
     C2<T> *f1;
     T *f3, *f4, *f2b;

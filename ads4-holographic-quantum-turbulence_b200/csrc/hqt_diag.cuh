@@ -182,22 +182,6 @@ __global__ void k_state_to_f32(const double2 *psi, const double *at, const doubl
     }
 }
 
-// rhoi bookkeeping of one stage from F2 at the boundary slice (2-D):
-// stages 1-3 accumulate k2 = h*F2, stage 4 applies rhoi -= (1/6)(sum).
-__global__ void k_rho_stage(const double *f2, double h, int mode, long long plane,
-                            const double *zrho, double *krho, double *wrho) {
-    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < plane;
-         s += (long long)gridDim.x * blockDim.x) {
-        const double k = h * f2[s];
-        if (mode == 1)
-            krho[s] = k;
-        else if (mode == 2 || mode == 3)
-            krho[s] = krho[s] + 2 * k;
-        else
-            wrho[s] = zrho[s] - (1.0 / 6.0) * (krho[s] + k);
-    }
-}
-
 // rhoi replicated along z -> 2-D, and back.
 __global__ void k_rho_gather(const double *rho3, int nz, long long plane, double *rho2) {
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < plane;

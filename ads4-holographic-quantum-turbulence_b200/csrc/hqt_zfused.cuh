@@ -250,22 +250,6 @@ __global__ void __launch_bounds__(kZThreads, 3)
         __syncthreads();  // every thread's copies are in
 
         // ---- F3, F4: both gauge components at once -------------------------
-        if (a.f2x) {
-            // boundary-row contractions Lz(nz,:) A (mixed precision forms F2)
-            double bx = 0.0, by = 0.0;
-#pragma unroll
-            for (int m = 0; m < MT; ++m) {
-                const double2 v = AXY(8 * m + g, cw + q);
-                bx = fma(lzr[m], v.x, bx);
-                by = fma(lzr[m], v.y, by);
-            }
-            bx = zf_colsum(bx);
-            by = zf_colsum(by);
-            if (g == 0 && site < P) {
-                a.f2x[site] = bx;
-                a.f2y[site] = by;
-            }
-        }
         {  // g = d A_t + f Lz A
             double c[MT][2];
             zm_pair<MT, KS>(ALz, AXYw, c, lane);
@@ -439,7 +423,7 @@ __global__ void __launch_bounds__(kZThreads, 3)
             const long long sl = site;
             if (MODE == 0) {
                 a.f2b[sl] = kb;
-            } else if (!a.f2x) {
+            } else {
                 const TS k = a.h * TS(kb);
                 if (MODE == 1)
                     a.krho[sl] = k;
