@@ -47,6 +47,7 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 2>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 3>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 4>);
+    opt((const void *)k_zcons_tc<HQT_ZN>);
     return e;
 }
 
@@ -111,10 +112,22 @@ cudaError_t z_stage_mixed<HQT_ZN>(int mode, const ZStageArgs<double, double, flo
 }
 
 template <>
-cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, int grid, int threads,
+cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, int, int,
                            cudaStream_t s) {
+    static int per_sm = 0, nsm = 0;
+    constexpr size_t smem = zcons_smem_bytes<HQT_ZN>();
+    if (per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zcons_tc<HQT_ZN>, kZThreads,
+                                                      smem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const long long tiles = (a.plane + kZTile - 1) / kZTile;
+    const long long full = (long long)per_sm * (nsm > 0 ? nsm : 1);
     const ZOps<double, HQT_ZN> op = make_zops(h);
-    k_zcons<double, HQT_ZN><<<grid, threads, 0, s>>>(a, op);
+    k_zcons_tc<HQT_ZN><<<(int)(tiles < full ? tiles : full), kZThreads, smem, s>>>(a, op);
     return cudaGetLastError();
 }
 

@@ -440,4 +440,126 @@ __global__ void __launch_bounds__(kZThreads, 3)
     cp_wait<0>();
 }
 
+// Constraint, A_t rebuild, boundary rows and O after the RK combine
+// (scripts/simulation/tevol_driven_cluster.m:129-136) on the same block
+// tiles and FP64 tensor-core products as k_zstage:
+//   cons = Lz(div A) - 2 Im(conj(Psi) Lz Psi),  v = Lzr(cons) - rhoi,
+//   A_t = Lzr(v) + mu (A_t(nz) = mu),  d_z A_t = Lz A_t,
+//   Psi(nz) = A_x(nz) = 0, A_y(nz) = -vy,  O = Lz(nz,:) Psi (Psi(nz) = 0).
+// Real fields use the x parts of pair tiles (y parts stay zero).
+constexpr int kZConsTiles = 4;  // pair tiles: Psi, div A, two scratch
+template <int NZP>
+__host__ __device__ constexpr int zcons_smem_bytes() {
+    return kZConsTiles * ZmDims<NZP>::LV * kZTile * 16;
+}
+
+template <int NZP>
+__global__ void __launch_bounds__(kZThreads)
+    k_zcons_tc(const __grid_constant__ ZConsArgs<double> a,
+               const __grid_constant__ ZOps<double, NZP> op) {
+    using D = ZmDims<NZP>;
+    constexpr int MT = D::MT, KS = D::KS, L = D::LV * kZTile;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+    const int cw = kZCols * warp;
+    const int nz = a.nz;
+    const long long P = a.plane;
+    double2 *sm = reinterpret_cast<double2 *>(g_smem);
+    for (int i = tid; i < kZConsTiles * L; i += kZThreads) sm[i] = make_double2(0.0, 0.0);
+    double ALz[MT][KS], ALz1[MT][KS], lzr[MT];
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+        const int i = 8 * m + g;
+        lzr[m] = i < NZP ? op.lzb[i < NZP ? i : 0] : 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            const int j = 4 * s + q;
+            const bool in = (i < NZP) && (j < NZP);
+            ALz[m][s] = in ? op.Lz[in ? i : 0][in ? j : 0] : 0.0;
+            ALz1[m][s] = in ? op.Lz1[in ? i : 0][in ? j : 0] : 0.0;
+        }
+    }
+    __syncthreads();
+    const ZTileF<double2> PS{sm}, DV{sm + L}, V1{sm + 2 * L}, V2{sm + 3 * L};
+    const auto PSw = PS.cols(cw), DVw = DV.cols(cw), V1w = V1.cols(cw), V2w = V2.cols(cw);
+    const long long ntiles = (P + kZTile - 1) / kZTile;
+#pragma unroll 1
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long site0 = tile * kZTile, site = site0 + cw + q;
+        const bool ok = site < P;
+        zf_real<NZP, double2>(PS, a.psi, nz, P, site0, tid);
+#pragma unroll
+        for (int it = 0; it < (NZP * kZTile + kZThreads - 1) / kZThreads; ++it) {
+            const int e = tid + kZThreads * it, l = e / kZTile, c = e % kZTile;
+            if (l < nz && site0 + c < P) cp_async<8>(&DV(l, c).x, a.divA + l * P + site0 + c);
+        }
+        cp_commit();
+        cp_wait<0>();
+        __syncthreads();
+        {  // cons (levels < nz-1 enter Lzr)
+            double c1[MT][2], c2[MT][2];
+            zm_pair<MT, KS>(ALz, PSw, c1, lane);
+            zm_pair<MT, KS>(ALz, DVw, c2, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                const double2 ps = PS(i < nz ? i : 0, cw + q);
+                const double cons = c2[m][0] - 2.0 * (ps.x * c1[m][1] - ps.y * c1[m][0]);
+                V1(i, cw + q) = make_double2(i < nz - 1 ? cons : 0.0, 0.0);
+            }
+        }
+        __syncwarp();
+        const double rho = ok ? a.rho[site] : 0.0;
+        {  // v = Lzr(cons) - rhoi
+            double v[MT][2];
+            zm_pair<MT, KS>(ALz1, V1w, v, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                V2(i, cw + q) = make_double2(i < nz - 1 ? v[m][0] - rho : 0.0, 0.0);
+            }
+        }
+        __syncwarp();
+        {  // A_t = Lzr(v) + mu, A_t(nz) = mu
+            double t[MT][2];
+            zm_pair<MT, KS>(ALz1, V2w, t, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                const double at = i < nz - 1 ? t[m][0] + a.mu : (i == nz - 1 ? a.mu : 0.0);
+                V1(i, cw + q) = make_double2(at, 0.0);
+                if (i < nz && ok) a.at[(long long)i * P + site] = at;
+            }
+        }
+        __syncwarp();
+        {  // d_z A_t of the rebuilt potential (step-constant during the next step)
+            double d[MT][2];
+            zm_pair<MT, KS>(ALz, V1w, d, lane);
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int i = 8 * m + g;
+                if (i < nz && ok) a.dat[(long long)i * P + site] = d[m][0];
+            }
+        }
+        // O = (Lz Psi)(nz) with Psi(nz) = 0 (:136), then the boundary rows (:133)
+        double orr = 0.0, oi = 0.0;
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            const int i = 8 * m + g;
+            const double2 ps = PS(i < nz - 1 ? i : 0, cw + q);
+            orr = fma(i < nz - 1 ? lzr[m] : 0.0, ps.x, orr);
+            oi = fma(i < nz - 1 ? lzr[m] : 0.0, ps.y, oi);
+        }
+        orr = zf_colsum(orr);
+        oi = zf_colsum(oi);
+        if (g == 0 && ok) {
+            if (a.O) a.O[site] = make_double2(orr, oi);
+            const long long gb = (long long)(nz - 1) * P + site;
+            a.psi[gb] = make_double2(0.0, 0.0);
+            a.ax[gb] = 0.0;
+            a.ay[gb] = -a.vy;
+        }
+        __syncthreads();  // every warp is done with the tiles: the next tile refills them
+    }
+}
+
 }  // namespace hqt
