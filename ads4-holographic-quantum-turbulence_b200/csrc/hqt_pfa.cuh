@@ -119,47 +119,58 @@ template <int P, int Q> struct PfaStageA<double, P, Q> {
             for (int s = 0; s < KSA; ++s) As[m][s] = frag[32 * j++ + lane];
     }
 
+    // Two operand tiles per pass: twice the independent accumulator chains
+    // in flight.  Tiles past NTA read as zero and put nothing (uc, u >= U).
     template <int SIGN, typename Put>
     __device__ __forceinline__ void run(PfaBuf<double> in, Put put, int g, int q) const {
 #pragma unroll 1
-        for (int nt = 0; nt < D::NTA; ++nt) {
-            double pa[MTA][2], qa[MTA][2];
+        for (int n0 = 0; n0 < D::NTA; n0 += 2) {
+            double pa[2][MTA][2], qa[2][MTA][2];
 #pragma unroll
-            for (int m = 0; m < MTA; ++m) pa[m][0] = pa[m][1] = qa[m][0] = qa[m][1] = 0.0;
-            const int uc = 4 * nt + (g >> 1);  // operand column (u, part g&1)
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int m = 0; m < MTA; ++m)
+                    pa[j][m][0] = pa[j][m][1] = qa[j][m][0] = qa[j][m][1] = 0.0;
             const double *pl = (g & 1) ? in.im : in.re;
-            const bool okc = uc < D::U;
 #pragma unroll
             for (int s = 0; s < KSA; ++s) {
                 const int t = 4 * s + q;
-                double a = 0.0, b = 0.0;
-                if (okc && t <= M) {
-                    const double xt = pl[uc * Q + t];
-                    if (t == 0) {
-                        a = xt;
-                    } else {
-                        const double xr = pl[uc * Q + (Q - t)];
-                        a = xt + xr;
-                        b = xt - xr;
-                    }
-                }
 #pragma unroll
-                for (int m = 0; m < MTA; ++m) {
-                    pfa_mma(pa[m][0], pa[m][1], Ac[m][s], a);
-                    pfa_mma(qa[m][0], qa[m][1], As[m][s], b);
+                for (int j = 0; j < 2; ++j) {
+                    const int uc = 4 * (n0 + j) + (g >> 1);  // operand column (u, part g&1)
+                    double a = 0.0, b = 0.0;
+                    if (uc < D::U && t <= M) {
+                        const double xt = pl[uc * Q + t];
+                        if (t == 0) {
+                            a = xt;
+                        } else {
+                            const double xr = pl[uc * Q + (Q - t)];
+                            a = xt + xr;
+                            b = xt - xr;
+                        }
+                    }
+#pragma unroll
+                    for (int m = 0; m < MTA; ++m) {
+                        pfa_mma(pa[j][m][0], pa[j][m][1], Ac[m][s], a);
+                        pfa_mma(qa[j][m][0], qa[j][m][1], As[m][s], b);
+                    }
                 }
             }
             // lane holds rows k = 8m+g, column u = 4nt+q, parts re (0) and im (1).
-            // A tile writes only its own columns, after all its reads: stage A
-            // may run in place.
+            // The tiles write only their own columns, after all their reads:
+            // stage A may run in place.
             __syncwarp();
-            const int u = 4 * nt + q;
-            if (u < D::U) {
 #pragma unroll
-                for (int m = 0; m < MTA; ++m) {
-                    const int k = 8 * m + g;
-                    if (k > M) continue;
-                    pfa_unfold<SIGN, Q>(u, k, pa[m][0], pa[m][1], qa[m][0], qa[m][1], put);
+            for (int j = 0; j < 2; ++j) {
+                const int u = 4 * (n0 + j) + q;
+                if (u < D::U) {
+#pragma unroll
+                    for (int m = 0; m < MTA; ++m) {
+                        const int k = 8 * m + g;
+                        if (k > M) continue;
+                        pfa_unfold<SIGN, Q>(u, k, pa[j][m][0], pa[j][m][1], qa[j][m][0],
+                                            qa[j][m][1], put);
+                    }
                 }
             }
         }
@@ -191,66 +202,74 @@ template <int P, int Q> struct PfaStageA<float, P, Q> {
         ld(Sl);
     }
 
+    // Two operand tiles per pass, as in FP64.
     template <int SIGN, typename Put>
     __device__ __forceinline__ void run(PfaBuf<float> in, Put put, int g, int q) const {
 #pragma unroll 1
-        for (int nt = 0; nt < D::NTA; ++nt) {
-            float pa[MT][4], qa[MT][4];
+        for (int n0 = 0; n0 < D::NTA; n0 += 2) {
+            float pa[2][MT][4], qa[2][MT][4];
 #pragma unroll
-            for (int m = 0; m < MT; ++m)
-#pragma unroll
-                for (int r = 0; r < 4; ++r) pa[m][r] = qa[m][r] = 0.0f;
-            const int uc = 4 * nt + (g >> 1);
-            const float *pl = (g & 1) ? in.im : in.re;
-            const bool okc = uc < D::U;
-#pragma unroll
-            for (int s = 0; s < KS; ++s) {
-                float av[2], bv[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int t = 8 * s + q + 4 * h;
-                    float a = 0.0f, b = 0.0f;
-                    if (okc && t <= M) {
-                        const float xt = pl[uc * Q + t];
-                        if (t == 0) {
-                            a = xt;
-                        } else {
-                            const float xr = pl[uc * Q + (Q - t)];
-                            a = xt + xr;
-                            b = xt - xr;
-                        }
-                    }
-                    av[h] = a;
-                    bv[h] = b;
-                }
-                const unsigned ah0 = pfa_tf32(av[0]), ah1 = pfa_tf32(av[1]);
-                const unsigned al0 = pfa_tf32(av[0] - __uint_as_float(ah0));
-                const unsigned al1 = pfa_tf32(av[1] - __uint_as_float(ah1));
-                const unsigned bh0 = pfa_tf32(bv[0]), bh1 = pfa_tf32(bv[1]);
-                const unsigned bl0 = pfa_tf32(bv[0] - __uint_as_float(bh0));
-                const unsigned bl1 = pfa_tf32(bv[1] - __uint_as_float(bh1));
-#pragma unroll
-                for (int m = 0; m < MT; ++m) {
-                    pfa_mma_tf32(pa[m], Cl[m][s], ah0, ah1);
-                    pfa_mma_tf32(pa[m], Ch[m][s], al0, al1);
-                    pfa_mma_tf32(pa[m], Ch[m][s], ah0, ah1);
-                    pfa_mma_tf32(qa[m], Sl[m][s], bh0, bh1);
-                    pfa_mma_tf32(qa[m], Sh[m][s], bl0, bl1);
-                    pfa_mma_tf32(qa[m], Sh[m][s], bh0, bh1);
-                }
-            }
-            __syncwarp();  // in-place safe, as in FP64
-            const int u = 4 * nt + q;
-            if (u < D::U) {
+            for (int j = 0; j < 2; ++j)
 #pragma unroll
                 for (int m = 0; m < MT; ++m)
 #pragma unroll
+                    for (int r = 0; r < 4; ++r) pa[j][m][r] = qa[j][m][r] = 0.0f;
+            const float *pl = (g & 1) ? in.im : in.re;
+#pragma unroll
+            for (int s = 0; s < KS; ++s) {
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int uc = 4 * (n0 + j) + (g >> 1);
+                    float av[2], bv[2];
+#pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const int k = 16 * m + g + 8 * h;
-                        if (k > M) continue;
-                        pfa_unfold<SIGN, Q>(u, k, pa[m][2 * h], pa[m][2 * h + 1], qa[m][2 * h],
-                                            qa[m][2 * h + 1], put);
+                        const int t = 8 * s + q + 4 * h;
+                        float a = 0.0f, b = 0.0f;
+                        if (uc < D::U && t <= M) {
+                            const float xt = pl[uc * Q + t];
+                            if (t == 0) {
+                                a = xt;
+                            } else {
+                                const float xr = pl[uc * Q + (Q - t)];
+                                a = xt + xr;
+                                b = xt - xr;
+                            }
+                        }
+                        av[h] = a;
+                        bv[h] = b;
                     }
+                    const unsigned ah0 = pfa_tf32(av[0]), ah1 = pfa_tf32(av[1]);
+                    const unsigned al0 = pfa_tf32(av[0] - __uint_as_float(ah0));
+                    const unsigned al1 = pfa_tf32(av[1] - __uint_as_float(ah1));
+                    const unsigned bh0 = pfa_tf32(bv[0]), bh1 = pfa_tf32(bv[1]);
+                    const unsigned bl0 = pfa_tf32(bv[0] - __uint_as_float(bh0));
+                    const unsigned bl1 = pfa_tf32(bv[1] - __uint_as_float(bh1));
+#pragma unroll
+                    for (int m = 0; m < MT; ++m) {
+                        pfa_mma_tf32(pa[j][m], Cl[m][s], ah0, ah1);
+                        pfa_mma_tf32(pa[j][m], Ch[m][s], al0, al1);
+                        pfa_mma_tf32(pa[j][m], Ch[m][s], ah0, ah1);
+                        pfa_mma_tf32(qa[j][m], Sl[m][s], bh0, bh1);
+                        pfa_mma_tf32(qa[j][m], Sh[m][s], bl0, bl1);
+                        pfa_mma_tf32(qa[j][m], Sh[m][s], bh0, bh1);
+                    }
+                }
+            }
+            __syncwarp();  // in-place safe, as in FP64
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int u = 4 * (n0 + j) + q;
+                if (u < D::U) {
+#pragma unroll
+                    for (int m = 0; m < MT; ++m)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int k = 16 * m + g + 8 * h;
+                            if (k > M) continue;
+                            pfa_unfold<SIGN, Q>(u, k, pa[j][m][2 * h], pa[j][m][2 * h + 1],
+                                                qa[j][m][2 * h], qa[j][m][2 * h + 1], put);
+                        }
+                }
             }
         }
     }

@@ -5,25 +5,26 @@
 // (:120-124,128).
 //
 // Every radial operator is an Nz x Nz matrix applied to all columns, i.e. a
-// product (Nz x Nz) x (Nz x columns).  A warp owns a tile of kZCols = 4
-// adjacent (x, y) columns and runs each product on the FP64 tensor cores
-// (mma.sync m8n8k4 f64).  The mma's 8 columns are (column, part) pairs: the
-// real and imaginary parts of Psi, or the x and y components of the gauge
-// field, so both gauge components share one product.  The zero-padded Lz and
-// Lz1 stay in the warp's registers as A fragments for the life of the
-// (persistent) warp; the column data is the B operand, read from the warp's
-// own shared-memory tile.  The tile's inputs are staged there with cp.async
-// in phase groups; buffers of finished phases are refilled with the inputs
-// of later ones (and of the next tile) while the current phase computes.
-// Warps share nothing, so there are no block barriers.
+// product (Nz x Nz) x (Nz x columns), run on the FP64 tensor cores
+// (mma.sync m8n8k4 f64).  A block stages a tile of kZTile = 16 adjacent
+// (x, y) columns (128-byte level rows) with cp.async shared by all its
+// threads; each of its 4 warps owns kZCols = 4 of the columns.  The mma's 8
+// columns are (column, part) pairs: the real and imaginary parts of Psi, or
+// the x and y components of the gauge field, so both gauge components share
+// one product.  The zero-padded Lz and Lz1 stay in registers as A fragments
+// for the life of the (persistent) block; the column data is the B operand,
+// read from the shared tile.  Buffers of finished phases are refilled with
+// the inputs of later ones (and of the next tile) while the current phase
+// computes.
 //
 // Fragment layouts (g = lane/4, q = lane%4): A a0 = L[8m+g][4s+q];
 // B b0 = V[level 4s+q][column g/2].part(g%2); C c_i = out[level 8m+g]
 // [column q].part(i).  A lane thus holds whole complex values (or both gauge
 // components) of levels 8m+g of column q, where the pointwise terms are
-// evaluated.  Each tile field is [level][4 columns]; operand reads, C-fragment
-// accesses and the cp.async fills are all contiguous runs of 32 lanes.
-//
+// evaluated.  Each tile field is [level][kZTile columns] with a per-level
+// XOR swizzle of the 4-column groups (zswz), so both access shapes are free
+// of bank conflicts.
+
 // Phases of a tile (MODE 1..4 = RK stage, MODE 0 = right-hand side only);
 // R, G and V are the warp's shared-memory regions:
 //   Gm  Psi, (A_x, A_y), d_x Psi, d_y Psi -> R            (prefetched)
@@ -64,12 +65,23 @@ template <int NZP> struct ZmDims {
     static constexpr int LV = MP > KP ? MP : KP;  // levels stored per tile field
 };
 
+// Column swizzle of level row l for elements of B bytes: the 4-column group
+// of a column is XORed with a function of l, so that the level rows a warp
+// touches at once (rows 8m+g of its 4 columns in the pointwise terms, rows
+// 4s+q of the mma B operand) fall on disjoint shared-memory banks.  A
+// 4-aligned group of columns stays contiguous and in order.
+template <int B> __host__ __device__ constexpr int zswz(int l) {
+    return B == 16 ? (l & 1) << 2 : B == 8 ? (l & 3) << 2 : ((l >> 1) & 3) << 2;
+}
 // Field of a tile in shared memory: element (level l, column c) at
-// l*kZTile + c.  A warp's view starts at its first column.
+// l*kZTile + (c ^ zswz(l)).  A warp's view carries its first column c0.
 template <typename V> struct ZTileF {
     V *p;
-    __device__ __forceinline__ V &operator()(int l, int c) const { return p[l * kZTile + c]; }
-    __device__ __forceinline__ ZTileF<V> cols(int c0) const { return ZTileF<V>{p + c0}; }
+    int c0 = 0;
+    __device__ __forceinline__ V &operator()(int l, int c) const {
+        return p[l * kZTile + ((c0 + c) ^ zswz<(int)sizeof(V)>(l))];
+    }
+    __device__ __forceinline__ ZTileF<V> cols(int c) const { return ZTileF<V>{p, c0 + c}; }
 };
 
 template <typename TD, int NZP> struct ZfLayout {
@@ -143,11 +155,13 @@ __device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double
                                         double (&C)[MT][2], int lane) {
     const double *v = reinterpret_cast<const double *>(V.p);
     const int g = lane >> 2, q = lane & 3;
+    // level 4s+q, column c0 + g/2, part g%2 (the row's swizzle depends on q only)
+    const int cg = 2 * (V.c0 ^ zswz<16>(q)) + g;
 #pragma unroll
     for (int m = 0; m < MT; ++m) C[m][0] = C[m][1] = 0.0;
 #pragma unroll
     for (int s = 0; s < KS; ++s) {
-        const double b = v[(4 * s + q) * 2 * kZTile + g];
+        const double b = v[(4 * s + q) * 2 * kZTile + cg];
 #pragma unroll
         for (int m = 0; m < MT; ++m) dmma(C[m][0], C[m][1], A[m][s], b);
     }
