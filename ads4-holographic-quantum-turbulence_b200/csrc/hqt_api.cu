@@ -50,6 +50,9 @@ struct hqt_ctx {
     double2 *rootsx = nullptr, *rootsy = nullptr;
     float2 *rootsx32 = nullptr, *rootsy32 = nullptr;
     double *mx = nullptr, *my = nullptr;
+    // x-spectral columns zeroed by the symmetrised filter weight,
+    // mx(kx) = mx(-kx) = 0: one contiguous range (dead0 > dead1 when empty)
+    int dead0 = 1, dead1 = 0;
     // operators (host copies, nz x nz row-major)
     std::vector<double> Lz, Lz1, zz;
     // state
@@ -486,6 +489,8 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
             a.spec[f] = spec[f];
         }
         a.st = phase ? c->st : nullptr;
+        a.dead0 = c->dead0;
+        a.dead1 = c->dead1;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_FWD);
         if (c->px) {
@@ -510,6 +515,8 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.mx = c->mx;
         a.my = c->my;
         a.scale = 1.0 / ((double)c->nx * (double)c->ny);
+        a.dead0 = c->dead0;
+        a.dead1 = c->dead1;
         dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
         Prof pr(c, K_FILT_Y);
         if (c->py) {
@@ -534,6 +541,8 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
             a.out[f] = out[f];
         }
         a.st = check ? c->st : nullptr;
+        a.dead0 = c->dead0;
+        a.dead1 = c->dead1;
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_INV);
         if (c->px) {
@@ -1168,6 +1177,19 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         filter_band(p.nx, lo, hi);
         for (int i = lo - 1; i <= hi - 1; ++i)
             if (i >= 0 && i < p.nx) hmx[i] = 0.0;
+        for (int k = 0; k < p.nx; ++k) {
+            const bool dead = hmx[k] == 0.0 && hmx[(p.nx - k) % p.nx] == 0.0;
+            if (!dead) continue;
+            if (c->dead0 > c->dead1) {
+                c->dead0 = c->dead1 = k;
+            } else if (k == c->dead1 + 1) {
+                c->dead1 = k;
+            } else {  // not one range: skip nothing
+                c->dead0 = 1;
+                c->dead1 = 0;
+                break;
+            }
+        }
         filter_band(p.ny, lo, hi);
         for (int i = lo - 1; i <= hi - 1; ++i)
             if (i >= 0 && i < p.ny) hmy[i] = 0.0;

@@ -26,8 +26,10 @@ template <typename T, int P, int Q> struct PfaLines {
     using D = PfaDims<P, Q>;
     static constexpr int N = D::N, LN = kPfaLines * N;
     PfaBuf<T> b0, b1;
-    int valid;  // lines of this warp inside the grid
+    int valid;          // lines of this warp inside the grid
+    unsigned skip = 0;  // lines read as zero and never stored (bit ln)
     int lane;
+    __device__ __forceinline__ bool live(int ln) const { return ln < valid && !((skip >> ln) & 1u); }
 
     __device__ __forceinline__ PfaLines(int valid_) : valid(valid_), lane(threadIdx.x & 31) {
         T *sm = reinterpret_cast<T *>(g_smem);
@@ -46,7 +48,7 @@ template <typename T, int P, int Q> struct PfaLines {
     template <typename F> __device__ __forceinline__ void each(F f) const {
         for (int e = lane; e < LN; e += 32) {
             const int ln = e % kPfaLines, n = e / kPfaLines;
-            if (ln < valid) f(ln, n, pos(ln, n));
+            if (live(ln)) f(ln, n, pos(ln, n));
         }
     }
     // cp.async of the values re(ln, n), im(ln, n) (pointers) into `dst`;
@@ -60,7 +62,7 @@ template <typename T, int P, int Q> struct PfaLines {
     __device__ __forceinline__ void fetch(PfaBuf<T> dst, Re re, Im im, At at) const {
         for (int e = lane; e < LN; e += 32) {
             const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
-            if (ln < valid) {
+            if (live(ln)) {
                 cp_async<sizeof(T)>(dst.re + i, re(ln, n));
                 cp_async<sizeof(T)>(dst.im + i, im(ln, n));
             } else {
@@ -81,7 +83,7 @@ template <typename T, int P, int Q> struct PfaLines {
                                                 At at) const {
         for (int e = lane; e < LN; e += 32) {
             const int ln = e % kPfaLines, n = e / kPfaLines, i = at(ln, n);
-            if (ln < valid) {
+            if (live(ln)) {
                 const long long g = gi(ln, n);
                 if (f.c) {
                     cp_async<sizeof(T)>(dst.re + i, &f.c[g].x);
@@ -106,6 +108,15 @@ template <typename T, int P, int Q> struct PfaLines {
         };
     }
 };
+
+// Column kx of the x spectra survives the filter weight
+// (M(kx,ky) + M(-kx,-ky))/2 for some ky iff mx(kx) or mx(-kx) is nonzero.
+// The others form one range [dead0, dead1] (set up with the masks); they
+// are zero after the y pass, so they are neither transformed along y nor
+// read back.
+__device__ __forceinline__ bool filt_col_live(int kx, int dead0, int dead1) {
+    return kx < dead0 || kx > dead1;
+}
 
 // cos/sin(2 pi j/P), j = 0..P-1, for the CUDA-core stage B
 template <typename T, int P> __device__ __forceinline__ void pfa_twiddles(T (&cs)[2][P]) {
@@ -478,7 +489,7 @@ __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ X
         double2 *spec = a.spec[f];
         for (int e = L.lane; e < L_t::LN; e += 32) {
             const int ln = e % kPfaLines, k = e / kPfaLines;
-            if (ln < L.valid) {
+            if (ln < L.valid && filt_col_live(k, a.dead0, a.dead1)) {
                 const int i = L_t::spos(ln, k);
                 spec[gi(ln, k)] = mk2<T>(L.b1.re[i], L.b1.im[i]);
             }
@@ -501,7 +512,11 @@ __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFilt
     pfa_twiddles<T, P>(cs);
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
-    const L_t L(min(kPfaLines, a.nx - x0));
+    L_t L(min(kPfaLines, a.nx - x0));
+#pragma unroll
+    for (int ln = 0; ln < kPfaLines; ++ln)
+        if (ln < L.valid && !filt_col_live(x0 + ln, a.dead0, a.dead1)) L.skip |= 1u << ln;
+    if (L.skip == (1u << L.valid) - 1u) return;  // every column filtered out
     double2 *spec = a.spec[blockIdx.z];
     auto gi = [&](int ln, int n) { return zoff + (long long)n * a.nx + ln; };
     L.fetch(L.b0, [&](int ln, int n) { return &spec[gi(ln, n)].x; },
@@ -545,9 +560,16 @@ __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ X
 #pragma unroll 1
     for (int f = 0; f < a.nf; ++f) {
         const double2 *spec = a.spec[f];
-        L.fetch(L.b0, [&](int ln, int k) { return &spec[gi(ln, k)].x; },
-                [&](int ln, int k) { return &spec[gi(ln, k)].y; },
-                [](int ln, int k) { return L_t::spos(ln, k); });
+        for (int e = L.lane; e < L_t::LN; e += 32) {
+            const int ln = e % kPfaLines, k = e / kPfaLines, i = L_t::spos(ln, k);
+            if (ln < L.valid && filt_col_live(k, a.dead0, a.dead1)) {
+                cp_async<sizeof(T)>(L.b0.re + i, &spec[gi(ln, k)].x);
+                cp_async<sizeof(T)>(L.b0.im + i, &spec[gi(ln, k)].y);
+            } else {
+                L.b0.re[i] = T(0);
+                L.b0.im[i] = T(0);
+            }
+        }
         cp_commit();
         cp_wait<0>();
         __syncwarp();
