@@ -30,7 +30,8 @@ EXPORTS = [
     "hqt_winding_device", "hqt_count_vortices", "hqt_count_vortices_device",
     "hqt_profile", "hqt_profile_report",
     "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
-    "hqt_energy_spectrum_device",
+    "hqt_energy_spectrum_device", "hqt_boundary_velocity_device",
+    "hqt_find_vortices_device", "hqt_vortex_structure_factor_device",
     "hqt_ensemble_create", "hqt_ensemble_destroy", "hqt_ensemble_set_stream",
     "hqt_ensemble_last_error", "hqt_ensemble_step_device",
 ]
@@ -105,6 +106,12 @@ def load() -> ctypes.CDLL:
         "hqt_noalloc_last_error": (c_char_p, []),
         "hqt_energy_spectrum_device": (c_int, [c_void_p, c_void_p, c_int32, dp, dp, dp,
                                                dp, ip]),
+        "hqt_boundary_velocity_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "hqt_find_vortices_device": (c_int, [c_void_p, c_void_p, c_double, c_int32, c_int32,
+                                             dp, dp, ip]),
+        "hqt_vortex_structure_factor_device": (c_int, [c_void_p, c_void_p, c_double, c_double,
+                                                       c_int32, dp, ip, c_int32, dp, dp, dp,
+                                                       ip, dp]),
         "hqt_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
         "hqt_ensemble_destroy": (None, [c_void_p]),
         "hqt_ensemble_set_stream": (c_int, [c_void_p, c_void_p]),

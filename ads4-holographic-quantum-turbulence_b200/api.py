@@ -267,6 +267,67 @@ class Simulation:
         n = nb.value
         return k[:n].copy(), E[:n].copy(), Ec[:n].copy(), Ei[:n].copy()
 
+    def boundary_velocity_device(self, O):
+        """``(vx, vy)``, real ``(ny, nx)`` tensors, of a ``(ny, nx)`` complex
+        CUDA tensor ``O``: ``VX_temp``, ``VY_temp`` of
+        ``scripts/analysis/plots_cluster.m:92-93``."""
+        import torch
+        p = self._dev2(O, True)
+        vx = torch.empty((self.ny, self.nx), dtype=torch.float64, device=O.device)
+        vy = torch.empty_like(vx)
+        self._sync_stream()
+        self._check(self._lib.hqt_boundary_velocity_device(
+            self._ctx, p, ctypes.c_void_p(vx.data_ptr()), ctypes.c_void_p(vy.data_ptr())))
+        return vx, vy
+
+    def boundary_fields_device(self, Z1):
+        """One frame of the boundary-field extraction
+        (``scripts/analysis/plots_cluster.m:89-97``): ``O = func_Lz(Z1)(:,:,nz)``,
+        the velocity observables ``vx, vy`` and ``NofV`` (the total of
+        ``countN``).  Returns ``(O, vx, vy, NofV)`` with device tensors."""
+        O = self.order_parameter_device(Z1)
+        vx, vy = self.boundary_velocity_device(O)
+        n, _, _ = self.count_vortices_device(O)
+        return O, vx, vy, n
+
+    def find_vortices_device(self, O, threshold: float, window_radius: int):
+        """``find_vortices(O, threshold, window_radius)``
+        (``src/diagnostics/find_vortices.m:1-28``) of a ``(ny, nx)`` complex
+        CUDA tensor: ``(vortices, antivortices)``, each ``(n, 2)`` host arrays
+        of refined 1-based ``[row, col]`` positions."""
+        cap = max(self.nx * self.ny // 2, 1)
+        v, a = np.zeros((cap, 2)), np.zeros((cap, 2))
+        n = ctypes.c_int32()
+        p = self._dev2(O, True)
+        self._sync_stream()
+        self._check(self._lib.hqt_find_vortices_device(
+            self._ctx, p, float(threshold), int(window_radius), cap, _dptr(v), _dptr(a),
+            ctypes.byref(n)))
+        k = n.value
+        return v[:k].copy(), a[:k].copy()
+
+    def vortex_structure_factor_device(self, Phi, Lx: float, Ly: float):
+        """``compute_vortex_structure_factor(Phi, Lx, Ly)``
+        (``src/diagnostics/compute_vortex_structure_factor.m:1-104``) of a
+        ``(ny, nx)`` complex CUDA tensor read as the routine's ``[Ny, Nx]``
+        matrix with ``Ny = nx``: ``(k_bin, Sc, Sn, vortices, spacing)``;
+        ``vortices`` rows are ``[x, y, charge]``; ``spacing`` a dict (None
+        without vortices)."""
+        cap = self.nx * self.ny
+        bcap = self.nx + self.ny + 4
+        vort = np.zeros((cap, 3))
+        kb, Sc, Sn, sp = np.zeros(bcap), np.zeros(bcap), np.zeros(bcap), np.zeros(5)
+        nv, nb = ctypes.c_int32(), ctypes.c_int32()
+        p = self._dev2(Phi, True)
+        self._sync_stream()
+        self._check(self._lib.hqt_vortex_structure_factor_device(
+            self._ctx, p, float(Lx), float(Ly), cap, _dptr(vort), ctypes.byref(nv), bcap,
+            _dptr(kb), _dptr(Sc), _dptr(Sn), ctypes.byref(nb), _dptr(sp)))
+        k, b = nv.value, nb.value
+        spacing = None if k == 0 else dict(zip(
+            ("rho", "d_density", "d_nnd", "k_density", "k_nnd"), map(float, sp)))
+        return kb[:b].copy(), Sc[:b].copy(), Sn[:b].copy(), vort[:k].copy(), spacing
+
     def count_vortices(self, O) -> tuple[int, int, int]:
         """``countN`` of a host ``(nx, ny)`` complex field."""
         O = np.asarray(O)

@@ -80,6 +80,8 @@ struct hqt_ctx {
     double *slice_partial = nullptr;                        // 5 per (z, chunk)
     double2 *O = nullptr;
     double *partial = nullptr;
+    double *colmax = nullptr;  // spectrum: max |O| per y index
+    int *d_vcount = nullptr;   // vortex compaction: counts and offsets per block
     double *kxv = nullptr, *kyv = nullptr, *bins = nullptr;  // spectrum scratch
     int max_bins = 0;
     int *d_int = nullptr;  // scratch ints (winding, counts)
@@ -942,6 +944,193 @@ void signed_k(int n, double scale, std::vector<double> &k) {
     }
 }
 
+// Density-weighted boundary velocity of O (scripts/analysis/plots_cluster.m:92-93,
+// movie_show.m:93-94) with spectral first derivatives: as U = ux + i uy, or
+// into vx, vy when U is null.  Scratch: dxxpsi, dypsi.
+int boundary_velocity(hqt_ctx *c, const double2 *O, double2 *U, double *vx, double *vy) {
+    double2 *dOx = c->dxxpsi, *dOy = c->dypsi;
+    RC(launch_x_d1(c, FieldIn<double>{O, nullptr, nullptr}, FieldOut<double>{dOx, nullptr, nullptr}, 1));
+    RC(launch_y_d1(c, FieldIn<double>{O, nullptr, nullptr}, nullptr,
+                   FieldOut<double>{dOy, nullptr, nullptr}, 1));
+    k_spec_colmax<<<c->ny, kRedThreads, 0, c->stream>>>(O, c->nx, c->colmax);
+    CK(cudaGetLastError());
+    k_spec_velocity<<<kPartials, 256, 0, c->stream>>>(O, dOx, dOy, c->nx, c->plane, c->colmax,
+                                                      U, vx, vy);
+    CK(cudaGetLastError());
+    return HQT_OK;
+}
+
+// Ordered compaction of the charge grid q (memory = MATLAB find order) into
+// list0 (q == +1, or q != 0 with any) and list1 (q == -1); counts out.
+int vortex_compact(hqt_ctx *c, const signed char *q, bool any, int *list0, int *list1,
+                   int *n0_out, int *n1_out) {
+    const long long n = c->plane;
+    const long long chunk = (n + kPartials - 1) / kPartials;
+    int *counts = c->d_vcount, *offs = c->d_vcount + 2 * kPartials;
+    if (any)
+        k_vort_compact<true, 0><<<kPartials, kVortThreads, 0, c->stream>>>(q, n, chunk, counts,
+                                                                           nullptr, nullptr, nullptr);
+    else
+        k_vort_compact<false, 0><<<kPartials, kVortThreads, 0, c->stream>>>(q, n, chunk, counts,
+                                                                            nullptr, nullptr, nullptr);
+    CK(cudaGetLastError());
+    std::vector<int> h(2 * kPartials), o(2 * kPartials);
+    CK(cudaMemcpyAsync(h.data(), counts, sizeof(int) * 2 * kPartials, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    int t0 = 0, t1 = 0;
+    for (int b = 0; b < kPartials; ++b) {
+        o[2 * b] = t0;
+        o[2 * b + 1] = t1;
+        t0 += h[2 * b];
+        t1 += h[2 * b + 1];
+    }
+    CK(cudaMemcpyAsync(offs, o.data(), sizeof(int) * 2 * kPartials, cudaMemcpyHostToDevice,
+                       c->stream));
+    if (any)
+        k_vort_compact<true, 1><<<kPartials, kVortThreads, 0, c->stream>>>(q, n, chunk, nullptr,
+                                                                           offs, list0, list1);
+    else
+        k_vort_compact<false, 1><<<kPartials, kVortThreads, 0, c->stream>>>(q, n, chunk, nullptr,
+                                                                            offs, list0, list1);
+    CK(cudaGetLastError());
+    *n0_out = t0;
+    *n1_out = t1;
+    return HQT_OK;
+}
+
+// find_vortices (src/diagnostics/find_vortices.m:1-28) of O [nx, ny]
+int find_vortices_dev(hqt_ctx *c, const double2 *O, double threshold, int radius, int capacity,
+                      double *vort, double *avort, int32_t *n_out) {
+    signed char *q = reinterpret_cast<signed char *>(c->dxB);
+    int *list0 = reinterpret_cast<int *>(c->dyB), *list1 = list0 + c->plane;
+    k_vort_charge<0><<<kPartials, 256, 0, c->stream>>>(O, c->nx, c->ny, q);
+    CK(cudaGetLastError());
+    int nv = 0, na = 0;
+    RC(vortex_compact(c, q, false, list0, list1, &nv, &na));
+    *n_out = nv;
+    if (nv == 0) return HQT_OK;
+    if (na < nv) return fail(c, HQT_EINVAL, "fewer antivortices than vortices");
+    if (nv > capacity) return fail(c, HQT_EINVAL, "vortex capacity too small");
+    if (4 * (long long)nv > c->vol) return fail(c, HQT_EUNSUPPORTED, "too many vortices");
+    k_vort_absmax2<<<kPartials, kRedThreads, 0, c->stream>>>(O, c->plane, c->partial);
+    CK(cudaGetLastError());
+    double *out = c->divA;  // 4 nv doubles: vortices then antivortices
+    const int g = (nv + 127) / 128;
+    k_vort_refine<<<g, 128, 0, c->stream>>>(O, c->nx, c->ny, list0, nv, c->partial, kPartials,
+                                            threshold, radius, out);
+    CK(cudaGetLastError());
+    k_vort_refine<<<g, 128, 0, c->stream>>>(O, c->nx, c->ny, list1, nv, c->partial, kPartials,
+                                            threshold, radius, out + 2 * nv);
+    CK(cudaGetLastError());
+    std::vector<double> h(4 * (size_t)nv);
+    CK(cudaMemcpyAsync(h.data(), out, sizeof(double) * 4 * nv, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(vort, h.data(), sizeof(double) * 2 * nv);
+    std::memcpy(avort, h.data() + 2 * nv, sizeof(double) * 2 * nv);
+    return HQT_OK;
+}
+
+// compute_vortex_structure_factor (src/diagnostics/compute_vortex_structure_factor.m:1-104)
+// of Phi, the routine's [Ny, Nx] matrix stored as this context's [nx, ny]
+// field (Ny = nx rows, Nx = ny columns).
+int structure_factor_dev(hqt_ctx *c, const double2 *Phi, double Lx, double Ly, int capacity,
+                         double *vort, int32_t *nv_out, int bins_capacity, double *k_bin,
+                         double *Sc, double *Sn, int32_t *nbins_out, double *spacing) {
+    const int n0 = c->nx, n1 = c->ny;  // Ny, Nx of the routine
+    const double dx = Lx / n1, dy = Ly / n0;
+    signed char *q = reinterpret_cast<signed char *>(c->dxB);
+    int *list0 = reinterpret_cast<int *>(c->dyB), *list1 = list0 + c->plane;
+    k_vort_charge<1><<<kPartials, 256, 0, c->stream>>>(Phi, n0, n1, q);
+    CK(cudaGetLastError());
+    int nv = 0, unused = 0;
+    RC(vortex_compact(c, q, true, list0, list1, &nv, &unused));
+    *nv_out = nv;
+    *nbins_out = 0;
+    if (nv == 0) return HQT_OK;  // the routine warns and returns empty results
+    if (nv > capacity) return fail(c, HQT_EINVAL, "vortex capacity too small");
+    if (4 * (long long)nv > c->vol) return fail(c, HQT_EUNSUPPORTED, "too many vortices");
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    const double dkx = two_pi / Lx, dky = two_pi / Ly;
+    const double dk = std::min(dkx, dky);
+    const double kmax = std::min(std::floor(n1 / 2.0) * dkx, std::floor(n0 / 2.0) * dky);
+    const int nbins = (int)std::floor(kmax / dk + 1e-9);
+    *nbins_out = nbins;
+    if (nbins > c->max_bins) return fail(c, HQT_EUNSUPPORTED, "too many structure-factor bins");
+    if (bins_capacity < nbins) return fail(c, HQT_EINVAL, "bin capacity too small");
+    double *dv = c->divA, *nnd = c->divA + 3 * (size_t)nv;
+    const int g = (nv + 127) / 128;
+    k_vort_sf_points<<<g, 128, 0, c->stream>>>(q, list0, nv, n0, dx, dy, dv);
+    CK(cudaGetLastError());
+    k_vort_nnd<<<g, 128, 0, c->stream>>>(dv, nv, Lx, Ly, nnd);
+    CK(cudaGetLastError());
+    // 2-D transform of W = W_c + i W_n with the filter's forward passes
+    double2 *W = c->E, *S = c->dxpsi;
+    k_vort_weights<<<kPartials, 256, 0, c->stream>>>(q, c->plane, W);
+    CK(cudaGetLastError());
+    {
+        XFiltFwdArgs<double> a{};
+        a.plan = c->planx;
+        a.roots = c->rootsx;
+        a.NB = c->NBx_2;
+        a.nlines = c->ny;
+        a.ny = c->ny;
+        a.nf = 1;
+        a.in[0] = FieldIn<double>{W, nullptr, nullptr};
+        a.spec[0] = S;
+        a.st = nullptr;
+        if (c->cx) {
+            const int nb = ct_lines(c->nx, 2);
+            RC(ct_dispatch(c, c->nx, CT_FX_FWD, &a, dim3((c->ny + nb - 1) / nb), smem_x(c->nx, 2, nb)));
+        } else {
+            CK(launch_x_filt_fwd(a, (c->ny + a.NB - 1) / a.NB, smem_x(c->nx, 2, a.NB), c->stream));
+        }
+    }
+    {
+        YFiltArgs<double> a{};
+        a.plan = c->plany;
+        a.roots = c->rootsy;
+        a.TX = c->TXy_2;
+        a.nx = c->nx;
+        a.ny = c->ny;
+        a.nf = 1;
+        a.spec[0] = S;
+        CK(launch_y_fwd(a, dim3((c->nx + a.TX - 1) / a.TX, 1), smem_x(c->ny, 2, a.TX), c->stream));
+    }
+    std::vector<double> ky, kx;
+    signed_k(n0, dky, ky);
+    signed_k(n1, dkx, kx);
+    CK(cudaMemcpyAsync(c->kxv, ky.data(), sizeof(double) * n0, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->kyv, kx.data(), sizeof(double) * n1, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->bins, 0, sizeof(double) * 3 * nbins, c->stream));
+    k_vort_sf_bins<<<kPartials, 256, 0, c->stream>>>(S, n0, n1, c->kxv, c->kyv, dk, nbins,
+                                                     1.0 / nv, c->bins);
+    CK(cudaGetLastError());
+    std::vector<double> hb(3 * (size_t)nbins), hv(4 * (size_t)nv);
+    CK(cudaMemcpyAsync(hb.data(), c->bins, sizeof(double) * 3 * nbins, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaMemcpyAsync(hv.data(), dv, sizeof(double) * 4 * nv, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(vort, hv.data(), sizeof(double) * 3 * nv);
+    double snnd = 0.0;
+    for (int i = 0; i < nv; ++i) snnd += hv[3 * (size_t)nv + i];
+    const double rho = nv / (Lx * Ly), d_density = 1.0 / std::sqrt(rho), d_nnd = snnd / nv;
+    if (spacing) {
+        spacing[0] = rho;
+        spacing[1] = d_density;
+        spacing[2] = d_nnd;
+        spacing[3] = two_pi / d_density;
+        spacing[4] = two_pi / d_nnd;
+    }
+    for (int b = 0; b < nbins; ++b) {
+        const double cnt = hb[2 * (size_t)nbins + b];
+        if (k_bin) k_bin[b] = (b + 0.5) * dk;
+        if (Sc) Sc[b] = cnt > 0 ? hb[b] / cnt : 0.0;
+        if (Sn) Sn[b] = cnt > 0 ? hb[(size_t)nbins + b] / cnt : 0.0;
+    }
+    return HQT_OK;
+}
+
 int energy_spectrum(hqt_ctx *c, const double2 *O, int capacity, double *kout, double *E,
                     double *Ec, double *Ei, int32_t *nbins_out) {
     const double two_pi = 2.0 * 3.14159265358979323846;
@@ -957,15 +1146,8 @@ int energy_spectrum(hqt_ctx *c, const double2 *O, int capacity, double *kout, do
     *nbins_out = nbins;
     if (nbins > c->max_bins) return fail(c, HQT_EUNSUPPORTED, "too many spectrum bins");
     if (capacity < nbins) return fail(c, HQT_EINVAL, "spectrum capacity too small");
-    const long long P = c->plane;
-    double2 *dOx = c->dxxpsi, *dOy = c->dypsi, *U = c->E, *S = c->dxpsi;
-    RC(launch_x_d1(c, FieldIn<double>{O, nullptr, nullptr}, FieldOut<double>{dOx, nullptr, nullptr}, 1));
-    RC(launch_y_d1(c, FieldIn<double>{O, nullptr, nullptr}, nullptr,
-                   FieldOut<double>{dOy, nullptr, nullptr}, 1));
-    k_spec_absmax<<<kPartials, kRedThreads, 0, c->stream>>>(O, P, c->partial);
-    CK(cudaGetLastError());
-    k_spec_velocity<<<kPartials, 256, 0, c->stream>>>(O, dOx, dOy, P, c->partial, kPartials, U);
-    CK(cudaGetLastError());
+    double2 *U = c->E, *S = c->dxpsi;
+    RC(boundary_velocity(c, O, U, nullptr, nullptr));
     {
         XFiltFwdArgs<double> a{};
         a.plan = c->planx;
@@ -1163,6 +1345,8 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->rootsx32, sizeof(float2) * p.nx);
     A(&c->rootsy32, sizeof(float2) * p.ny);
     A(&c->partial, sizeof(double) * kPartials);
+    A(&c->colmax, sizeof(double) * p.ny);
+    A(&c->d_vcount, sizeof(int) * 4 * kPartials);
     c->max_bins = p.nx + p.ny + 4;
     A(&c->kxv, sizeof(double) * p.nx);
     A(&c->kyv, sizeof(double) * p.ny);
@@ -1513,6 +1697,39 @@ int hqt_energy_spectrum_device(hqt_ctx *c, const void *dO, int32_t capacity, dou
     if (!dO || !nbins || capacity < 0) return fail(c, HQT_EINVAL, "bad argument");
     DeviceGuard guard(c->device);
     return energy_spectrum(c, (const double2 *)dO, capacity, k, E, Ec, Ei, nbins);
+}
+
+int hqt_boundary_velocity_device(hqt_ctx *c, const void *dO, void *dvx, void *dvy) {
+    if (!c) return HQT_EINVAL;
+    if (!dO || !dvx || !dvy) return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    RC(boundary_velocity(c, (const double2 *)dO, nullptr, (double *)dvx, (double *)dvy));
+    CK(cudaStreamSynchronize(c->stream));
+    return HQT_OK;
+}
+
+int hqt_find_vortices_device(hqt_ctx *c, const void *dO, double threshold, int32_t radius,
+                             int32_t capacity, double *vortices, double *antivortices,
+                             int32_t *n) {
+    if (!c) return HQT_EINVAL;
+    if (!dO || !n || radius < 0 || capacity < 0 || (capacity > 0 && (!vortices || !antivortices)))
+        return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    return find_vortices_dev(c, (const double2 *)dO, threshold, radius, capacity, vortices,
+                             antivortices, n);
+}
+
+int hqt_vortex_structure_factor_device(hqt_ctx *c, const void *dPhi, double Lx, double Ly,
+                                       int32_t capacity, double *vortices, int32_t *nv,
+                                       int32_t bins_capacity, double *k_bin, double *Sc,
+                                       double *Sn, int32_t *nbins, double *spacing) {
+    if (!c) return HQT_EINVAL;
+    if (!dPhi || !nv || !nbins || capacity < 0 || bins_capacity < 0 || !(Lx > 0) ||
+        !(Ly > 0) || (capacity > 0 && !vortices))
+        return fail(c, HQT_EINVAL, "bad argument");
+    DeviceGuard guard(c->device);
+    return structure_factor_dev(c, (const double2 *)dPhi, Lx, Ly, capacity, vortices, nv,
+                                bins_capacity, k_bin, Sc, Sn, nbins, spacing);
 }
 
 int hqt_count_vortices(hqt_ctx *c, const double *O, int32_t *n, int32_t *np, int32_t *nm) {

@@ -70,8 +70,8 @@ template <typename T> struct XFiltFwdArgs {
     FieldIn<T> in[kMaxFilt];
     C2<T> *spec[kMaxFilt];
     const DevStatus *st;  // phase e^{-2 pi i y w/ny} on field 0 when non-null
-    int dead0, dead1;     // spectral columns dead0 <= kx <= dead1 may be left
-                          // unwritten (prime-factor engine; see filt_col_live)
+    int dead0 = 1, dead1 = 0;  // spectral columns dead0 <= kx <= dead1 may be left
+                               // unwritten (prime-factor engine; empty by default)
 };
 
 template <typename T> struct YFiltArgs {
@@ -82,7 +82,7 @@ template <typename T> struct YFiltArgs {
     C2<T> *spec[kMaxFilt];
     const T *mx, *my;  // 1 - fx, 1 - fy
     T scale;           // 1/(nx*ny)
-    int dead0, dead1;  // columns dead0 <= kx <= dead1 are zero after the weight
+    int dead0 = 1, dead1 = 0;  // columns dead0 <= kx <= dead1 are zero after the weight
 };
 
 template <typename T> struct XFiltInvArgs {
@@ -93,7 +93,7 @@ template <typename T> struct XFiltInvArgs {
     const C2<T> *spec[kMaxFilt];
     FieldOut<T> out[kMaxFilt];
     DevStatus *st;  // non-finite check when non-null
-    int dead0, dead1;  // spectral columns dead0 <= kx <= dead1 read as zero
+    int dead0 = 1, dead1 = 0;  // spectral columns dead0 <= kx <= dead1 read as zero
 };
 
 template <typename T, int NZP> struct ZOps {

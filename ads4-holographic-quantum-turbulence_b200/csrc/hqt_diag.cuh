@@ -200,42 +200,44 @@ __global__ void k_step_end(DevStatus *st) {
 }
 
 // ---- energy spectrum of the boundary superflow --------------------------
-// partial[b] = max |O| over block b
+// colmax[j] = max_i |O(i, j)| over x for each y index j (one block per j).
+// MATLAB's max of the nx x ny boundary slice is the row vector of column
+// maxima, and |O|./max(...) divides column j by its own maximum
+// (scripts/analysis/movie_show.m:93-94, plots_cluster.m:92-93).
 __global__ void __launch_bounds__(kRedThreads)
-    k_spec_absmax(const double2 *O, long long n, double *partial) {
+    k_spec_colmax(const double2 *O, int nx, double *colmax) {
     __shared__ double sh[kRedThreads];
+    const double2 *col = O + (long long)blockIdx.x * nx;
     double m = 0.0;
-    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-         s += (long long)gridDim.x * blockDim.x)
-        m = fmax(m, hypot(O[s].x, O[s].y));
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) m = fmax(m, hypot(col[i].x, col[i].y));
     sh[threadIdx.x] = m;
     __syncthreads();
     for (int w = kRedThreads / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+    if (threadIdx.x == 0) colmax[blockIdx.x] = sh[0];
 }
 
-// U = ux + i uy with u = |O|/max|O| * Im(dO/O)  (= Re(-i(dO - d|O| O/|O|)/O))
+// u = |O|/colmax * Im(dO/O)  (= Re(-i(dO - d|O| O/|O|)/O)) as U = ux + i uy,
+// or into the real fields vx, vy when U is null
 __global__ void k_spec_velocity(const double2 *O, const double2 *dOx, const double2 *dOy,
-                                long long n, const double *partial, int nparts, double2 *U) {
-    __shared__ double amax;
-    if (threadIdx.x == 0) {
-        double m = 0.0;
-        for (int i = 0; i < nparts; ++i) m = fmax(m, partial[i]);
-        amax = m;
-    }
-    __syncthreads();
+                                int nx, long long n, const double *colmax, double2 *U,
+                                double *vx, double *vy) {
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
          s += (long long)gridDim.x * blockDim.x) {
         const double2 o = O[s], a = dOx[s], b = dOy[s];
         const double r2 = o.x * o.x + o.y * o.y;
-        const double w = sqrt(r2) / amax;
+        const double w = sqrt(r2) / colmax[s / nx];
         // Im(d/O) = Im(d conj(O)) / |O|^2
         const double ux = w * (a.y * o.x - a.x * o.y) / r2;
         const double uy = w * (b.y * o.x - b.x * o.y) / r2;
-        U[s] = make_double2(ux, uy);
+        if (U) {
+            U[s] = make_double2(ux, uy);
+        } else {
+            vx[s] = ux;
+            vy[s] = uy;
+        }
     }
 }
 
@@ -268,6 +270,226 @@ __global__ void k_spec_bins(const double2 *Uh, int nx, int ny, const double *kx,
         atomicAdd(&bins[b], e);
         atomicAdd(&bins[nbins + b], ec);
         atomicAdd(&bins[2 * nbins + b], ei);
+    }
+}
+
+// ---- vortex positions and structure factors ---------------------------------
+// The field is a column-major n0 x n1 matrix (element (r, c) at r + c*n0), as
+// the MATLAB routines index it.
+
+__device__ __forceinline__ double mat_mod(double a, double m) { return a - floor(a / m) * m; }
+__device__ __forceinline__ double mat_round(double v) {
+    return v < 0 ? -floor(-v + 0.5) : floor(v + 0.5);
+}
+__device__ __forceinline__ double arg_mul_conj(double2 a, double2 b) {  // angle(a .* conj(b))
+    return atan2(__dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y)),
+                 __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)));
+}
+
+// Plaquette charges.  SF = 1: compute_vortex_structure_factor.m:24-35 (phase
+// differences mod 2 pi around theta -> next column -> diagonal -> next row);
+// SF = 0: find_vortices.m:89-104 (angle(p_next conj(p)) around (r,c) ->
+// (r+1,c) -> (r+1,c+1) -> (r,c+1)).
+template <int SF>
+__global__ void k_vort_charge(const double2 *F, int n0, int n1, signed char *q) {
+    const long long n = (long long)n0 * n1;
+    const double tp = 2.0 * 3.14159265358979323846, pi = 0.5 * tp;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(s % n0), c = (int)(s / n0);
+        const int r1 = r + 1 == n0 ? 0 : r + 1, c1 = c + 1 == n1 ? 0 : c + 1;
+        const double2 p1 = F[s], p2 = F[r1 + (long long)c * n0];
+        const double2 p3 = F[r1 + (long long)c1 * n0], p4 = F[r + (long long)c1 * n0];
+        double w;
+        if (SF) {
+            const double t = atan2(p1.y, p1.x), tx = atan2(p4.y, p4.x);
+            const double txy = atan2(p3.y, p3.x), ty = atan2(p2.y, p2.x);
+            w = (mat_mod(tx - t + pi, tp) - pi) + (mat_mod(txy - tx + pi, tp) - pi);
+            w = w + (mat_mod(ty - txy + pi, tp) - pi);
+            w = w + (mat_mod(t - ty + pi, tp) - pi);
+        } else {
+            w = arg_mul_conj(p2, p1) + arg_mul_conj(p3, p2);
+            w = w + arg_mul_conj(p4, p3);
+            w = w + arg_mul_conj(p1, p4);
+        }
+        q[s] = (signed char)mat_round(w / tp);
+    }
+}
+
+// Ordered compaction of the sites whose charge matches (list 0: q == +1 or,
+// with ANY, q != 0; list 1: q == -1) in memory (= MATLAB find) order.  Block
+// b owns the contiguous chunk [b*chunk, (b+1)*chunk).  Pass 0 counts, pass 1
+// writes at the host-scanned offsets.
+constexpr int kVortThreads = 256;
+template <bool ANY>
+__device__ __forceinline__ bool vort_sel(signed char v, int list) {
+    return ANY ? (list == 0 && v != 0) : (list == 0 ? v == 1 : v == -1);
+}
+template <bool ANY, int PASS>
+__global__ void __launch_bounds__(kVortThreads)
+    k_vort_compact(const signed char *q, long long n, long long chunk, int *counts,
+                   const int *offsets, int *list0, int *list1) {
+    __shared__ int wsum[2][kVortThreads / 32];
+    __shared__ int base[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long b0 = (long long)blockIdx.x * chunk;
+    const long long b1 = b0 + chunk < n ? b0 + chunk : n;
+    if (threadIdx.x < 2) base[threadIdx.x] = PASS ? offsets[2 * blockIdx.x + threadIdx.x] : 0;
+    __syncthreads();
+    for (long long t0 = b0; t0 < b1; t0 += kVortThreads) {
+        const long long s = t0 + threadIdx.x;
+        const signed char v = s < b1 ? q[s] : 0;
+        int rank[2];
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const unsigned m = __ballot_sync(0xffffffffu, s < b1 && vort_sel<ANY>(v, l));
+            rank[l] = __popc(m & ((1u << lane) - 1u));
+            if (lane == 0) wsum[l][warp] = __popc(m);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            int before = 0, total = 0;
+            for (int w = 0; w < kVortThreads / 32; ++w) {
+                before += w < warp ? wsum[l][w] : 0;
+                total += wsum[l][w];
+            }
+            if (PASS && s < b1 && vort_sel<ANY>(v, l)) {
+                int *dst = l == 0 ? list0 : list1;
+                dst[base[l] + before + rank[l]] = (int)s;
+            }
+            rank[l] = total;
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) base[threadIdx.x] += rank[threadIdx.x];
+        __syncthreads();
+    }
+    if (!PASS && threadIdx.x < 2) counts[2 * blockIdx.x + threadIdx.x] = base[threadIdx.x];
+}
+
+// abs(F).^2 as MATLAB forms it (hypot, then the square)
+__device__ __forceinline__ double abs2(double2 v) {
+    const double h = hypot(v.x, v.y);
+    return h * h;
+}
+
+// partial[b] = max |F|^2 over block b
+__global__ void __launch_bounds__(kRedThreads)
+    k_vort_absmax2(const double2 *F, long long n, double *partial) {
+    __shared__ double sh[kRedThreads];
+    double m = 0.0;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, abs2(F[s]));
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// refine_positions (find_vortices.m:30-78) of sites list[k], k < nv: centroid
+// of the (2R+1)^2 periodic window cells with |F|^2/max|F|^2 < threshold, in
+// 1-based matrix-index units, out[2k], out[2k+1] = row, column.
+__global__ void k_vort_refine(const double2 *F, int n0, int n1, const int *list, int nv,
+                              const double *partial, int nparts, double threshold, int R,
+                              double *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    double mx = 0.0;
+    for (int i = 0; i < nparts; ++i) mx = fmax(mx, partial[i]);
+    const int s = list[k];
+    const int rc = s % n0 + 1, cc = s / n0 + 1;  // 1-based
+    long long sr = 0, sc = 0;
+    int cnt = 0;
+    for (int dr = -R; dr <= R; ++dr) {
+        const int r = ((rc + dr - 1) % n0 + n0) % n0;
+        for (int dc = -R; dc <= R; ++dc) {
+            const int c = ((cc + dc - 1) % n1 + n1) % n1;
+            const double2 v = F[r + (long long)c * n0];
+            const double d = abs2(v) / mx;
+            if (d < threshold) {
+                sr += dr;
+                sc += dc;
+                ++cnt;
+            }
+        }
+    }
+    double fr, fc;
+    if (cnt > 0) {
+        const double orr = (double)sr / cnt, occ = (double)sc / cnt;
+        fr = mat_mod((rc + orr) - 1, (double)n0) + 1;
+        fc = mat_mod((cc + occ) - 1, (double)n1) + 1;
+    } else {
+        fr = rc + 0.5;
+        fc = cc + 0.5;
+    }
+    out[2 * k] = fr;
+    out[2 * k + 1] = fc;
+}
+
+// vortices of the structure factor: [x, y, charge] rows (x from the column,
+// y from the row), W = charge + i |charge| for the transform, and the
+// minimum-image nearest-neighbour distance of each vortex
+// (compute_vortex_structure_factor.m:37-75)
+__global__ void k_vort_sf_points(const signed char *q, const int *list, int nv, int n0,
+                                 double dx, double dy, double *vort) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    const int s = list[k];
+    const int iy = s % n0 + 1, ix = s / n0 + 1;
+    vort[3 * k] = (ix - 0.5) * dx;
+    vort[3 * k + 1] = (iy - 0.5) * dy;
+    vort[3 * k + 2] = (double)q[s];
+}
+__global__ void k_vort_weights(const signed char *q, long long n, double2 *W) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const double v = (double)q[s];
+        W[s] = make_double2(v, fabs(v));
+    }
+}
+__global__ void k_vort_nnd(const double *vort, int nv, double Lx, double Ly, double *nnd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const double xi = vort[3 * i], yi = vort[3 * i + 1];
+    double best = INFINITY;
+    for (int j = 0; j < nv; ++j) {
+        if (j == i) continue;
+        double ddx = fabs(vort[3 * j] - xi), ddy = fabs(vort[3 * j + 1] - yi);
+        ddx = fmin(ddx, Lx - ddx);
+        ddy = fmin(ddy, Ly - ddy);
+        best = fmin(best, __dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)));
+    }
+    nnd[i] = sqrt(best);
+}
+
+// shell sums of S_c, S_n = |fft2(W_c)|^2/Nv, |fft2(W_n)|^2/Nv and cell
+// counts from the spectrum Z of W = W_c + i W_n (both real): W_c^ =
+// (Z(k) + conj Z(-k))/2, W_n^ = (Z(k) - conj Z(-k))/(2i).  Row index i0 <-> ky,
+// column i1 <-> kx; bin b with b dk <= |k| < (b+1) dk (edges as products).
+__global__ void k_vort_sf_bins(const double2 *Z, int n0, int n1, const double *ky,
+                               const double *kx, double dk, int nbins, double inv_nv,
+                               double *bins) {
+    const long long n = (long long)n0 * n1;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        const int i0 = (int)(s % n0), i1 = (int)(s / n0);
+        const double a = kx[i1], b = ky[i0];
+        const double K = sqrt(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+        long long bb = (long long)floor(K / dk);
+        if (K < (double)bb * dk) --bb;
+        if (K >= (double)(bb + 1) * dk) ++bb;
+        if (bb < 0 || bb >= nbins) continue;
+        const int m0 = (n0 - i0) % n0, m1 = (n1 - i1) % n1;
+        const double2 c = Z[s], p = Z[m0 + (long long)m1 * n0];
+        const double cr = 0.5 * (c.x + p.x), ci = 0.5 * (c.y - p.y);
+        const double nr = 0.5 * (c.y + p.y), ni = -0.5 * (c.x - p.x);
+        atomicAdd(&bins[bb], (cr * cr + ci * ci) * inv_nv);
+        atomicAdd(&bins[nbins + bb], (nr * nr + ni * ni) * inv_nv);
+        atomicAdd(&bins[2 * nbins + bb], 1.0);
     }
 }
 

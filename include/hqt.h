@@ -152,6 +152,43 @@ int hqt_energy_spectrum_device(hqt_ctx *ctx, const void *dO, int32_t capacity,
                                double *k, double *E, double *Ec, double *Ei,
                                int32_t *nbins);
 
+/* Boundary velocity observables of a device field O (interleaved complex
+ * [nx,ny]) into real device arrays vx, vy [nx,ny]:
+ *   v = |O|./max(|O|) .* real(-1i*(d O - d|O| .* O./|O|)./O)
+ * with spectral d = d/dx, d/dy and max over x per y column (MATLAB's max of a
+ * matrix).  Replaces VX_temp, VY_temp of scripts/analysis/plots_cluster.m:92-93
+ * (same as movie_show.m:93-94). */
+int hqt_boundary_velocity_device(hqt_ctx *ctx, const void *dO, void *dvx,
+                                 void *dvy);
+
+/* find_vortices(O, threshold, radius) (src/diagnostics/find_vortices.m:1-28)
+ * of a device field O (interleaved complex [nx,ny]): plaquette charges
+ * (find_vortices_old, :80-118), then the centroid of the periodic
+ * (2*radius+1)^2 window cells with |O|^2/max|O|^2 < threshold (:30-78).
+ * Writes *n vortices and as many antivortices as [row, col] pairs in 1-based
+ * matrix-index units (row-major n x 2).  Like the reference, it assumes equal
+ * counts: extra antivortices are dropped and fewer are an error
+ * (HQT_EINVAL).  capacity < *n is HQT_EINVAL with *n set. */
+int hqt_find_vortices_device(hqt_ctx *ctx, const void *dO, double threshold,
+                             int32_t radius, int32_t capacity,
+                             double *vortices, double *antivortices,
+                             int32_t *n);
+
+/* compute_vortex_structure_factor(Phi, Lx, Ly)
+ * (src/diagnostics/compute_vortex_structure_factor.m:1-104) of a device field
+ * Phi stored as this context's [nx,ny] array and read as the routine's
+ * [Ny,Nx] matrix (Ny = nx rows, Nx = ny columns), as plots_cluster.m:318
+ * calls it with O1(:,:,1).  Writes *nv vortices as [x, y, charge] rows
+ * (row-major nv x 3, MATLAB find order), *nbins shells k_bin, S_c, S_n and
+ * spacing[5] = rho, d_density, d_nnd, k_density, k_nnd.  No vortices: *nv =
+ * *nbins = 0 (the routine's warning and empty outputs). */
+int hqt_vortex_structure_factor_device(hqt_ctx *ctx, const void *dPhi,
+                                       double Lx, double Ly, int32_t capacity,
+                                       double *vortices, int32_t *nv,
+                                       int32_t bins_capacity, double *k_bin,
+                                       double *Sc, double *Sn, int32_t *nbins,
+                                       double *spacing);
+
 /* Allocation-free vortex count (no counterpart in the reference).
  * countN of the boundary order parameter O = (Lz Z1)(nz) of a DEVICE field
  * dZ1 (interleaved complex [nx,ny,nz]), computed on `cuda_stream` (NULL: the

@@ -412,25 +412,17 @@ def signed_wavenumbers(n: int) -> np.ndarray:
     return np.r_[np.arange(0, h + 1), np.arange(-h, 0)].astype(np.float64)
 
 
-def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
-    """Incompressible/compressible kinetic-energy spectrum of the boundary flow.
-
-    Restates ``scripts/analysis/movie_show.m``: the density-weighted velocity
-    ``u = |O|/max|O| * Re(-i(dO - d|O| O/|O|)/O)`` (:93-94, with spectral
-    derivatives), the mean removed (:140-141), ``E2d = |u^|^2/2`` (:142-145),
-    shell sums ``sum(E2d(K >= kbins(i) & K < kbins(i+1)))`` over
-    ``kbins = 0:dk:kmax``, ``dk = 2*pi/L0``, ``kmax = floor(max K)`` (:146-160),
-    and the Helmholtz split ``u_c = grad Phi``, ``lap Phi = div u`` (:217-233)
-    done in Fourier space as ``u_c^ = k (k.u^)/|k|^2``.  Returns
-    ``(kplot, E, E_c, E_i)``.
-    """
+def boundary_velocity(O: np.ndarray, Lx: float, Ly: float):
+    """``(vx, vy)``: ``VX_temp``, ``VY_temp`` of
+    ``scripts/analysis/plots_cluster.m:92-93`` (= ``movie_show.m:93-94``),
+    ``|O|./max(|O|) .* real(-1i*(func_Lx(O) - func_Lx(|O|).*O./|O|)./O)`` on
+    the boundary slice, with spectral derivatives (``fourdif``: ``ik``,
+    Nyquist 0).  ``max`` of the nx x ny slice is MATLAB's column max: one
+    maximum over x per y index."""
     O = np.asarray(O, dtype=np.complex128)
     nx, ny = O.shape
-    kx = (2.0 * np.pi / Lx) * signed_wavenumbers(nx)
-    ky = (2.0 * np.pi / Ly) * signed_wavenumbers(ny)
-    # spectral derivatives (func_Lx / func_Ly on the boundary slice)
-    ikx = 1j * kx
-    iky = 1j * ky
+    ikx = 1j * (2.0 * np.pi / Lx) * signed_wavenumbers(nx)
+    iky = 1j * (2.0 * np.pi / Ly) * signed_wavenumbers(ny)
     if nx % 2 == 0:
         ikx[nx // 2] = 0
     if ny % 2 == 0:
@@ -442,9 +434,39 @@ def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
     ahat = np.fft.fft2(a)
     dax = np.real(np.fft.ifft2(ikx[:, None] * ahat))
     day = np.real(np.fft.ifft2(iky[None, :] * ahat))
-    w = a / np.max(a)
-    ux = w * np.real(-1j * (dOx - dax * O / a) / O)
-    uy = w * np.real(-1j * (dOy - day * O / a) / O)
+    w = a / np.max(a, axis=0, keepdims=True)
+    vx = w * np.real(-1j * (dOx - dax * O / a) / O)
+    vy = w * np.real(-1j * (dOy - day * O / a) / O)
+    return vx, vy
+
+
+def boundary_fields(op: Operators, Z1: np.ndarray):
+    """One frame of ``scripts/analysis/plots_cluster.m:89-97``:
+    ``(O, vx, vy, NofV)`` with ``O = func_Lz(Z1)(:,:,nz)`` and ``NofV`` the
+    first output of ``countN``."""
+    O = boundary_order_parameter(op, Z1)
+    vx, vy = boundary_velocity(O, op.Lx_len, op.Ly_len)
+    n, _, _ = countN(O)
+    return O, vx, vy, n
+
+
+def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
+    """Incompressible/compressible kinetic-energy spectrum of the boundary flow.
+
+    Restates ``scripts/analysis/movie_show.m``: the density-weighted velocity
+    ``u = |O|/max|O| * Re(-i(dO - d|O| O/|O|)/O)`` (:93-94, with spectral
+    derivatives; ``max`` of the slice is per y column, MATLAB's column max), the mean removed (:140-141), ``E2d = |u^|^2/2`` (:142-145),
+    shell sums ``sum(E2d(K >= kbins(i) & K < kbins(i+1)))`` over
+    ``kbins = 0:dk:kmax``, ``dk = 2*pi/L0``, ``kmax = floor(max K)`` (:146-160),
+    and the Helmholtz split ``u_c = grad Phi``, ``lap Phi = div u`` (:217-233)
+    done in Fourier space as ``u_c^ = k (k.u^)/|k|^2``.  Returns
+    ``(kplot, E, E_c, E_i)``.
+    """
+    O = np.asarray(O, dtype=np.complex128)
+    nx, ny = O.shape
+    kx = (2.0 * np.pi / Lx) * signed_wavenumbers(nx)
+    ky = (2.0 * np.pi / Ly) * signed_wavenumbers(ny)
+    ux, uy = boundary_velocity(O, Lx, Ly)
     ux = ux - np.mean(ux)
     uy = uy - np.mean(uy)
     uxh = np.fft.fft2(ux)
@@ -470,3 +492,149 @@ def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
     Ei = np.bincount(idx[sel], weights=E2i[sel], minlength=nbins)[:nbins]
     kplot = (np.arange(nbins) + 0.5) * dk
     return kplot, E, Ec, Ei
+
+
+# ---------------------------------------------------------------------------
+# Vortex positions and structure factors
+# ---------------------------------------------------------------------------
+def _find_colmajor(mask: np.ndarray):
+    """MATLAB ``[r, c] = find(mask)``: 1-based indices in column-major order."""
+    r, c = np.nonzero(mask.T)          # rows of mask.T are the columns of mask
+    return c + 1, r + 1
+
+
+def find_vortices_coarse(O: np.ndarray):
+    """``find_vortices_old`` (``src/diagnostics/find_vortices.m:80-118``):
+    plaquette charges ``round((d1+d2+d3+d4)/(2*pi))`` with
+    ``d = angle(p_next .* conj(p))`` around p1=(i,j), p2=(i+1,j),
+    p3=(i+1,j+1), p4=(i,j+1) (periodic); returns 1-based ``[row, col]``
+    arrays of the +1 and -1 plaquettes in ``find`` order and the charges."""
+    O = np.asarray(O, dtype=np.complex128)
+    p1 = O
+    p2 = np.roll(O, -1, axis=0)
+    p3 = np.roll(np.roll(O, -1, axis=0), -1, axis=1)
+    p4 = np.roll(O, -1, axis=1)
+    W = (np.angle(p2 * np.conj(p1)) + np.angle(p3 * np.conj(p2))
+         + np.angle(p4 * np.conj(p3)) + np.angle(p1 * np.conj(p4)))
+    charge = matlab_round(W / (2.0 * np.pi))
+    vr, vc = _find_colmajor(charge == 1)
+    ar, ac = _find_colmajor(charge == -1)
+    return (np.stack([vr, vc], axis=1).astype(np.float64),
+            np.stack([ar, ac], axis=1).astype(np.float64), charge)
+
+
+def refine_vortex(pos, density: np.ndarray, threshold: float, radius: int):
+    """``refine_positions`` (``find_vortices.m:30-78``): centroid of the
+    periodic (2r+1)^2 window cells with density below the threshold, in
+    1-based matrix-index units; ``pos + 0.5`` when no cell qualifies."""
+    nx, ny = density.shape
+    r_c, c_c = int(pos[0]), int(pos[1])
+    off = np.arange(-radius, radius + 1)
+    rows = np.mod(r_c + off - 1, nx)
+    cols = np.mod(c_c + off - 1, ny)
+    local = density[np.ix_(rows, cols)]
+    mask = local < threshold
+    s = int(mask.sum())
+    if s == 0:
+        return np.array([r_c + 0.5, c_c + 0.5])
+    dR, dC = off[:, None] * np.ones((1, off.size)), np.ones((off.size, 1)) * off[None, :]
+    orr = float(np.sum(dR * mask)) / s
+    occ = float(np.sum(dC * mask)) / s
+    return np.array([np.mod(r_c + orr - 1, nx) + 1, np.mod(c_c + occ - 1, ny) + 1])
+
+
+def find_vortices(O: np.ndarray, threshold: float, radius: int):
+    """``find_vortices`` (``src/diagnostics/find_vortices.m:1-28``): coarse
+    plaquettes refined on ``density = |O|^2 / max(|O|^2,[],'all')``.  The k-th
+    vortex and the k-th antivortex are refined for k = 1..#vortices (the
+    routine assumes equal counts: extra antivortices are dropped, fewer
+    raise, as MATLAB's indexing would)."""
+    v, av, _ = find_vortices_coarse(O)
+    if len(v) == 0:
+        return np.zeros((0, 2)), np.zeros((0, 2))
+    if len(av) < len(v):
+        raise IndexError("fewer antivortices than vortices")
+    a2 = np.abs(np.asarray(O)) ** 2
+    density = a2 / np.max(a2)
+    sv = np.array([refine_vortex(p, density, threshold, radius) for p in v])
+    sa = np.array([refine_vortex(p, density, threshold, radius) for p in av[:len(v)]])
+    return sv, sa
+
+
+def shell_index(K: np.ndarray, dk: float) -> np.ndarray:
+    """Bin b with ``b*dk <= K < (b+1)*dk`` (edges as products, so a value
+    on an edge lands in the upper bin whatever the division rounds to)."""
+    b = np.floor(K / dk)
+    b = np.where(K < b * dk, b - 1, b)
+    b = np.where(K >= (b + 1) * dk, b + 1, b)
+    return b.astype(np.int64)
+
+
+def vortex_structure_factor(Phi: np.ndarray, Lx: float, Ly: float):
+    """``compute_vortex_structure_factor``
+    (``src/diagnostics/compute_vortex_structure_factor.m:1-104``).
+
+    ``Phi`` is ``[Ny, Nx]`` (rows = y).  Charges
+    ``round(sum(mod(dtheta + pi, 2 pi) - pi)/(2 pi))`` around theta ->
+    theta_x (next column) -> theta_xy -> theta_y (next row); positions
+    ``((ix-0.5) dx, (iy-0.5) dy)`` in ``find`` order; spacing from the density
+    and the mean minimum-image nearest-neighbour distance;
+    ``S = |fft2(W)|^2 / Nv`` for W = charge and |charge|, averaged over shells
+    ``k_edges = 0:dk:k_max`` (``dk = min(dkx, dky)``,
+    ``k_max = min(max|kx|, max|ky|)``).  Returns
+    ``(k_bin, Sc, Sn, vortices, spacing)``; ``spacing`` is a dict with
+    rho, d_density, d_nnd, k_density, k_nnd.  No vortices: all empty/None.
+    """
+    Phi = np.asarray(Phi, dtype=np.complex128)
+    Ny, Nx = Phi.shape
+    dx, dy = Lx / Nx, Ly / Ny
+    th = np.angle(Phi)
+    tx = np.roll(th, -1, axis=1)
+    ty = np.roll(th, -1, axis=0)
+    txy = np.roll(np.roll(th, -1, axis=0), -1, axis=1)
+    tp = 2.0 * np.pi
+    d1 = np.mod(tx - th + np.pi, tp) - np.pi
+    d2 = np.mod(txy - tx + np.pi, tp) - np.pi
+    d3 = np.mod(ty - txy + np.pi, tp) - np.pi
+    d4 = np.mod(th - ty + np.pi, tp) - np.pi
+    charge = matlab_round((d1 + d2 + d3 + d4) / tp)
+    iy, ix = _find_colmajor(np.abs(charge) > 0.5)
+    q = charge[iy - 1, ix - 1]
+    Nv = len(q)
+    if Nv == 0:
+        return np.zeros(0), np.zeros(0), np.zeros(0), np.zeros((0, 3)), None
+    xv, yv = (ix - 0.5) * dx, (iy - 0.5) * dy
+    vort = np.stack([xv, yv, q], axis=1)
+    rho = Nv / (Lx * Ly)
+    d_density = 1.0 / np.sqrt(rho)
+    ddx = np.abs(xv[:, None] - xv[None, :])
+    ddx = np.minimum(ddx, Lx - ddx)
+    ddy = np.abs(yv[:, None] - yv[None, :])
+    ddy = np.minimum(ddy, Ly - ddy)
+    d2m = ddx ** 2 + ddy ** 2
+    np.fill_diagonal(d2m, np.inf)
+    nnd = np.sqrt(np.min(d2m, axis=1))
+    d_nnd = float(np.mean(nnd))
+    spacing = {"rho": rho, "d_density": d_density, "d_nnd": d_nnd,
+               "k_density": 2 * np.pi / d_density, "k_nnd": 2 * np.pi / d_nnd}
+    Sc2 = np.abs(np.fft.fft2(charge)) ** 2 / Nv
+    Sn2 = np.abs(np.fft.fft2(np.abs(charge))) ** 2 / Nv
+    dkx, dky = 2 * np.pi / Lx, 2 * np.pi / Ly
+    # unshifted FFT index -> signed frequency of (-floor(N/2) : ceil(N/2)-1)
+    kx = dkx * signed_wavenumbers(Nx)
+    ky = dky * signed_wavenumbers(Ny)
+    KX, KY = np.meshgrid(kx, ky)                     # [Ny, Nx], like Phi
+    K = np.sqrt(KX * KX + KY * KY)                   # hypot(KX, KY)
+    dk = min(dkx, dky)
+    kmax = min(np.floor(Nx / 2) * dkx, np.floor(Ny / 2) * dky)
+    nb = int(np.floor(kmax / dk + 1e-9))             # len(0:dk:k_max) - 1
+    b = shell_index(K, dk)
+    sel = (b >= 0) & (b < nb)
+    cnt = np.bincount(b[sel], minlength=nb)[:nb]
+    sc = np.bincount(b[sel], weights=Sc2[sel], minlength=nb)[:nb]
+    sn = np.bincount(b[sel], weights=Sn2[sel], minlength=nb)[:nb]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        Sc = np.where(cnt > 0, sc / np.maximum(cnt, 1), 0.0)
+        Sn = np.where(cnt > 0, sn / np.maximum(cnt, 1), 0.0)
+    k_bin = (np.arange(nb) + 0.5) * dk
+    return k_bin, Sc, Sn, vort, spacing

@@ -102,3 +102,50 @@ def test_energy_spectrum_helmholtz_split(oracle):
 def test_signed_wavenumbers(oracle):
     assert list(oracle.signed_wavenumbers(4)) == [0, 1, -2, -1]
     assert list(oracle.signed_wavenumbers(5)) == [0, 1, 2, -2, -1]
+
+
+def _smoke_phi():
+    # tests/hqt_smoke_test.m:148: [x, y] = ndgrid((0:32)*2*pi/33, ...)
+    g = np.arange(33) * 2 * np.pi / 33
+    x, y = np.meshgrid(g, g, indexing="ij")
+    return np.sin(x + 0.271) + 1j * np.sin(y + 0.613)
+
+
+def test_find_vortices_smoke_pins(oracle):
+    # tests/hqt_smoke_test.m:154-157: two refined vortices and antivortices on
+    # phi; none on a uniform field
+    phi = _smoke_phi()
+    pos, neg = oracle.find_vortices(phi, 0.4, 2)
+    assert pos.shape == (2, 2) and neg.shape == (2, 2)
+    n, npos, nneg = oracle.countN(phi)
+    assert (npos, nneg) == (len(pos), len(neg))
+    pos, neg = oracle.find_vortices(np.ones((9, 9)), 0.4, 2)
+    assert pos.size == 0 and neg.size == 0
+    # refined positions stay within the window of the coarse plaquette
+    v, av, q = oracle.find_vortices_coarse(phi)
+    pos, neg = oracle.find_vortices(phi, 0.4, 2)
+    assert np.all(np.abs(pos - v) <= 2.5) and np.all(np.abs(neg - av[:2]) <= 2.5)
+    assert int(np.sum(q == 1)) == npos and int(np.sum(q == -1)) == nneg
+
+
+def test_structure_factor_smoke_pins(oracle):
+    # tests/hqt_smoke_test.m:158-159: equal bin counts, one row per vortex of
+    # countN, finite nearest-neighbour spacing
+    phi = _smoke_phi()
+    k, Sc, Sn, vort, spacing = oracle.vortex_structure_factor(phi.T, 2 * np.pi, 2 * np.pi)
+    assert len(k) == len(Sc) == len(Sn) > 0
+    n, _, _ = oracle.countN(phi)
+    assert vort.shape == (n, 3) and np.isfinite(spacing["d_nnd"])
+    assert sorted(vort[:, 2]) == [-1, -1, 1, 1]
+    # the k = 0 cell of S_n is Nv^2/Nv = Nv and sits in the first shell
+    assert np.all(Sc >= 0) and np.all(Sn >= 0)
+    none = oracle.vortex_structure_factor(np.ones((8, 8), complex), 1.0, 1.0)
+    assert none[0].size == 0 and none[3].shape == (0, 3) and none[4] is None
+
+
+def test_shell_index_edges(oracle):
+    dk = 0.1
+    K = np.array([0.0, 0.1, 0.3, 0.29999999999999993, 0.7, 1.05])
+    b = oracle.shell_index(K, dk)
+    for Ki, bi in zip(K, b):
+        assert bi * dk <= Ki < (bi + 1) * dk
