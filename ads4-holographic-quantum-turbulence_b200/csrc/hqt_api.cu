@@ -90,6 +90,10 @@ struct hqt_ctx {
     int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
     bool cx = false, cy = false;  // compile-time line transforms along x / y
     bool px = false, py = false;  // prime-factor tensor-core transforms along x / y
+    // mixed precision with the filter on the prime-factor engine: the filter
+    // passes leave the slice means and the FP32 stage-1 copies of the state,
+    // so a step starts without the separate conversion
+    bool fused_convert = false;
     int smem_optin = 0;
     // state arrays the step acts on (internal buffers, or the caller's
     // device arrays for hqt_step_device)
@@ -475,8 +479,13 @@ int launch_d1_32(hqt_ctx *c, bool along_x, const float *in, float *out) {
 }
 
 // Filter nf (<= 3) complex fields in place through the x-spectra buffers.
+// f32: fields (Psi, A_t + i d_z A_t, A_x + i A_y); the y pass writes their
+// slice means and the x inverse the FP32 stage-1 copies (fused_convert)
+constexpr int kMeanSlot[3][2] = {{0, 1}, {2, -1}, {3, 4}};
 int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<double> *out,
-                  bool phase, bool check) {
+                  bool phase, bool check, bool f32 = false) {
+    if (f32 && (nf != 3 || !c->px || !c->py))
+        return fail(c, HQT_EUNSUPPORTED, "fused FP32 copies need the prime-factor engine");
     double2 *spec[3] = {c->dxpsi, c->dypsi, c->E};
     {
         XFiltFwdArgs<double> a{};
@@ -519,6 +528,11 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.scale = 1.0 / ((double)c->nx * (double)c->ny);
         a.dead0 = c->dead0;
         a.dead1 = c->dead1;
+        if (f32) {
+            a.slice_mean = c->slice_mean;
+            for (int f = 0; f < 3; ++f)
+                for (int k = 0; k < 2; ++k) a.slot[f][k] = kMeanSlot[f][k];
+        }
         dim3 grid((c->nx + a.TX - 1) / a.TX, c->nz);
         Prof pr(c, K_FILT_Y);
         if (c->py) {
@@ -545,6 +559,16 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         a.st = check ? c->st : nullptr;
         a.dead0 = c->dead0;
         a.dead1 = c->dead1;
+        if (f32) {
+            a.slice_mean = c->slice_mean;
+            a.ny = c->ny;
+            for (int f = 0; f < 3; ++f)
+                for (int k = 0; k < 2; ++k) a.slot[f][k] = kMeanSlot[f][k];
+            a.c32[0] = c->ypsi32[2];
+            a.re32[1] = c->at32;
+            a.re32[2] = c->yax32[2];
+            a.im32[2] = c->yay32[2];
+        }
         const int grid = (a.nlines + a.NB - 1) / a.NB;
         Prof pr(c, K_FILT_X_INV);
         if (c->px) {
@@ -653,22 +677,27 @@ int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
 // copies of the stage input; the column kernels contract in FP64 on the FP64
 // stage input (D_z^2 would amplify FP32 storage error by ~|Lz^2|) and keep
 // the state and RK accumulators in FP64.
+// slice means of the state and its FP32 stage-1 copies (mixed precision)
+int enqueue_convert(hqt_ctx *c) {
+    Prof pr(c, K_CONVERT, 3);
+    k_slice_partials<<<dim3(kSliceChunks, c->nz), kRedThreads, 0, c->stream>>>(
+        c->cpsi, c->cat, c->cax, c->cay, c->plane, c->slice_partial);
+    CK(cudaGetLastError());
+    k_slice_finalize<<<(5 * c->nz + 127) / 128, 128, 0, c->stream>>>(
+        c->slice_partial, c->nz, c->plane, c->slice_mean);
+    CK(cudaGetLastError());
+    k_state_to_f32<<<592, 256, 0, c->stream>>>(c->cpsi, c->cat, c->cax, c->cay, c->plane,
+                                              c->vol, c->slice_mean, c->ypsi32[2], c->at32,
+                                              c->yax32[2], c->yay32[2]);
+    CK(cudaGetLastError());
+    return HQT_OK;
+}
+
 int enqueue_stages_mixed(hqt_ctx *c) {
     double2 *psi = c->cpsi;
     double *at = c->cat, *ax = c->cax, *ay = c->cay;
-    {
-        Prof pr(c, K_CONVERT, 3);
-        k_slice_partials<<<dim3(kSliceChunks, c->nz), kRedThreads, 0, c->stream>>>(
-            psi, at, ax, ay, c->plane, c->slice_partial);
-        CK(cudaGetLastError());
-        k_slice_finalize<<<(5 * c->nz + 127) / 128, 128, 0, c->stream>>>(
-            c->slice_partial, c->nz, c->plane, c->slice_mean);
-        CK(cudaGetLastError());
-        k_state_to_f32<<<592, 256, 0, c->stream>>>(psi, at, ax, ay, c->plane, c->vol,
-                                                  c->slice_mean, c->ypsi32[2], c->at32,
-                                                  c->yax32[2], c->yay32[2]);
-        CK(cudaGetLastError());
-    }
+    // with fused_convert the previous step's filter (or prestep) left them
+    if (!c->fused_convert) RC(enqueue_convert(c));
     RC(launch_d1_32(c, true, c->at32, c->dxat32));
     RC(launch_d1_32(c, false, c->at32, c->dyat32));
     for (int s = 1; s <= 4; ++s) {
@@ -790,7 +819,7 @@ int enqueue_step(hqt_ctx *c) {
     if (c->p.apply_filter) {
         FieldIn<double> in[3] = {{psi, nullptr, nullptr}, {nullptr, at, c->dat}, {nullptr, ax, ay}};
         FieldOut<double> out[3] = {{psi, nullptr, nullptr}, {nullptr, at, c->dat}, {nullptr, ax, ay}};
-        RC(launch_filter(c, 3, in, out, c->p.remove_winding != 0, true));
+        RC(launch_filter(c, 3, in, out, c->p.remove_winding != 0, true, c->fused_convert));
     } else if (c->p.remove_winding) {
         Prof pr(c, K_PHASE);
         k_phase_multiply<<<592, 256, 0, c->stream>>>(psi, c->nx, c->ny, c->vol, c->st);
@@ -836,7 +865,7 @@ int build_graph(hqt_ctx *c) {
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed ? 3 : 0);
+    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed && !c->fused_convert ? 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -862,6 +891,15 @@ int count_vortices_dev(hqt_ctx *c, const double2 *O, int32_t *n, int32_t *np, in
 }
 
 // Advance the current state nsteps steps.
+// Work on the incoming state before the first step of a call: d_z A_t and,
+// with fused_convert, the FP32 stage-1 copies (later steps get both from the
+// previous step's constraint and filter).
+int prestep(hqt_ctx *c) {
+    RC(launch_zcol_misc(c, c->cat, c->dat, nullptr, nullptr));
+    if (c->fused_convert) RC(enqueue_convert(c));
+    return HQT_OK;
+}
+
 int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
     DevStatus h0{};
     CK(cudaMemcpyAsync(&h0, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
@@ -870,8 +908,7 @@ int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
     h0.first_bad_step = LLONG_MAX;
     h0.winding = 0;
     CK(cudaMemcpyAsync(c->st, &h0, sizeof(DevStatus), cudaMemcpyHostToDevice, c->stream));
-    // d_z A_t of the incoming potential
-    RC(launch_zcol_misc(c, c->cat, c->dat, nullptr, nullptr));
+    RC(prestep(c));
     if (!c->prof_on) RC(build_graph(c));
     if (diag) {
         diag->n_records = 0;
@@ -1410,6 +1447,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         if (std::string(env) == "runtime" || std::string(env) == "stockham")
             c->px = c->py = false;
     }
+    c->fused_convert = c->mixed && p.apply_filter && c->px && c->py;
     {
         const size_t lim = 227 * 1024 - 1024;
         const size_t need = std::max({smem_x(p.nx, 3, c->NBx_rhs), smem_x(p.ny, 4, c->TXy_rhs),
@@ -1890,7 +1928,7 @@ int hqt_ensemble_step_device(hqt_ensemble *e, void *const *dZ1, void *const *dZ2
                                                          c->plane, c->rho);
                 CK(cudaGetLastError());
             }
-            RC(launch_zcol_misc(c, c->cat, c->dat, nullptr, nullptr));
+            RC(prestep(c));
             RC(build_graph(c));
             CK(cudaStreamSynchronize(c->stream));
             return HQT_OK;

@@ -83,6 +83,11 @@ template <typename T> struct YFiltArgs {
     const T *mx, *my;  // 1 - fx, 1 - fy
     T scale;           // 1/(nx*ny)
     int dead0 = 1, dead1 = 0;  // columns dead0 <= kx <= dead1 are zero after the weight
+    // optional: the weighted (0,0) coefficient of field f's real and imaginary
+    // parts, i.e. the slice means of the filtered field, go to
+    // slice_mean[5*z + slot[f][c]] (slot < 0: not written)
+    T *slice_mean = nullptr;
+    int slot[kMaxFilt][2] = {};
 };
 
 template <typename T> struct XFiltInvArgs {
@@ -93,6 +98,14 @@ template <typename T> struct XFiltInvArgs {
     const C2<T> *spec[kMaxFilt];
     FieldOut<T> out[kMaxFilt];
     DevStatus *st;  // non-finite check when non-null
+    // optional FP32 copies minus the slice means (slice_mean[5*z + slot]):
+    // interleaved c32[f], or re32[f] / im32[f]; z = line / ny
+    const T *slice_mean = nullptr;
+    int slot[kMaxFilt][2] = {};
+    int ny = 0;
+    C2<float> *c32[kMaxFilt] = {};
+    float *re32[kMaxFilt] = {};
+    float *im32[kMaxFilt] = {};
     int dead0 = 1, dead1 = 0;  // spectral columns dead0 <= kx <= dead1 read as zero
 };
 

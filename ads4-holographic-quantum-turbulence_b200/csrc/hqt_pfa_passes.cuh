@@ -524,6 +524,26 @@ __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFilt
     cp_commit();
     cp_wait<0>();
     __syncwarp();
+    if (a.slice_mean && x0 == 0) {
+        // slice means of the field: the (0,0) coefficient (weight 1) is the
+        // sum over y of the kx = 0 column times 1/(nx*ny)
+        double sr = 0.0, si = 0.0;
+        for (int n = L.lane; n < N; n += 32) {
+            sr += L.b0.re[L_t::pos(0, n)];
+            si += L.b0.im[L_t::pos(0, n)];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if (L.lane == 0) {
+            double *m = a.slice_mean + 5 * blockIdx.y;
+            const int f = blockIdx.z;
+            if (a.slot[f][0] >= 0) m[a.slot[f][0]] = sr * a.scale;
+            if (a.slot[f][1] >= 0) m[a.slot[f][1]] = si * a.scale;
+        }
+    }
     w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
     __syncwarp();
     w.template stage_b<true, true>(L.b0, L.b1, cs,
@@ -577,11 +597,41 @@ __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ X
         __syncwarp();
         w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
         __syncwarp();
-        L.each([&](int ln, int n, int i) {
-            const double re = L.b1.re[i], im = L.b1.im[i];
-            if (!(isfinite(re) && isfinite(im))) bad = true;
-            pfa_store_field(a.out[f], gi(ln, n), re, im);
-        });
+        const bool f32 = a.slice_mean && (a.c32[f] || a.re32[f] || a.im32[f]);
+        if (!f32) {
+            L.each([&](int ln, int n, int i) {
+                const double re = L.b1.re[i], im = L.b1.im[i];
+                if (!(isfinite(re) && isfinite(im))) bad = true;
+                pfa_store_field(a.out[f], gi(ln, n), re, im);
+            });
+        } else {
+            // the lines' slice means, once per field (lines of a warp may lie
+            // in two slices)
+            static_assert(kPfaLines == 2, "two lines per warp");
+            double mr[kPfaLines], mi[kPfaLines];
+#pragma unroll
+            for (int ln = 0; ln < kPfaLines; ++ln) {
+                const double *m = a.slice_mean + 5 * ((L0 + min(ln, L.valid - 1)) / a.ny);
+                mr[ln] = a.slot[f][0] >= 0 ? m[a.slot[f][0]] : 0.0;
+                mi[ln] = a.slot[f][1] >= 0 ? m[a.slot[f][1]] : 0.0;
+            }
+            C2<float> *c32 = a.c32[f];
+            float *re32 = a.re32[f], *im32 = a.im32[f];
+            L.each([&](int ln, int n, int i) {
+                const double re = L.b1.re[i], im = L.b1.im[i];
+                if (!(isfinite(re) && isfinite(im))) bad = true;
+                const long long g = gi(ln, n);
+                pfa_store_field(a.out[f], g, re, im);
+                const double m0 = ln == 0 ? mr[0] : mr[kPfaLines - 1];
+                const double m1 = ln == 0 ? mi[0] : mi[kPfaLines - 1];
+                if (c32) {
+                    c32[g] = make_float2((float)(re - m0), (float)(im - m1));
+                } else {
+                    if (re32) re32[g] = (float)(re - m0);
+                    if (im32) im32[g] = (float)(im - m1);
+                }
+            });
+        }
         __syncwarp();
     }
     if (a.st && __any_sync(0xffffffffu, bad) && L.lane == 0)
