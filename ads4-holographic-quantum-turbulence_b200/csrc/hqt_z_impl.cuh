@@ -124,7 +124,7 @@ cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, int, int,
                                                       smem);
         if (per_sm < 1) per_sm = 1;
     }
-    const long long tiles = (a.plane + kZTile - 1) / kZTile;
+    const long long tiles = (a.plane + kZConsSites - 1) / kZConsSites;
     const long long full = (long long)per_sm * (nsm > 0 ? nsm : 1);
     const ZOps<double, HQT_ZN> op = make_zops(h);
     k_zcons_tc<HQT_ZN><<<(int)(tiles < full ? tiles : full), kZThreads, smem, s>>>(a, op);

@@ -455,13 +455,18 @@ __global__ void __launch_bounds__(kZThreads, 3)
 }
 
 // Constraint, A_t rebuild, boundary rows and O after the RK combine
-// (scripts/simulation/tevol_driven_cluster.m:129-136) on the same block
-// tiles and FP64 tensor-core products as k_zstage:
+// (scripts/simulation/tevol_driven_cluster.m:129-136) on the same tiles and
+// FP64 tensor-core products as k_zstage:
 //   cons = Lz(div A) - 2 Im(conj(Psi) Lz Psi),  v = Lzr(cons) - rhoi,
 //   A_t = Lzr(v) + mu (A_t(nz) = mu),  d_z A_t = Lz A_t,
 //   Psi(nz) = A_x(nz) = 0, A_y(nz) = -vy,  O = Lz(nz,:) Psi (Psi(nz) = 0).
-// Real fields use the x parts of pair tiles (y parts stay zero).
-constexpr int kZConsTiles = 4;  // pair tiles: Psi, div A, two scratch
+// A block takes 32 sites, a warp 8: sites 8w+j and 8w+j+4 (j = 0..3) share
+// pair column 4w+j.  Psi needs two pair tiles (PA: sites 8w+j, PB: 8w+4+j);
+// the real fields (div A, cons, v, A_t) pack both sites into one pair tile
+// (x: site 8w+j, y: site 8w+4+j), so the real chain costs one product per 8
+// sites.  Lane (g, q) owns sites 8w+q and 8w+4+q at levels 8m+g.
+constexpr int kZConsTiles = 5;  // pair tiles: PA, PB, div A, two scratch
+constexpr int kZConsSites = 2 * kZTile;
 template <int NZP>
 __host__ __device__ constexpr int zcons_smem_bytes() {
     return kZConsTiles * ZmDims<NZP>::LV * kZTile * 16;
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(kZThreads)
     using D = ZmDims<NZP>;
     constexpr int MT = D::MT, KS = D::KS, L = D::LV * kZTile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
-    const int cw = kZCols * warp;
+    const int cw = kZCols * warp;  // pair column base of this warp
     const int nz = a.nz;
     const long long P = a.plane;
     double2 *sm = reinterpret_cast<double2 *>(g_smem);
@@ -493,43 +498,54 @@ __global__ void __launch_bounds__(kZThreads)
         }
     }
     __syncthreads();
-    const ZTileF<double2> PS{sm}, DV{sm + L}, V1{sm + 2 * L}, V2{sm + 3 * L};
-    const auto PSw = PS.cols(cw), DVw = DV.cols(cw), V1w = V1.cols(cw), V2w = V2.cols(cw);
-    const long long ntiles = (P + kZTile - 1) / kZTile;
+    const ZTileF<double2> PA{sm}, PB{sm + L}, DV{sm + 2 * L}, V1{sm + 3 * L}, V2{sm + 4 * L};
+    const auto PAw = PA.cols(cw), PBw = PB.cols(cw), DVw = DV.cols(cw), V1w = V1.cols(cw),
+               V2w = V2.cols(cw);
+    const long long ntiles = (P + kZConsSites - 1) / kZConsSites;
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long site0 = tile * kZTile, site = site0 + cw + q;
-        const bool ok = site < P;
-        zf_real<NZP, double2>(PS, a.psi, nz, P, site0, tid);
+        const long long site0 = tile * kZConsSites;
+        // site c of the tile -> pair column 4(c/8) + c%4, half (c/4)%2
 #pragma unroll
-        for (int it = 0; it < (NZP * kZTile + kZThreads - 1) / kZThreads; ++it) {
-            const int e = tid + kZThreads * it, l = e / kZTile, c = e % kZTile;
-            if (l < nz && site0 + c < P) cp_async<8>(&DV(l, c).x, a.divA + l * P + site0 + c);
+        for (int it = 0; it < (NZP * kZConsSites + kZThreads - 1) / kZThreads; ++it) {
+            const int e = tid + kZThreads * it, l = e / kZConsSites, c = e % kZConsSites;
+            const int pc = 4 * (c >> 3) + (c & 3), h = (c >> 2) & 1;
+            if (l < nz && site0 + c < P) {
+                const long long gi = l * P + site0 + c;
+                cp_async<16>(h ? &PB(l, pc) : &PA(l, pc), a.psi + gi);
+                cp_async<8>(h ? &DV(l, pc).y : &DV(l, pc).x, a.divA + gi);
+            }
         }
         cp_commit();
         cp_wait<0>();
         __syncthreads();
+        const long long sA = site0 + 8 * warp + q, sB = sA + 4;  // this lane's two sites
+        const bool okA = sA < P, okB = sB < P;
         {  // cons (levels < nz-1 enter Lzr)
-            double c1[MT][2], c2[MT][2];
-            zm_pair<MT, KS>(ALz, PSw, c1, lane);
+            double cA[MT][2], cB[MT][2], c2[MT][2];
+            zm_pair<MT, KS>(ALz, PAw, cA, lane);
+            zm_pair<MT, KS>(ALz, PBw, cB, lane);
             zm_pair<MT, KS>(ALz, DVw, c2, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
-                const int i = 8 * m + g;
-                const double2 ps = PS(i < nz ? i : 0, cw + q);
-                const double cons = c2[m][0] - 2.0 * (ps.x * c1[m][1] - ps.y * c1[m][0]);
-                V1(i, cw + q) = make_double2(i < nz - 1 ? cons : 0.0, 0.0);
+                const int i = 8 * m + g, ic = i < nz ? i : 0;
+                const double2 pa = PA(ic, cw + q), pb = PB(ic, cw + q);
+                const double xA = c2[m][0] - 2.0 * (pa.x * cA[m][1] - pa.y * cA[m][0]);
+                const double xB = c2[m][1] - 2.0 * (pb.x * cB[m][1] - pb.y * cB[m][0]);
+                const bool in = i < nz - 1;
+                V1(i, cw + q) = make_double2(in ? xA : 0.0, in ? xB : 0.0);
             }
         }
         __syncwarp();
-        const double rho = ok ? a.rho[site] : 0.0;
+        const double rA = okA ? a.rho[sA] : 0.0, rB = okB ? a.rho[sB] : 0.0;
         {  // v = Lzr(cons) - rhoi
             double v[MT][2];
             zm_pair<MT, KS>(ALz1, V1w, v, lane);
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
-                V2(i, cw + q) = make_double2(i < nz - 1 ? v[m][0] - rho : 0.0, 0.0);
+                const bool in = i < nz - 1;
+                V2(i, cw + q) = make_double2(in ? v[m][0] - rA : 0.0, in ? v[m][1] - rB : 0.0);
             }
         }
         __syncwarp();
@@ -539,9 +555,13 @@ __global__ void __launch_bounds__(kZThreads)
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
-                const double at = i < nz - 1 ? t[m][0] + a.mu : (i == nz - 1 ? a.mu : 0.0);
-                V1(i, cw + q) = make_double2(at, 0.0);
-                if (i < nz && ok) a.at[(long long)i * P + site] = at;
+                const double atA = i < nz - 1 ? t[m][0] + a.mu : (i == nz - 1 ? a.mu : 0.0);
+                const double atB = i < nz - 1 ? t[m][1] + a.mu : (i == nz - 1 ? a.mu : 0.0);
+                V1(i, cw + q) = make_double2(atA, atB);
+                if (i < nz) {
+                    if (okA) a.at[(long long)i * P + sA] = atA;
+                    if (okB) a.at[(long long)i * P + sB] = atB;
+                }
             }
         }
         __syncwarp();
@@ -551,26 +571,42 @@ __global__ void __launch_bounds__(kZThreads)
 #pragma unroll
             for (int m = 0; m < MT; ++m) {
                 const int i = 8 * m + g;
-                if (i < nz && ok) a.dat[(long long)i * P + site] = d[m][0];
+                if (i < nz) {
+                    if (okA) a.dat[(long long)i * P + sA] = d[m][0];
+                    if (okB) a.dat[(long long)i * P + sB] = d[m][1];
+                }
             }
         }
         // O = (Lz Psi)(nz) with Psi(nz) = 0 (:136), then the boundary rows (:133)
-        double orr = 0.0, oi = 0.0;
+        double oar = 0.0, oai = 0.0, obr = 0.0, obi = 0.0;
 #pragma unroll
         for (int m = 0; m < MT; ++m) {
-            const int i = 8 * m + g;
-            const double2 ps = PS(i < nz - 1 ? i : 0, cw + q);
-            orr = fma(i < nz - 1 ? lzr[m] : 0.0, ps.x, orr);
-            oi = fma(i < nz - 1 ? lzr[m] : 0.0, ps.y, oi);
+            const int i = 8 * m + g, ic = i < nz - 1 ? i : 0;
+            const double w = i < nz - 1 ? lzr[m] : 0.0;
+            const double2 pa = PA(ic, cw + q), pb = PB(ic, cw + q);
+            oar = fma(w, pa.x, oar);
+            oai = fma(w, pa.y, oai);
+            obr = fma(w, pb.x, obr);
+            obi = fma(w, pb.y, obi);
         }
-        orr = zf_colsum(orr);
-        oi = zf_colsum(oi);
-        if (g == 0 && ok) {
-            if (a.O) a.O[site] = make_double2(orr, oi);
-            const long long gb = (long long)(nz - 1) * P + site;
-            a.psi[gb] = make_double2(0.0, 0.0);
-            a.ax[gb] = 0.0;
-            a.ay[gb] = -a.vy;
+        oar = zf_colsum(oar);
+        oai = zf_colsum(oai);
+        obr = zf_colsum(obr);
+        obi = zf_colsum(obi);
+        if (g == 0) {
+            const long long gb = (long long)(nz - 1) * P;
+            if (okA) {
+                if (a.O) a.O[sA] = make_double2(oar, oai);
+                a.psi[gb + sA] = make_double2(0.0, 0.0);
+                a.ax[gb + sA] = 0.0;
+                a.ay[gb + sA] = -a.vy;
+            }
+            if (okB) {
+                if (a.O) a.O[sB] = make_double2(obr, obi);
+                a.psi[gb + sB] = make_double2(0.0, 0.0);
+                a.ax[gb + sB] = 0.0;
+                a.ay[gb + sB] = -a.vy;
+            }
         }
         __syncthreads();  // every warp is done with the tiles: the next tile refills them
     }
