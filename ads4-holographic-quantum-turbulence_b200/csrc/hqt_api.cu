@@ -628,12 +628,11 @@ int launch_zcons(hqt_ctx *c) {
     a.divA = c->divA;
     a.rho = c->rho;
     a.O = c->O;
-    const int grid = (int)((c->plane + kThreadsZ - 1) / kThreadsZ);
     Prof pr(c, K_ZCONS);
     switch (c->NZP) {
-#define HQT_Z(N)                                              \
-    case N:                                                   \
-        CK(z_cons<N>(a, zhost(c), grid, kThreadsZ, c->stream)); \
+#define HQT_Z(N)                                   \
+    case N:                                        \
+        CK(z_cons<N>(a, zhost(c), c->stream));     \
         return HQT_OK;
         HQT_NZP_LIST(HQT_Z)
 #undef HQT_Z

@@ -59,8 +59,7 @@ template <int N>
 cudaError_t z_stage_mixed(int mode, const ZStageArgs<double, double, float> &a, const ZHost &h,
                           int grid, int threads, size_t smem, cudaStream_t s);
 template <int N>
-cudaError_t z_cons(const ZConsArgs<double> &a, const ZHost &h, int grid, int threads,
-                   cudaStream_t s);
+cudaError_t z_cons(const ZConsArgs<double> &a, const ZHost &h, cudaStream_t s);
 template <int N>
 cudaError_t z_misc(const ZColArgs<double> &a, const ZHost &h, int grid, int threads,
                    cudaStream_t s);
@@ -82,7 +81,7 @@ namespace hqt {
     cudaError_t z_stage_mixed<N>(int, const ZStageArgs<double, double, float> &,            \
                                  const ZHost &, int, int, size_t, cudaStream_t);           \
     template <>                                                                            \
-    cudaError_t z_cons<N>(const ZConsArgs<double> &, const ZHost &, int, int, cudaStream_t); \
+    cudaError_t z_cons<N>(const ZConsArgs<double> &, const ZHost &, cudaStream_t);             \
     template <>                                                                            \
     cudaError_t z_misc<N>(const ZColArgs<double> &, const ZHost &, int, int, cudaStream_t);
 HQT_NZP_LIST(HQT_ZDECL)

@@ -112,8 +112,7 @@ cudaError_t z_stage_mixed<HQT_ZN>(int mode, const ZStageArgs<double, double, flo
 }
 
 template <>
-cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, int, int,
-                           cudaStream_t s) {
+cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, cudaStream_t s) {
     static int per_sm = 0, nsm = 0;
     constexpr size_t smem = zcons_smem_bytes<HQT_ZN>();
     if (per_sm == 0) {
