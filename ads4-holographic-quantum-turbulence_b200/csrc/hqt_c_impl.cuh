@@ -116,6 +116,11 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
     auto ygrid = [&](int nx, int nz_) {
         return dim3((nx + kPfaLines - 1) / kPfaLines, nz_);
     };
+    // real-field first derivatives: kPfaRealLines real lines per warp
+    const int rgrid = (nlines + kPfaRealLines - 1) / kPfaRealLines;
+    auto yrgrid = [&](int nx, int nz_) {
+        return dim3((nx + kPfaRealLines - 1) / kPfaRealLines, nz_);
+    };
     switch (kind) {
         case CT_X_RHS:
             k_x_rhs_pfa<double, P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
@@ -125,12 +130,20 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
             k_y_rhs_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
             break;
         }
-        case CT_X_D1:
-            k_x_d1_pfa<double, P, Q><<<grid, 32, smem, s>>>(*(const XD1Args<double> *)args);
+        case CT_X_D1: {
+            const XD1Args<double> &a = *(const XD1Args<double> *)args;
+            if (pfa_real_d1(a.in, a.out))
+                k_x_d1r_pfa<double, P, Q><<<rgrid, 32, smem, s>>>(a);
+            else
+                k_x_d1_pfa<double, P, Q><<<grid, 32, smem, s>>>(a);
             break;
+        }
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
-            k_y_d1_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
+            if (pfa_real_d1(a.in, a.out))
+                k_y_d1r_pfa<double, P, Q><<<yrgrid(a.nx, nlines), 32, smem, s>>>(a);
+            else
+                k_y_d1_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
             break;
         }
         case CT_X_RHS_F:
@@ -141,12 +154,20 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
             k_y_rhs_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
             break;
         }
-        case CT_X_D1_F:
-            k_x_d1_pfa<float, P, Q><<<grid, 32, smem32, s>>>(*(const XD1Args<float> *)args);
+        case CT_X_D1_F: {
+            const XD1Args<float> &a = *(const XD1Args<float> *)args;
+            if (pfa_real_d1(a.in, a.out))
+                k_x_d1r_pfa<float, P, Q><<<rgrid, 32, smem32, s>>>(a);
+            else
+                k_x_d1_pfa<float, P, Q><<<grid, 32, smem32, s>>>(a);
             break;
+        }
         case CT_Y_D1_F: {
             const YD1Args<float> &a = *(const YD1Args<float> *)args;
-            k_y_d1_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
+            if (pfa_real_d1(a.in, a.out))
+                k_y_d1r_pfa<float, P, Q><<<yrgrid(a.nx, nlines), 32, smem32, s>>>(a);
+            else
+                k_y_d1_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
             break;
         }
         case CT_FX_FWD:

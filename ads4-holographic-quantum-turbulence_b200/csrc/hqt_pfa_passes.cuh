@@ -447,6 +447,97 @@ __global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args
     });
 }
 
+// First x / y derivative of a REAL field with two real lines per complex
+// line: the derivative multiplier is a real operator, so one transform of
+// A + iB gives dA + i dB.  A warp takes 2*kPfaLines real lines; complex line
+// ln carries real lines 2ln (real part) and 2ln+1 (imaginary part).
+template <typename T>
+__host__ __device__ inline bool pfa_real_d1(const FieldIn<T> &in, const FieldOut<T> &out) {
+    return in.re && !in.im && !in.c && out.re && !out.im && !out.c;
+}
+constexpr int kPfaRealLines = 2 * kPfaLines;
+
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_x_d1r_pfa(const __grid_constant__ XD1Args<T> a) {
+    constexpr int N = P * Q;
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
+    const int R0 = blockIdx.x * kPfaRealLines;
+    const int nr = min(kPfaRealLines, a.nlines - R0);  // real lines inside the grid
+    const L_t L((nr + 1) / 2);
+    const T *src = a.in.re + (long long)R0 * N;
+    T *dst = a.out.re + (long long)R0 * N;
+    for (int e = L.lane; e < L_t::LN; e += 32) {
+        const int ln = e % kPfaLines, n = e / kPfaLines, i = L_t::pos(ln, n);
+        const int r0 = 2 * ln, r1 = r0 + 1;
+        if (r0 < nr) cp_async<sizeof(T)>(L.b0.re + i, src + (long long)r0 * N + n);
+        else L.b0.re[i] = T(0);
+        if (r1 < nr) cp_async<sizeof(T)>(L.b0.im + i, src + (long long)r1 * N + n);
+        else L.b0.im[i] = T(0);
+    }
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, T(0), cs);
+    __syncwarp();
+    w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    for (int e = L.lane; e < L_t::LN; e += 32) {
+        const int ln = e % kPfaLines, n = e / kPfaLines, i = L_t::pos(ln, n);
+        const int r0 = 2 * ln, r1 = r0 + 1;
+        if (r0 < nr) dst[(long long)r0 * N + n] = L.b1.re[i];
+        if (r1 < nr) dst[(long long)r1 * N + n] = L.b1.im[i];
+    }
+}
+
+template <typename T, int P, int Q>
+__global__ void __launch_bounds__(32) k_y_d1r_pfa(const __grid_constant__ YD1Args<T> a) {
+    using L_t = PfaLines<T, P, Q>;
+    PfaWarp<T, P, Q> w;
+    w.init(pfa_frag<T>());
+    T cs[2][P];
+    pfa_twiddles<T, P>(cs);
+    const int x0 = blockIdx.x * kPfaRealLines;
+    const int nr = min(kPfaRealLines, a.nx - x0);  // columns inside the grid
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    const L_t L((nr + 1) / 2);
+    auto gi = [&](int r, int n) { return zoff + (long long)n * a.nx + r; };
+    for (int e = L.lane; e < L_t::LN; e += 32) {
+        const int ln = e % kPfaLines, n = e / kPfaLines, i = L_t::pos(ln, n);
+        const int r0 = 2 * ln, r1 = r0 + 1;
+        if (r0 < nr) cp_async<sizeof(T)>(L.b0.re + i, a.in.re + gi(r0, n));
+        else L.b0.re[i] = T(0);
+        if (r1 < nr) cp_async<sizeof(T)>(L.b0.im + i, a.in.re + gi(r1, n));
+        else L.b0.im[i] = T(0);
+    }
+    cp_commit();
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    __syncwarp();
+    w.template stage_b_deriv<1>(L.b0, L.b1, a.s1, T(0), cs);
+    __syncwarp();
+    w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    for (int e = L.lane; e < L_t::LN; e += 32) {
+        const int ln = e % kPfaLines, n = e / kPfaLines, i = L_t::pos(ln, n);
+        const int r0 = 2 * ln, r1 = r0 + 1;
+        if (r0 < nr) {
+            const long long g = gi(r0, n);
+            a.out.re[g] = L.b1.re[i] + (a.add_re ? a.add_re[g] : T(0));
+        }
+        if (r1 < nr) {
+            const long long g = gi(r1, n);
+            a.out.re[g] = L.b1.im[i] + (a.add_re ? a.add_re[g] : T(0));
+        }
+    }
+}
+
 // Filter, x forward: spectra along x of nf fields (field 0 times the winding
 // phase exp(-2 pi i y w / ny) when a status is given), natural order k.
 template <int P, int Q>
