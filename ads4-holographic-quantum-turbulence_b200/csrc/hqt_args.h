@@ -18,6 +18,14 @@ template <typename T> struct FieldOut {
     T *im;
 };
 
+// A first derivative of one real field into one real field: the line
+// passes then carry two real lines per complex transform (the multiplier
+// ik is a real operator, so a transform of A + iB gives dA + i dB).
+template <typename T>
+__host__ __device__ inline bool real_field_d1(const FieldIn<T> &in, const FieldOut<T> &out) {
+    return in.re && !in.im && !in.c && out.re && !out.im && !out.c;
+}
+
 template <typename T> struct XRhsArgs {
     FFTPlan plan;
     const C2<T> *roots;

@@ -58,6 +58,10 @@ cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const 
     opt((const void *)k_y_rhs_c<float, HQT_CN>);
     opt((const void *)k_x_d1_c<float, HQT_CN>);
     opt((const void *)k_y_d1_c<float, HQT_CN>);
+    opt((const void *)k_x_d1r_c<double, HQT_CN>);
+    opt((const void *)k_y_d1r_c<double, HQT_CN>);
+    opt((const void *)k_x_d1r_c<float, HQT_CN>);
+    opt((const void *)k_y_d1r_c<float, HQT_CN>);
     return e;
 }
 
@@ -72,12 +76,26 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
         case CT_Y_RHS:
             k_y_rhs_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<double> *)args);
             break;
-        case CT_X_D1:
-            k_x_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const XD1Args<double> *)args);
+        case CT_X_D1: {
+            const XD1Args<double> &a = *(const XD1Args<double> *)args;
+            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(double2));
+            if (real_field_d1(a.in, a.out))
+                k_x_d1r_c<double, HQT_CN>
+                    <<<(a.nlines + nb2 - 1) / nb2, T, smem, s>>>(a);
+            else
+                k_x_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(a);
             break;
-        case CT_Y_D1:
-            k_y_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YD1Args<double> *)args);
+        }
+        case CT_Y_D1: {
+            const YD1Args<double> &a = *(const YD1Args<double> *)args;
+            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(double2));
+            if (real_field_d1(a.in, a.out))
+                k_y_d1r_c<double, HQT_CN>
+                    <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);
+            else
+                k_y_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(a);
             break;
+        }
         case CT_FX_FWD:
             k_x_filt_fwd_c<double, HQT_CN>
                 <<<grid, T, smem, s>>>(*(const XFiltFwdArgs<double> *)args);
@@ -95,12 +113,25 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
         case CT_Y_RHS_F:
             k_y_rhs_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<float> *)args);
             break;
-        case CT_X_D1_F:
-            k_x_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const XD1Args<float> *)args);
+        case CT_X_D1_F: {
+            const XD1Args<float> &a = *(const XD1Args<float> *)args;
+            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(float2));
+            if (real_field_d1(a.in, a.out))
+                k_x_d1r_c<float, HQT_CN><<<(a.nlines + nb2 - 1) / nb2, T, smem, s>>>(a);
+            else
+                k_x_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(a);
             break;
-        case CT_Y_D1_F:
-            k_y_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const YD1Args<float> *)args);
+        }
+        case CT_Y_D1_F: {
+            const YD1Args<float> &a = *(const YD1Args<float> *)args;
+            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(float2));
+            if (real_field_d1(a.in, a.out))
+                k_y_d1r_c<float, HQT_CN>
+                    <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);
+            else
+                k_y_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(a);
             break;
+        }
         default:
             return cudaErrorInvalidValue;
     }
@@ -132,7 +163,7 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
         }
         case CT_X_D1: {
             const XD1Args<double> &a = *(const XD1Args<double> *)args;
-            if (pfa_real_d1(a.in, a.out))
+            if (real_field_d1(a.in, a.out))
                 k_x_d1r_pfa<double, P, Q><<<rgrid, 32, smem, s>>>(a);
             else
                 k_x_d1_pfa<double, P, Q><<<grid, 32, smem, s>>>(a);
@@ -140,7 +171,7 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
         }
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
-            if (pfa_real_d1(a.in, a.out))
+            if (real_field_d1(a.in, a.out))
                 k_y_d1r_pfa<double, P, Q><<<yrgrid(a.nx, nlines), 32, smem, s>>>(a);
             else
                 k_y_d1_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
@@ -156,7 +187,7 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
         }
         case CT_X_D1_F: {
             const XD1Args<float> &a = *(const XD1Args<float> *)args;
-            if (pfa_real_d1(a.in, a.out))
+            if (real_field_d1(a.in, a.out))
                 k_x_d1r_pfa<float, P, Q><<<rgrid, 32, smem32, s>>>(a);
             else
                 k_x_d1_pfa<float, P, Q><<<grid, 32, smem32, s>>>(a);
@@ -164,7 +195,7 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
         }
         case CT_Y_D1_F: {
             const YD1Args<float> &a = *(const YD1Args<float> *)args;
-            if (pfa_real_d1(a.in, a.out))
+            if (real_field_d1(a.in, a.out))
                 k_y_d1r_pfa<float, P, Q><<<yrgrid(a.nx, nlines), 32, smem32, s>>>(a);
             else
                 k_y_d1_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);

@@ -201,6 +201,71 @@ __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
     });
 }
 
+// First x / y derivative of a real field into a real field, two real lines
+// per complex line (real_field_d1): block b takes 2*NB real lines, complex
+// line j carrying real lines 2j (real part) and 2j+1 (imaginary part).
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_x_d1r_c(XD1Args<T> a) {
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
+    const int L0 = blockIdx.x * 2 * NB;
+    const int nr = min(2 * NB, a.nlines - L0);
+    const int valid = (nr + 1) / 2;
+    constexpr int R = 0, A = N, B = N + NB * N;
+    const T *src = a.in.re + (long long)L0 * N;
+    T *dst = a.out.re + (long long)L0 * N;
+    load_roots<T>(R, a.roots, N);
+    cx_load<T, N, NB>(A, valid, [&](int t) {
+        const int j = t / N, e = t - j * N;
+        const int r0 = 2 * j, r1 = r0 + 1;
+        return mk2<T>(r0 < nr ? src[(long long)r0 * N + e] : T(0),
+                      r1 < nr ? src[(long long)r1 * N + e] : T(0));
+    });
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
+    __syncthreads();
+    const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    cx_store<T, N, NB>(r, valid, [&](int t, C2<T> v) {
+        const int j = t / N, e = t - j * N;
+        const int r0 = 2 * j, r1 = r0 + 1;
+        if (r0 < nr) dst[(long long)r0 * N + e] = v.x;
+        if (r1 < nr) dst[(long long)r1 * N + e] = v.y;
+    });
+}
+
+template <typename T, int N>
+__global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
+    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
+    const int x0 = blockIdx.x * 2 * NB;
+    const int nr = min(2 * NB, a.nx - x0);
+    const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
+    constexpr int R = 0, A = N, B = N + NB * N;
+    load_roots<T>(R, a.roots, N);
+    {  // the layout of cy_load: element (y, j) at y*NB + j
+        C2<T> *sa = sptr<T>(A);
+        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+            const int y = t / NB, j = t - y * NB;
+            const int r0 = 2 * j, r1 = r0 + 1;
+            const long long gy = zoff + (long long)y * a.nx;
+            sa[t] = mk2<T>(r0 < nr ? a.in.re[gy + r0] : T(0), r1 < nr ? a.in.re[gy + r1] : T(0));
+        }
+    }
+    __syncthreads();
+    const int X = ct_fft<T, N, NB, -1>(A, B, R);
+    ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
+    __syncthreads();
+    const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    const C2<T> *sr = sptr<T>(r);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int y = t / NB, j = t - y * NB;
+        const int r0 = 2 * j, r1 = r0 + 1;
+        const long long gy = zoff + (long long)y * a.nx;
+        const C2<T> v = sr[t];
+        if (r0 < nr) a.out.re[gy + r0] = v.x + (a.add_re ? a.add_re[gy + r0] : T(0));
+        if (r1 < nr) a.out.re[gy + r1] = v.y + (a.add_re ? a.add_re[gy + r1] : T(0));
+    }
+}
+
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
     constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));

@@ -448,13 +448,9 @@ __global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args
 }
 
 // First x / y derivative of a REAL field with two real lines per complex
-// line: the derivative multiplier is a real operator, so one transform of
-// A + iB gives dA + i dB.  A warp takes 2*kPfaLines real lines; complex line
+// line (real_field_d1): the derivative multiplier is a real operator, so one
+// transform of A + iB gives dA + i dB.  A warp takes 2*kPfaLines real lines; complex line
 // ln carries real lines 2ln (real part) and 2ln+1 (imaginary part).
-template <typename T>
-__host__ __device__ inline bool pfa_real_d1(const FieldIn<T> &in, const FieldOut<T> &out) {
-    return in.re && !in.im && !in.c && out.re && !out.im && !out.c;
-}
 constexpr int kPfaRealLines = 2 * kPfaLines;
 
 template <typename T, int P, int Q>
