@@ -26,10 +26,9 @@ __all__ = ["checkpoint_name", "save_checkpoint", "load_checkpoint", "num2str",
 
 
 def checkpoint_name(t: float) -> str:
-    """``['check_point_t=',num2str(t),'.mat']`` -- num2str keeps up to four
-    decimals and drops trailing zeros."""
-    s = f"{t:.4f}".rstrip("0").rstrip(".")
-    return f"check_point_t={s}.mat"
+    """``['check_point_t=',num2str(t),'.mat']``
+    (``scripts/simulation/tevol_driven_cluster.m:179``)."""
+    return f"check_point_t={num2str(t)}.mat"
 
 
 def save_checkpoint(path, Z1, Z2, Z3, Z4, rhoi, params: dict | None = None):
@@ -57,11 +56,12 @@ def load_checkpoint(path):
 
 def num2str(x: float) -> str:
     """MATLAB ``num2str`` of a real scalar: integers in full, otherwise
-    ``%.<floor(log10|x|)+5>g`` (four digits after the leading one)."""
+    ``%.<d>g`` with ``d = max(floor(log10|x|) + 5, 5)`` significant digits
+    (at most 16): four digits after the leading one, and at least five."""
     x = float(x)
     if np.isfinite(x) and x == np.round(x):
         return str(int(np.round(x)))
-    digits = max(int(np.floor(np.log10(abs(x)))) + 5, 1)
+    digits = min(max(int(np.floor(np.log10(abs(x)))) + 5, 5), 16)
     return f"{x:.{digits}g}"
 
 

@@ -839,32 +839,59 @@ void drop_graph(hqt_ctx *c) {
     c->graph = nullptr;
 }
 
-int build_graph(hqt_ctx *c) {
-    const void *key[4] = {c->cpsi, c->cat, c->cax, c->cay};
-    if (c->gexec && std::memcmp(key, c->graph_key, sizeof(key)) == 0) return HQT_OK;
-    drop_graph(c);
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+// Append one guarded step of c to `parent`: a one-thread kernel sets the
+// condition of an IF node from the status word, and the IF body, the step's
+// launch sequence captured on c's stream, runs only while no step so far has
+// produced a non-finite value.  Later launches of a run that went bad leave
+// the fields as the bad step left them.
+int add_guarded_step(hqt_ctx *c, cudaGraph_t parent) {
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, parent, 0, 0));
+    const DevStatus *stp = c->st;
+    void *kargs[2] = {&h, &stp};
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void *>(k_step_guard);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = kargs;
+    cudaGraphNode_t guard, cond;
+    CK(cudaGraphAddKernelNode(&guard, parent, nullptr, 0, &kp));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    CK(cudaGraphAddNode(&cond, parent, &guard, 1, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
     c->capturing = true;
     const long long l0 = c->launches;
     const int r = enqueue_step(c);
     c->launches = l0;
     c->capturing = false;
-    cudaGraph_t g = nullptr;
+    cudaGraph_t g = body;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    if (r != HQT_OK) {
-        if (g) cudaGraphDestroy(g);
-        return r;
-    }
+    if (r != HQT_OK) return r;
     if (e != cudaSuccess) return fail(c, HQT_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    c->graph = g;
-    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    return HQT_OK;
+}
+
+int build_graph(hqt_ctx *c) {
+    const void *key[4] = {c->cpsi, c->cat, c->cax, c->cay};
+    if (c->gexec && std::memcmp(key, c->graph_key, sizeof(key)) == 0) return HQT_OK;
+    drop_graph(c);
+    CK(cudaGraphCreate(&c->graph, 0));
+    RC(add_guarded_step(c, c->graph));
+    CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
     std::memcpy(c->graph_key, key, sizeof(key));
     return HQT_OK;
 }
 
 // kernels one captured step launches (counted by a dry count of enqueue_step)
 long long launches_per_step(hqt_ctx *c) {
-    long long n = 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed && !c->fused_convert ? 3 : 0);
+    // guard, 2 d1 passes of A_t, 4 x (x, y, z), 2 d1 passes of A, zcons, step end
+    long long n = 1 + 2 + 4 * 3 + 2 + 1 + 1 + (c->mixed && !c->fused_convert ? 3 : 0);
     if (c->p.remove_winding) n += 2;
     if (c->p.apply_filter)
         n += 3;
@@ -938,7 +965,10 @@ int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
             r[3] = nm;
             diag->n_records++;
         }
-        if ((done % 64) == 0 || done == nsteps) {
+        // graph steps after a non-finite one are no-ops (the guard), so the
+        // status is polled only every 64 steps; eager (profiled) steps have
+        // no guard and are polled after each step
+        if ((done % 64) == 0 || done == nsteps || c->prof_on) {
             DevStatus h{};
             CK(cudaMemcpyAsync(&h, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
@@ -953,7 +983,8 @@ int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
     CK(cudaMemcpyAsync(&h, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (diag) {
-        diag->steps_done = done;
+        // steps that ran: the guard skipped every launch after a bad step
+        diag->steps_done = h.step - step0;
         diag->last_winding = h.winding;
     }
     if (bad) return fail(c, HQT_ENONFINITE, "non-finite value in the evolved fields");
@@ -1555,6 +1586,11 @@ static bool aligned_fields(const void *z1, const void *z2, const void *z3, const
            (reinterpret_cast<uintptr_t>(z4) % 8 == 0);
 }
 
+static bool al16(const void *p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; }
+static bool al8(const void *p) { return reinterpret_cast<uintptr_t>(p) % 8 == 0; }
+static const char *const kAlignMsg =
+    "device arrays must be aligned to their element size (16 bytes complex, 8 real)";
+
 int hqt_step_device(hqt_ctx *c, void *dZ1, void *dZ2, void *dZ3, void *dZ4, void *drhoi,
                     int64_t nsteps, hqt_diag *diag) {
     if (!c) return HQT_EINVAL;
@@ -1678,6 +1714,7 @@ int hqt_rhs_device(hqt_ctx *c, const void *dZ1, const void *dZ2, const void *dZ3
 int hqt_filter_device(hqt_ctx *c, const void *din, void *dout, int32_t nfields) {
     if (!c) return HQT_EINVAL;
     if (!din || !dout || nfields < 0) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al8(din) || !al8(dout)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     const double *in = (const double *)din;
     double *out = (double *)dout;
@@ -1703,6 +1740,7 @@ int hqt_filter_device(hqt_ctx *c, const void *din, void *dout, int32_t nfields) 
 int hqt_boundary_order_parameter_device(hqt_ctx *c, const void *dZ1, void *dO) {
     if (!c) return HQT_EINVAL;
     if (!dZ1 || !dO) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dZ1) || !al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     RC(launch_zcol_misc(c, nullptr, nullptr, (const double2 *)dZ1, (double2 *)dO));
     CK(cudaStreamSynchronize(c->stream));
@@ -1712,6 +1750,7 @@ int hqt_boundary_order_parameter_device(hqt_ctx *c, const void *dZ1, void *dO) {
 int hqt_winding_device(hqt_ctx *c, const void *dO, int32_t *winding) {
     if (!c) return HQT_EINVAL;
     if (!dO || !winding) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     RC(launch_winding(c, (const double2 *)dO, c->d_int + 4));
     int w = 0;
@@ -1724,6 +1763,7 @@ int hqt_winding_device(hqt_ctx *c, const void *dO, int32_t *winding) {
 int hqt_count_vortices_device(hqt_ctx *c, const void *dO, int32_t *n, int32_t *np, int32_t *nm) {
     if (!c) return HQT_EINVAL;
     if (!dO) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     return count_vortices_dev(c, (const double2 *)dO, n, np, nm);
 }
@@ -1732,6 +1772,7 @@ int hqt_energy_spectrum_device(hqt_ctx *c, const void *dO, int32_t capacity, dou
                                double *E, double *Ec, double *Ei, int32_t *nbins) {
     if (!c) return HQT_EINVAL;
     if (!dO || !nbins || capacity < 0) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     return energy_spectrum(c, (const double2 *)dO, capacity, k, E, Ec, Ei, nbins);
 }
@@ -1739,6 +1780,7 @@ int hqt_energy_spectrum_device(hqt_ctx *c, const void *dO, int32_t capacity, dou
 int hqt_boundary_velocity_device(hqt_ctx *c, const void *dO, void *dvx, void *dvy) {
     if (!c) return HQT_EINVAL;
     if (!dO || !dvx || !dvy) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dO) || !al8(dvx) || !al8(dvy)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     RC(boundary_velocity(c, (const double2 *)dO, nullptr, (double *)dvx, (double *)dvy));
     CK(cudaStreamSynchronize(c->stream));
@@ -1751,6 +1793,7 @@ int hqt_find_vortices_device(hqt_ctx *c, const void *dO, double threshold, int32
     if (!c) return HQT_EINVAL;
     if (!dO || !n || radius < 0 || capacity < 0 || (capacity > 0 && (!vortices || !antivortices)))
         return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     return find_vortices_dev(c, (const double2 *)dO, threshold, radius, capacity, vortices,
                              antivortices, n);
@@ -1764,6 +1807,7 @@ int hqt_vortex_structure_factor_device(hqt_ctx *c, const void *dPhi, double Lx, 
     if (!dPhi || !nv || !nbins || capacity < 0 || bins_capacity < 0 || !(Lx > 0) ||
         !(Ly > 0) || (capacity > 0 && !vortices))
         return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dPhi)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     return structure_factor_dev(c, (const double2 *)dPhi, Lx, Ly, capacity, vortices, nv,
                                 bins_capacity, k_bin, Sc, Sn, nbins, spacing);
@@ -1780,10 +1824,12 @@ int hqt_count_vortices(hqt_ctx *c, const double *O, int32_t *n, int32_t *np, int
 
 // ---------------------------------------------------------------- ensembles
 // Independent runs (each its own context: grid, nz, mu, seed, precision)
-// advanced together.  Each member's step is its captured step graph; the
-// ensemble graph holds one child-graph node per member with no edges between
-// them, so a single cudaGraphLaunch advances every member one step and the
-// members' kernels overlap on the device.
+// advanced together.  The ensemble graph holds one guarded step per member
+// (guard kernel + IF node whose body is the member's captured step) with no
+// edges between members, so a single cudaGraphLaunch advances every member
+// one step, the members' kernels overlap on the device, and a member that
+// went non-finite stops at its bad step while the others go on until the
+// next status poll.
 
 }  // extern "C"
 
@@ -1794,7 +1840,8 @@ struct hqt_ensemble {
     cudaStream_t own = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    std::vector<cudaGraph_t> key;  // member graphs the ensemble graph holds copies of
+    // state pointers of every member, as captured into the ensemble graph
+    std::vector<const void *> key;
     std::string err;
 };
 
@@ -1826,14 +1873,17 @@ void drop_ensemble_graph(hqt_ensemble *e) {
 }
 
 int build_ensemble_graph(hqt_ensemble *e) {
-    std::vector<cudaGraph_t> key;
-    for (hqt_ctx *c : e->m) key.push_back(c->graph);
+    // the graph bakes in each member's state pointers (and its internal
+    // buffers, fixed for the member's life): rebuild when any pointer changes
+    std::vector<const void *> key;
+    for (hqt_ctx *c : e->m) key.insert(key.end(), {c->cpsi, c->cat, c->cax, c->cay});
     if (e->gexec && key == e->key) return HQT_OK;
     drop_ensemble_graph(e);
     EK(cudaGraphCreate(&e->graph, 0));
-    for (hqt_ctx *c : e->m) {
-        cudaGraphNode_t node;
-        EK(cudaGraphAddChildGraphNode(&node, e->graph, nullptr, 0, c->graph));
+    for (size_t i = 0; i < e->m.size(); ++i) {
+        hqt_ctx *c = e->m[i];
+        const int r = add_guarded_step(c, e->graph);
+        if (r != HQT_OK) return efail(e, r, "member " + std::to_string(i) + ": " + c->err);
     }
     EK(cudaGraphInstantiate(&e->gexec, e->graph, 0));
     e->key = key;
@@ -1928,7 +1978,6 @@ int hqt_ensemble_step_device(hqt_ensemble *e, void *const *dZ1, void *const *dZ2
                 CK(cudaGetLastError());
             }
             RC(prestep(c));
-            RC(build_graph(c));
             CK(cudaStreamSynchronize(c->stream));
             return HQT_OK;
         };
@@ -1975,7 +2024,7 @@ int hqt_ensemble_step_device(hqt_ensemble *e, void *const *dZ1, void *const *dZ2
     EK(cudaStreamSynchronize(e->stream));
     if (diags)
         for (size_t i = 0; i < n; ++i) {
-            diags[i].steps_done = done;
+            diags[i].steps_done = hs[i].step - step0[i];
             diags[i].last_winding = hs[i].winding;
         }
     if (bad) return efail(e, HQT_ENONFINITE, "non-finite value in the fields of a member");

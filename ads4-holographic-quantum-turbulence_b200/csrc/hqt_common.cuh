@@ -76,6 +76,38 @@ __host__ __device__ constexpr int ct_lines(int N, int nbuf, int esize = 16) {
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
 
+#ifdef __CUDACC__
+// angle(a./b) as atan2 of a*conj(b) (same argument; |b|^2 > 0 only rescales),
+// with every product and sum rounded on its own so that all count paths give
+// the same bits.
+__device__ __forceinline__ double quot_angle(double2 a, double2 b) {
+    const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+    const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
+    return atan2(im, re);
+}
+
+// countN classification of the plaquette at linear index s of the periodic
+// [nx, ny] field O (src/diagnostics/countN.m:9-21): w = (1/2pi) * sum of the
+// four quotient angles around (i,j) -> (i+1,j) -> (i+1,j+1) -> (i,j+1);
+// +1 when |w-1| <= 1e-4, -1 when |w+1| <= 1e-4, else 0.
+__device__ __forceinline__ int plaquette_class(const double2 *O, int nx, int ny, long long s) {
+    const int i = (int)(s % nx);
+    const int j = (int)(s / nx);
+    const int i1 = (i + 1 == nx) ? 0 : i + 1;
+    const int j1 = (j + 1 == ny) ? 0 : j + 1;
+    const double2 x1 = O[s];
+    const double2 x2 = O[(long long)j * nx + i1];
+    const double2 x3 = O[(long long)j1 * nx + i1];
+    const double2 x4 = O[(long long)j1 * nx + i];
+    const double inv2pi = 1.0 / (2.0 * 3.14159265358979323846);
+    const double w = inv2pi * (quot_angle(x1, x2) + quot_angle(x2, x3) + quot_angle(x3, x4) +
+                               quot_angle(x4, x1));
+    if (w >= 1.0 - 1e-4 && w <= 1.0 + 1e-4) return 1;
+    if (w <= -1.0 + 1e-4 && w >= -1.0 - 1e-4) return -1;
+    return 0;
+}
+#endif
+
 // Status word shared by the step kernels (device memory).
 struct DevStatus {
     long long step;            // steps completed since the context was created

@@ -14,13 +14,6 @@ namespace hqt {
 
 constexpr int kRedThreads = 256;
 
-__device__ __forceinline__ double quot_angle(double2 a, double2 b) {
-    // angle(a./b)
-    const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
-    const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
-    return atan2(im, re);
-}
-
 // partial[blockIdx.x] = sum over this block's sites of angle(O(x,y+1)/O(x,y))
 __global__ void __launch_bounds__(kRedThreads)
     k_wind_partial(const double2 *O, int nx, int ny, double *partial) {
@@ -73,21 +66,11 @@ __global__ void __launch_bounds__(kRedThreads)
     __shared__ int sp[kRedThreads], sm[kRedThreads];
     const long long n = (long long)nx * ny;
     int cp = 0, cm = 0;
-    const double inv2pi = 1.0 / (2.0 * 3.14159265358979323846);
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
          s += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(s % nx);
-        const int j = (int)(s / nx);
-        const int i1 = (i + 1 == nx) ? 0 : i + 1;
-        const int j1 = (j + 1 == ny) ? 0 : j + 1;
-        const double2 x1 = O[s];
-        const double2 x2 = O[(long long)j * nx + i1];
-        const double2 x3 = O[(long long)j1 * nx + i1];
-        const double2 x4 = O[(long long)j1 * nx + i];
-        const double w = inv2pi * (quot_angle(x1, x2) + quot_angle(x2, x3) +
-                                   quot_angle(x3, x4) + quot_angle(x4, x1));
-        if (w >= 1.0 - 1e-4 && w <= 1.0 + 1e-4) ++cp;
-        if (w <= -1.0 + 1e-4 && w >= -1.0 - 1e-4) ++cm;
+        const int q = plaquette_class(O, nx, ny, s);
+        cp += (q == 1);
+        cm += (q == -1);
     }
     sp[threadIdx.x] = cp;
     sm[threadIdx.x] = cm;
@@ -193,6 +176,14 @@ __global__ void k_rho_scatter(const double *rho2, int nz, long long plane, doubl
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
          s += (long long)gridDim.x * blockDim.x)
         rho3[s] = rho2[s % plane];
+}
+
+// Guard of a captured step: the step graph runs its body (one RK4 step) only
+// while no earlier step has produced a non-finite value, so a run stops at
+// the first bad step like the reference's NaN guard
+// (scripts/simulation/tevol_driven_cluster.m:182-185).
+__global__ void k_step_guard(cudaGraphConditionalHandle h, const DevStatus *st) {
+    cudaGraphSetConditional(h, st->first_bad_step == LLONG_MAX ? 1u : 0u);
 }
 
 __global__ void k_step_end(DevStatus *st) {

@@ -12,7 +12,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "hqt.h"
@@ -24,7 +23,6 @@ namespace {
 
 constexpr long long kNoAllocMaxPlane = 1LL << 20;  // nx*ny <= 1024*1024 (16 MiB of O)
 constexpr int kNoAllocMaxNz = 40;
-constexpr int kMaxDevices = 64;
 constexpr int kThreads = 256;
 
 // Scratch shared by every call on a device: the boundary plane O and the
@@ -50,27 +48,15 @@ __global__ void k_na_boundary(const double2 *psi, long long plane, int nz, Bound
     }
 }
 
-__device__ __forceinline__ double na_angle(double2 a, double2 b) {
-    const double re = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
-    const double im = __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y));
-    return atan2(im, re);
-}
-
 __global__ void k_na_count(const double2 *O, int nx, int ny, int *counts) {
     __shared__ int sp[kThreads], sm[kThreads];
     const long long n = (long long)nx * ny;
     int cp = 0, cm = 0;
-    const double inv2pi = 1.0 / (2.0 * 3.14159265358979323846);
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
          s += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(s % nx), j = (int)(s / nx);
-        const int i1 = (i + 1 == nx) ? 0 : i + 1, j1 = (j + 1 == ny) ? 0 : j + 1;
-        const double2 x1 = O[s], x2 = O[(long long)j * nx + i1];
-        const double2 x3 = O[(long long)j1 * nx + i1], x4 = O[(long long)j1 * nx + i];
-        const double w = inv2pi * (na_angle(x1, x2) + na_angle(x2, x3) + na_angle(x3, x4) +
-                                   na_angle(x4, x1));
-        if (w >= 1.0 - 1e-4 && w <= 1.0 + 1e-4) ++cp;
-        if (w <= -1.0 + 1e-4 && w >= -1.0 - 1e-4) ++cm;
+        const int q = plaquette_class(O, nx, ny, s);  // shared with the context path
+        cp += (q == 1);
+        cm += (q == -1);
     }
     sp[threadIdx.x] = cp;
     sm[threadIdx.x] = cm;
@@ -89,9 +75,6 @@ __global__ void k_na_count(const double2 *O, int nx, int ny, int *counts) {
     }
 }
 
-std::mutex g_mu;
-double2 *g_O_ptr[kMaxDevices];
-int *g_cnt_ptr[kMaxDevices];
 thread_local std::string g_na_err;
 
 int na_fail(int code, const std::string &msg) {
@@ -111,6 +94,8 @@ extern "C" int hqt_count_vortices_field_noalloc(const void *dZ1, int32_t nx, int
                                                 int32_t nz, int32_t *n, int32_t *np,
                                                 int32_t *nm, void *stream) {
     if (!dZ1 || !n || !np || !nm) return na_fail(HQT_EINVAL, "null argument");
+    if (reinterpret_cast<uintptr_t>(dZ1) % 16 != 0)
+        return na_fail(HQT_EINVAL, "dZ1 must be 16-byte aligned (interleaved complex double)");
     if (nx < 2 || ny < 2 || nz < 3 || nz > kNoAllocMaxNz)
         return na_fail(HQT_EINVAL, "nx, ny must be >= 2 and nz in [3, 40]");
     if ((long long)nx * ny > kNoAllocMaxPlane) {
@@ -121,26 +106,22 @@ extern "C" int hqt_count_vortices_field_noalloc(const void *dZ1, int32_t nx, int
         return na_fail(HQT_EINVAL, msg);
     }
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
         return na_fail(HQT_ECUDA, "no current CUDA device");
-    double2 *O = nullptr;
-    int *cnt = nullptr;
+    // The scratch arrays' device addresses, looked up on every call with the
+    // caller's device current: the lookup is cheap next to the synchronising
+    // copy below, and a cached address would go stale after a device reset
+    // (cudaDeviceReset, MATLAB's reset(gpuDevice)), which reloads the module.
+    void *po = nullptr, *pc = nullptr;
     {
-        // once per device, with that device current: the scratch arrays' addresses
-        std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_O_ptr[dev]) {
-            void *po = nullptr, *pc = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&po, g_noalloc_O);
-            if (e == cudaSuccess) e = cudaGetSymbolAddress(&pc, g_noalloc_counts);
-            if (e != cudaSuccess)
-                return na_fail(HQT_ECUDA, std::string("cudaGetSymbolAddress: ") +
-                                              cudaGetErrorString(e));
-            g_O_ptr[dev] = (double2 *)po;
-            g_cnt_ptr[dev] = (int *)pc;
-        }
-        O = g_O_ptr[dev];
-        cnt = g_cnt_ptr[dev];
+        cudaError_t e = cudaGetSymbolAddress(&po, g_noalloc_O);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress(&pc, g_noalloc_counts);
+        if (e != cudaSuccess)
+            return na_fail(HQT_ECUDA, std::string("cudaGetSymbolAddress: ") +
+                                          cudaGetErrorString(e));
     }
+    double2 *O = (double2 *)po;
+    int *cnt = (int *)pc;
     // boundary row of Lz = 2*chebdif(nz,1), as the context path builds it
     BoundaryRow row{};
     chebdif_row(nz, nz - 1, row.w);

@@ -97,8 +97,11 @@ int hqt_set_stream(hqt_ctx *ctx, void *cuda_stream);
 
 /* Advance `nsteps` RK4 steps of the loop body tevol_driven_cluster.m:120-142
  * on HOST arrays, updated in place.  Copies in once, loops on the device,
- * copies out once.  Returns HQT_ENONFINITE (fields as of the last completed
- * step) when a step produced NaN/Inf. */
+ * copies out once.  When a step produces NaN/Inf the run stops there, as the
+ * reference's guard exits after the first bad step (:182-185): every later
+ * step is skipped on the device, the call returns HQT_ENONFINITE, the fields
+ * are those the bad step left, and diag->steps_done = diag->nonfinite_step
+ * counts the steps taken including the bad one. */
 int hqt_step(hqt_ctx *ctx, double *Z1, double *Z2, double *Z3, double *Z4,
              double *rhoi, int64_t nsteps, hqt_diag *diag);
 
@@ -198,11 +201,14 @@ int hqt_vortex_structure_factor_device(hqt_ctx *ctx, const void *dPhi,
  * pool, a framework whose caching allocator owns a fixed device budget, or a
  * real-time host that must not allocate after start-up.  Its scratch is a
  * file-scope device array of nx*ny <= 1048576 points (16 MiB, held by every
- * GPU that loads the library until exit); larger planes return HQT_EINVAL.
- * The first call on a device looks up the scratch address, so make that first
- * call before any stream capture.  All calls share the scratch: calls that
- * overlap on the GPU (other streams, other host threads) race.  Errors are
- * described by hqt_noalloc_last_error(). */
+ * GPU that loads the library until exit); larger planes return HQT_EINVAL,
+ * and so does a dZ1 that is not 16-byte aligned.  Every call looks up the
+ * scratch address with its device current, so a device reset between calls
+ * (cudaDeviceReset, MATLAB's reset(gpuDevice)) is harmless; make the first
+ * call on a device before any stream capture.  All calls share the scratch
+ * and each call clears its counters: calls that overlap on the GPU (other
+ * streams, other host threads) race.  Errors are described by
+ * hqt_noalloc_last_error(). */
 int hqt_count_vortices_field_noalloc(const void *dZ1, int32_t nx, int32_t ny,
                                      int32_t nz, int32_t *n, int32_t *np,
                                      int32_t *nm, void *cuda_stream);
@@ -218,9 +224,11 @@ const char *hqt_noalloc_last_error(void);
  * belongs to member i, same layout and in-place semantics as
  * hqt_step_device) with one CUDA-graph launch per step for the whole
  * ensemble.  `diags` is NULL or an array of one hqt_diag per member;
- * vortex-count records are not taken (n_records = 0).  A non-finite member
- * stops the whole ensemble at the next status poll (every 64 steps) with
- * HQT_ENONFINITE and its diags[i].nonfinite_step set. */
+ * vortex-count records are not taken (n_records = 0).  A member that produces
+ * NaN/Inf stops at its bad step (its later steps are skipped on the device,
+ * diags[i].steps_done = diags[i].nonfinite_step); the other members go on
+ * until the next status poll (every 64 steps), where the call returns
+ * HQT_ENONFINITE. */
 typedef struct hqt_ensemble hqt_ensemble;
 int hqt_ensemble_create(hqt_ctx *const *members, int32_t n, hqt_ensemble **out);
 void hqt_ensemble_destroy(hqt_ensemble *ens);

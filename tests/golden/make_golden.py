@@ -3,9 +3,10 @@
 Reads the reference's shipped stationary seed
 ``data/reference/mu=6,nz=30,vy=7_20.mat`` (MAT v5; its SHA-256 is recorded
 in the reference's ``data/metadata/manifest.csv:10``) and stores its arrays
-as ``seed_mu6_nz30_vy7.npz``.  Run it where the reference checkout exists:
+as ``seed_mu6_nz30_vy7.npz``.  Run it where a reference checkout exists,
+giving the checkout's root directory:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference-root>
 """
 import hashlib
 import json
@@ -32,4 +33,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference-root>")
+    main(sys.argv[1])

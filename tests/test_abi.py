@@ -71,3 +71,15 @@ def test_null_context_is_rejected(hqt):
     lib = hqt._lib.load()
     assert lib.hqt_step(None, None, None, None, None, None, 1, None) == 1
     assert lib.hqt_last_error(None) is not None
+
+
+def test_noalloc_rejects_misaligned_field_without_a_gpu(hqt):
+    """The allocation-free count checks its arguments before any CUDA call:
+    an interleaved-complex field that is not 16-byte aligned is HQT_EINVAL."""
+    lib = hqt._lib.load()
+    n = ctypes.c_int32()
+    code = lib.hqt_count_vortices_field_noalloc(ctypes.c_void_p(0x10008), 16, 16, 8,
+                                                ctypes.byref(n), ctypes.byref(n),
+                                                ctypes.byref(n), None)
+    assert code == 1
+    assert b"aligned" in lib.hqt_noalloc_last_error()

@@ -5,6 +5,24 @@ import numpy as np
 def test_name_formatting(hqt):
     assert hqt.checkpoint.checkpoint_name(50.0) == "check_point_t=50.mat"
     assert hqt.checkpoint.checkpoint_name(0.08) == "check_point_t=0.08.mat"
+    # t accumulated as t = t + h carries rounding noise that num2str hides
+    t = 0.0
+    for _ in range(4):
+        t += 0.02
+    assert hqt.checkpoint.checkpoint_name(t) == "check_point_t=0.08.mat"
+    assert hqt.checkpoint.checkpoint_name(0.123456) == "check_point_t=0.12346.mat"
+
+
+def test_num2str_known_answers(hqt):
+    """MATLAB num2str of non-integers: max(floor(log10|x|)+5, 5) significant
+    digits; integers in full."""
+    n2s = hqt.checkpoint.num2str
+    assert n2s(0.123456) == "0.12346"
+    assert n2s(3.14159) == "3.1416"
+    assert n2s(123.456789) == "123.4568"
+    assert n2s(-0.5) == "-0.5"
+    assert n2s(7.0) == "7"
+    assert n2s(-2.0) == "-2"
 
 
 def test_round_trip(hqt, tmp_path):

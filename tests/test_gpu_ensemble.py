@@ -58,6 +58,43 @@ def test_ensemble_members_match_solo_runs(hqt, cuda):
             assert np.array_equal(api.from_device(g), w), (k, f)
 
 
+def test_ensemble_follows_new_device_arrays(hqt, cuda):
+    """Calls on other device arrays must step those arrays: the ensemble graph
+    bakes in the members' state pointers and is rebuilt when they change.
+    Covered: a second set alive beside the first (the first must stay as its
+    own call left it), and a third set allocated after the second was freed
+    (the caching allocator may hand out the same addresses)."""
+    api = __import__(hqt.__name__ + ".api", fromlist=["to_device"])
+    states = [member_state(hqt, m) for m in MEMBERS[:2]]
+    solo = []
+    for m, st in zip(MEMBERS[:2], states):
+        t = [api.to_device(a) for a in st]
+        with member_sim(hqt, m) as sim:
+            sim.step_device(*t, nsteps=6)
+        solo.append([api.from_device(x) for x in t])
+
+    def check(sets):
+        for k, (want, got) in enumerate(zip(solo, sets)):
+            for f, (w, g) in enumerate(zip(want, got)):
+                assert np.array_equal(api.from_device(g), w), (k, f)
+
+    sims = [member_sim(hqt, m) for m in MEMBERS[:2]]
+    first = [[api.to_device(a) for a in st] for st in states]
+    second = [[api.to_device(a) for a in st] for st in states]
+    with hqt.Ensemble(sims) as ens:
+        ens.step_device(first, nsteps=6)
+        check(first)
+        ens.step_device(second, nsteps=6)
+        check(second)
+        check(first)  # untouched by the second call
+        del second
+        third = [[api.to_device(a) for a in st] for st in states]
+        ens.step_device(third, nsteps=6)
+        check(third)
+    for s in sims:
+        s.close()
+
+
 def test_ensemble_reports_the_nonfinite_member(hqt, cuda):
     api = __import__(hqt.__name__ + ".api", fromlist=["to_device"])
     states = [list(member_state(hqt, m)) for m in MEMBERS[:2]]
@@ -71,7 +108,9 @@ def test_ensemble_reports_the_nonfinite_member(hqt, cuda):
     for s in sims:
         s.close()
     assert e.value.info[1].nonfinite_step == 1
+    assert e.value.info[1].steps_done == 1  # stopped at its bad step
     assert e.value.info[0].nonfinite_step == -1
+    assert e.value.info[0].steps_done == 10
 
 
 def test_ensemble_rejects_duplicate_members(hqt, cuda):

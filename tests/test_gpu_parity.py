@@ -5,6 +5,8 @@ field's maximum (FFT versus dense-matrix derivatives differ at roundoff);
 evolved fields agree to 1e-10 relative L2 after 100 steps, the drop-in
 requirement; vortex counts and windings are bit-exact integers.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -227,9 +229,50 @@ def test_nonfinite_guard(hqt, cuda):
         with pytest.raises(hqt.NonfiniteEvolution) as e:
             sim.step(*state, nsteps=10)
         assert e.value.info.nonfinite_step == 1
+        assert e.value.info.steps_done == 1
         # the context stays usable after the error
         (g1, *_), info = sim.step(*driven_state(hqt, nx, nx, nz), nsteps=1)
         assert np.all(np.isfinite(g1))
+
+
+def test_nonfinite_run_stops_at_the_bad_step(hqt, dev):
+    """Like the reference's guard (tevol_driven_cluster.m:182-185), a run stops
+    at the first non-finite step: the device skips every later step, so the
+    fields returned after asking for 100 steps equal those after 1 step."""
+    to_d, from_d = dev
+    nx, nz = 24, 8
+    state = list(driven_state(hqt, nx, nx, nz))
+    state[2] = state[2].copy()
+    state[2][3, 4, 2] = np.nan
+    out = []
+    for nsteps in (1, 100):
+        t = [to_d(a) for a in state]
+        with hqt.Simulation(nx, nx, nz, Lx=12.0) as sim:
+            with pytest.raises(hqt.NonfiniteEvolution) as e:
+                sim.step_device(*t, nsteps=nsteps)
+        assert e.value.info.nonfinite_step == 1 and e.value.info.steps_done == 1
+        out.append([from_d(x) for x in t])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+def test_device_diagnostics_reject_misaligned_arrays(hqt, cuda):
+    """Interleaved-complex device arguments must be 16-byte aligned: a
+    misaligned pointer is HQT_EINVAL, not a fault on the GPU."""
+    torch = cuda
+    lib = hqt._lib.load()
+    nx, nz = 16, 8
+    buf = torch.zeros(2 * nx * nx * nz + 2, dtype=torch.float64, device="cuda")
+    bad = ctypes.c_void_p(buf.data_ptr() + 8)
+    good = ctypes.c_void_p(buf.data_ptr())
+    n = ctypes.c_int32()
+    with hqt.Simulation(nx, nx, nz, Lx=8.0) as sim:
+        ctx = sim._ctx
+        assert lib.hqt_boundary_order_parameter_device(ctx, bad, good) == 1
+        assert lib.hqt_count_vortices_device(ctx, bad, ctypes.byref(n), ctypes.byref(n),
+                                             ctypes.byref(n)) == 1
+        assert lib.hqt_winding_device(ctx, bad, ctypes.byref(n)) == 1
+        assert b"aligned" in lib.hqt_last_error(ctx)
 
 
 @pytest.mark.parametrize("engine", ["runtime", "stockham"])
