@@ -149,6 +149,31 @@ def oracle_rate(w, nsteps_cap: int, budget_s: float):
     return sites * n / dt, n, dt, cores
 
 
+def host_cpu():
+    """CPU model and logical-core count of this host."""
+    model = None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+def bench_config(workload: str, w: dict, ws: int) -> dict:
+    """The ``config`` of both arms' JSON lines (same workload, same keys)."""
+    sites = w["nx"] * w["ny"] * w["nz"]
+    return {"workload": workload, "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+            "L": w["L"], "mu": w["mu"], "vy": w["vy"], "dt": w["dt"],
+            "remove_winding": w["remove_winding"], "filter": True,
+            "noise": w["noise"], "amp": w["amp"], "seed": w["seed"],
+            "precision": "fp64", "parallelism": f"replicas{ws}",
+            "l2": "no flush: one step touches ~%.2f GB of distinct arrays (about 300 B "
+                  "per site), %.1fx the 126 MB L2" % (300e-9 * sites, 300 * sites / 126e6)}
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -179,18 +204,19 @@ def run_reference(args, w, ws, rank):
         return
     budget = max(20.0, 6.0 * args.steps)
     rate, n, dt, cores = oracle_rate(w, args.steps + args.warmup, budget)
+    host = host_cpu()
     sample = (f"{n} RK4 steps of the {w['nx']}x{w['ny']}x{w['nz']} workload, CPU FP64 "
               f"oracle (NumPy restatement of the reference step, dense fourdif/chebdif "
-              f"operators), {cores} BLAS threads, {dt:.1f} s")
+              f"operators), {cores} BLAS threads, {dt:.1f} s on {host['cpu_model']} "
+              f"({host['nproc']} logical cores)")
     line = {"metric": "RK4 site-updates/s", "value": rate, "unit": "site-updates/s",
             "n_gpus": args.gpus, "steps": n, "warmup": 0,
             "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.workload, **{k: w[k] for k in ("nx", "ny", "nz", "L", "mu", "dt")},
-                       "precision": "fp64"},
+            "config": bench_config(args.workload, w, int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": {"value": rate, "unit": "site-updates/s", "cores": cores,
-                             "kind": "port", "sample": sample},
+                             "kind": "port", "sample": sample, **host},
             "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -296,18 +322,22 @@ def run_ours(args, w, ws, rank, local):
     breakdown = {k["kernel"]: {"launches": k["launches"], "ms": round(k["ms"], 4),
                                "share": round(k["ms"] / tot, 4)} for k in rep["kernels"]}
 
-    # end to end through the host-array call (pinned buffers, 50-step calls:
-    # the reference's checkpoint cadence, tevol_driven_cluster.m:178)
+    # end to end through the host-array call hqt_step on pinned buffers.  Each
+    # call copies the whole state in (Z1..Z4 and rhoi's boundary plane) and
+    # out (Z1..Z4 and rhoi replicated along z).  Headline: calls of 50 steps,
+    # the reference's checkpoint cadence (tevol_driven_cluster.m:178), where
+    # the state has to reach the host for the save; the copies of a call are
+    # spread over its 50 steps.  Beside it: calls of one step each.
     pinned = []
     for a, dt_ in zip(state, (torch.complex128,) + (torch.float64,) * 4):
         t = torch.empty((nz, ny, nx), dtype=dt_, pin_memory=True)
         t.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)))
         pinned.append(t)
     H = [t.numpy().T for t in pinned]
-    per_call = 50
-    calls = max(1, int(round(args.steps / per_call)))
-    e2e = None
-    if not args.no_e2e:
+    h2d_call = (16 + 24) * sites + 8 * nx * ny
+    d2h_call = (16 + 24 + 8) * sites
+
+    def e2e_rate(per_call, calls):
         sim.step(*H, nsteps=per_call, inplace=True)  # warm the host path
         torch.cuda.synchronize()
         if ws > 1:
@@ -317,17 +347,35 @@ def run_ours(args, w, ws, rank, local):
             sim.step(*H, nsteps=per_call, inplace=True)
         torch.cuda.synchronize()
         e2e_s = allreduce_max(time.perf_counter() - t0, ws)
-        e2e = {"value": ws * sites * per_call * calls / e2e_s, "unit": "site-updates/s",
-               "h2d_bytes_per_step": (16 + 24) * sites + 8 * nx * ny,
-               "d2h_bytes_per_step": (16 + 24 + 8) * sites,
-               "step": f"one hqt_step call of {per_call} RK4 steps on pinned host arrays"}
+        return ws * sites * per_call * calls / e2e_s
+
+    e2e = None
+    if not args.no_e2e:
+        per_call = 50
+        calls = max(1, int(round(args.steps / per_call)))
+        e2e = {"value": e2e_rate(per_call, calls), "unit": "site-updates/s",
+               "h2d_bytes_per_step": h2d_call / per_call,
+               "d2h_bytes_per_step": d2h_call / per_call,
+               "h2d_bytes_per_call": h2d_call, "d2h_bytes_per_call": d2h_call,
+               "steps_per_call": per_call,
+               "step": f"hqt_step calls of {per_call} RK4 steps on pinned host arrays, "
+                       f"{calls} calls timed; per-step bytes are the per-call copies / "
+                       f"{per_call}"}
+        n1 = min(50, args.steps)
+        e2e["single_step_calls"] = {
+            "value": e2e_rate(1, n1), "unit": "site-updates/s",
+            "h2d_bytes_per_step": h2d_call, "d2h_bytes_per_step": d2h_call,
+            "step": f"{n1} hqt_step calls of one RK4 step each: the whole state "
+                    f"copied in and out every step"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        rate, n, dt_s, cores = oracle_rate(w, 3, 20.0)
+        rate, n, dt_s, cores = oracle_rate(w, 8, 20.0)
+        host = host_cpu()
         cpu = {"value": rate, "unit": "site-updates/s", "cores": cores, "kind": "port",
                "sample": f"{n} RK4 steps of {nx}x{ny}x{nz} on the CPU FP64 oracle "
-                         f"(NumPy restatement, dense fourdif/chebdif), {dt_s:.1f} s"}
+                         f"(NumPy restatement, dense fourdif/chebdif), {dt_s:.1f} s",
+               **host}
     sim.close()
     if rank == 0:
         line = {"metric": "RK4 site-updates/s", "value": value, "unit": "site-updates/s",
@@ -335,12 +383,7 @@ def run_ours(args, w, ws, rank, local):
                 "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (Newton stationary profile + seeded complex noise)",
-                "config": {"workload": args.workload, "nx": nx, "ny": ny, "nz": nz,
-                           "L": w["L"], "mu": w["mu"], "vy": w["vy"], "dt": w["dt"],
-                           "remove_winding": w["remove_winding"], "filter": True,
-                           "precision": "fp64", "parallelism": f"replicas{ws}",
-                           "l2": "no flush: one step touches ~0.57 GB of distinct "
-                                 "arrays, 4.5x the 126 MB L2"},
+                "config": bench_config(args.workload, w, ws),
                 "gpu_launches": launches, "roofline": roofline,
                 "step_hbm": {"alg_bytes_per_site": STEP_BYTES_FP64, "achieved_gbs": step_gbs,
                              "frac": step_gbs / peak},
