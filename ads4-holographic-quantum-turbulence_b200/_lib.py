@@ -30,7 +30,7 @@ EXPORTS = [
     "hqt_winding_device", "hqt_count_vortices", "hqt_count_vortices_device",
     "hqt_profile", "hqt_profile_report",
     "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
-    "hqt_energy_spectrum_device", "hqt_boundary_velocity_device",
+    "hqt_energy_spectrum_device", "hqt_boundary_velocity_device", "hqt_observables_device",
     "hqt_find_vortices_device", "hqt_vortex_structure_factor_device",
     "hqt_ensemble_create", "hqt_ensemble_destroy", "hqt_ensemble_set_stream",
     "hqt_ensemble_last_error", "hqt_ensemble_step_device",
@@ -49,7 +49,7 @@ class hqt_diag(Structure):
     _fields_ = [("steps_done", c_int64), ("nonfinite_step", c_int64),
                 ("last_winding", c_int32), ("n_records", c_int32),
                 ("capacity", c_int32), ("reserved", c_int32),
-                ("records", POINTER(c_int32))]
+                ("records", POINTER(c_int32)), ("obs", POINTER(c_double))]
 
 
 class HQTError(RuntimeError):
@@ -107,6 +107,7 @@ def load() -> ctypes.CDLL:
         "hqt_energy_spectrum_device": (c_int, [c_void_p, c_void_p, c_int32, dp, dp, dp,
                                                dp, ip]),
         "hqt_boundary_velocity_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "hqt_observables_device": (c_int, [c_void_p, c_void_p, c_void_p, dp]),
         "hqt_find_vortices_device": (c_int, [c_void_p, c_void_p, c_double, c_int32, c_int32,
                                              dp, dp, ip]),
         "hqt_vortex_structure_factor_device": (c_int, [c_void_p, c_void_p, c_double, c_double,

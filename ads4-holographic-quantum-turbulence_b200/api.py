@@ -32,6 +32,8 @@ class StepInfo:
     nonfinite_step: int
     last_winding: int
     records: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    # per record: (Q, E_kin, N_O) of hqt_observables_device
+    observables: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
 
 
 def _dptr(a: np.ndarray):
@@ -137,16 +139,20 @@ class Simulation:
 
     def _diag(self, records: int):
         buf = np.zeros((max(records, 0), 4), dtype=np.int32)
+        obs = np.zeros((max(records, 0), 3))
         d = _lib.hqt_diag()
         d.capacity = int(records)
-        d.records = (buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
-                     if records > 0 else None)
-        return d, buf
+        if records > 0:
+            d.records = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            d.obs = obs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        return d, (buf, obs)
 
     @staticmethod
-    def _info(d, buf) -> StepInfo:
+    def _info(d, bufs) -> StepInfo:
+        buf, obs = bufs
         return StepInfo(int(d.steps_done), int(d.nonfinite_step),
-                        int(d.last_winding), buf[:d.n_records].copy())
+                        int(d.last_winding), buf[:d.n_records].copy(),
+                        obs[:d.n_records].copy())
 
     # -- the loop body ----------------------------------------------------
     def step(self, Z1, Z2, Z3, Z4, rhoi, nsteps: int = 1, records: int = 0,
@@ -253,6 +259,18 @@ class Simulation:
         self._sync_stream()
         self._check(self._lib.hqt_winding_device(self._ctx, p, ctypes.byref(w)))
         return int(w.value)
+
+    def observables_device(self, Z1, rhoi) -> dict:
+        """Global observables of a device state (``hqt_observables_device``):
+        ``Q`` = sum of the boundary charge rhoi(:,:,nz) dx dy, ``E_kin`` =
+        sum |u|^2/2 dx dy of the density-weighted boundary velocity of
+        ``scripts/analysis/movie_show.m:93-94`` and ``N_O`` = sum |O|^2 dx dy,
+        as compensated FP64 sums."""
+        out = np.zeros(3)
+        p = [self._dev3(Z1, True), self._dev3(rhoi)]
+        self._sync_stream()
+        self._check(self._lib.hqt_observables_device(self._ctx, *p, _dptr(out)))
+        return {"Q": float(out[0]), "E_kin": float(out[1]), "N_O": float(out[2])}
 
     def energy_spectrum_device(self, O):
         """``(k, E, E_c, E_i)`` of the boundary superflow of a ``(ny, nx)``

@@ -85,6 +85,8 @@ struct hqt_ctx {
     double *kxv = nullptr, *kyv = nullptr, *bins = nullptr;  // spectrum scratch
     int max_bins = 0;
     int *d_int = nullptr;  // scratch ints (winding, counts)
+    double2 *obs_partial = nullptr;  // compensated observable sums per block
+    double *obs_out = nullptr;       // Q, E_kin, N_O
     DevStatus *st = nullptr;
     // launch geometry
     int NBx_rhs = 1, NBx_2 = 1, TXy_rhs = 1, TXy_2 = 1, TXy_filt = 1;
@@ -926,6 +928,8 @@ int prestep(hqt_ctx *c) {
     return HQT_OK;
 }
 
+int observables(hqt_ctx *c, const double2 *O, const double *rho2, double *out);
+
 int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
     DevStatus h0{};
     CK(cudaMemcpyAsync(&h0, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
@@ -963,6 +967,7 @@ int run_steps(hqt_ctx *c, int64_t nsteps, hqt_diag *diag) {
             r[1] = n;
             r[2] = np;
             r[3] = nm;
+            if (diag->obs) RC(observables(c, c->O, c->rho, diag->obs + kObs * diag->n_records));
             diag->n_records++;
         }
         // graph steps after a non-finite one are no-ops (the guard), so the
@@ -1024,6 +1029,23 @@ int boundary_velocity(hqt_ctx *c, const double2 *O, double2 *U, double *vx, doub
     k_spec_velocity<<<kPartials, 256, 0, c->stream>>>(O, dOx, dOy, c->nx, c->plane, c->colmax,
                                                       U, vx, vy);
     CK(cudaGetLastError());
+    return HQT_OK;
+}
+
+// Global observables of a boundary order parameter O and a boundary charge
+// plane rho2 (both on the device) into the host array out[kObs] =
+// {Q, E_kin, N_O}: compensated FP64 sums times dx*dy.  Scratch: the
+// velocity U in E, its derivatives in dxxpsi, dypsi (free between steps).
+int observables(hqt_ctx *c, const double2 *O, const double *rho2, double *out) {
+    double2 *U = c->E;
+    RC(boundary_velocity(c, O, U, nullptr, nullptr));
+    k_obs_partial<<<kPartials, kRedThreads, 0, c->stream>>>(rho2, U, O, c->plane, c->obs_partial);
+    CK(cudaGetLastError());
+    const double area = (c->p.Lx / c->nx) * (c->p.Ly / c->ny);
+    k_obs_final<<<1, 32, 0, c->stream>>>(c->obs_partial, kPartials, area, c->obs_out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, c->obs_out, sizeof(double) * kObs, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return HQT_OK;
 }
 
@@ -1419,6 +1441,8 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->kyv, sizeof(double) * p.ny);
     A(&c->bins, sizeof(double) * 3 * c->max_bins);
     A(&c->d_int, sizeof(int) * 8);
+    A(&c->obs_partial, sizeof(double2) * kObs * kPartials);
+    A(&c->obs_out, sizeof(double) * kObs);
     A(&c->st, sizeof(DevStatus));
     if (rc != HQT_OK) return bail(rc);
     {
@@ -1766,6 +1790,17 @@ int hqt_count_vortices_device(hqt_ctx *c, const void *dO, int32_t *n, int32_t *n
     if (!al16(dO)) return fail(c, HQT_EINVAL, kAlignMsg);
     DeviceGuard guard(c->device);
     return count_vortices_dev(c, (const double2 *)dO, n, np, nm);
+}
+
+int hqt_observables_device(hqt_ctx *c, const void *dZ1, const void *drhoi, double *obs) {
+    if (!c) return HQT_EINVAL;
+    if (!dZ1 || !drhoi || !obs) return fail(c, HQT_EINVAL, "bad argument");
+    if (!al16(dZ1) || !al8(drhoi)) return fail(c, HQT_EINVAL, kAlignMsg);
+    DeviceGuard guard(c->device);
+    // O into the context's own plane, the boundary slice of rhoi in place
+    RC(launch_zcol_misc(c, nullptr, nullptr, (const double2 *)dZ1, c->O));
+    const double *rho2 = (const double *)drhoi + (size_t)(c->nz - 1) * c->plane;
+    return observables(c, c->O, rho2, obs);
 }
 
 int hqt_energy_spectrum_device(hqt_ctx *c, const void *dO, int32_t capacity, double *k,

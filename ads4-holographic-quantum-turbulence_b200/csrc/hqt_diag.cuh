@@ -190,6 +190,72 @@ __global__ void k_step_end(DevStatus *st) {
     if (threadIdx.x == 0 && blockIdx.x == 0) st->step += 1;
 }
 
+// ---- global observables as compensated FP64 sums -------------------------
+// Q = sum rho dx dy (boundary charge), E_kin = sum |u|^2/2 dx dy (u the
+// density-weighted boundary velocity of movie_show.m:93-94, the field whose
+// spectrum the analysis takes) and N_O = sum |O|^2 dx dy.  Every thread keeps a
+// (sum, compensation) pair per observable updated with Knuth's TwoSum; pairs
+// are merged in a fixed tree per block and then over blocks in index order,
+// so the result is deterministic and carries about twice FP64's precision
+// before the final rounding.
+constexpr int kObs = 3;
+
+__device__ __forceinline__ void two_sum(double a, double b, double &t, double &e) {
+    t = a + b;
+    const double bp = t - a;
+    e = (a - (t - bp)) + (b - bp);
+}
+__device__ __forceinline__ void comp_add(double &s, double &c, double x) {
+    double t, e;
+    two_sum(s, x, t, e);
+    s = t;
+    c += e;
+}
+__device__ __forceinline__ void comp_merge(double &s, double &c, double s2, double c2) {
+    double t, e;
+    two_sum(s, s2, t, e);
+    s = t;
+    c += c2 + e;
+}
+
+// partial[b * kObs + k] = (sum, compensation) of block b for k = Q, E_kin, N_O
+__global__ void __launch_bounds__(kRedThreads)
+    k_obs_partial(const double *rho, const double2 *U, const double2 *O, long long n,
+                  double2 *partial) {
+    __shared__ double ss[kObs][kRedThreads], sc[kObs][kRedThreads];
+    double s[kObs] = {0.0, 0.0, 0.0}, c[kObs] = {0.0, 0.0, 0.0};
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        comp_add(s[0], c[0], rho[i]);
+        const double2 u = U[i], o = O[i];
+        comp_add(s[1], c[1], 0.5 * (u.x * u.x + u.y * u.y));
+        comp_add(s[2], c[2], o.x * o.x + o.y * o.y);
+    }
+    for (int k = 0; k < kObs; ++k) {
+        ss[k][threadIdx.x] = s[k];
+        sc[k][threadIdx.x] = c[k];
+    }
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < kObs; ++k)
+                comp_merge(ss[k][threadIdx.x], sc[k][threadIdx.x], ss[k][threadIdx.x + w],
+                           sc[k][threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x < kObs)
+        partial[blockIdx.x * kObs + threadIdx.x] = make_double2(ss[threadIdx.x][0], sc[threadIdx.x][0]);
+}
+
+// out[k] = area * (merged partials of observable k), one thread per observable
+__global__ void k_obs_final(const double2 *partial, int nparts, double area, double *out) {
+    const int k = threadIdx.x;
+    if (k >= kObs) return;
+    double s = 0.0, c = 0.0;
+    for (int b = 0; b < nparts; ++b) comp_merge(s, c, partial[b * kObs + k].x, partial[b * kObs + k].y);
+    out[k] = area * (s + c);
+}
+
 // ---- energy spectrum of the boundary superflow --------------------------
 // colmax[j] = max_i |O(i, j)| over x for each y index j (one block per j).
 // MATLAB's max of the nx x ny boundary slice is the row vector of column

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define HQT_ABI_VERSION 1
+#define HQT_ABI_VERSION 2  /* 2: hqt_diag.obs, hqt_observables_device */
 
 /* status codes */
 #define HQT_OK            0
@@ -60,7 +60,8 @@ typedef struct {
     int32_t remove_winding;/* 1: global y-winding removal (:136-139);
                               0: lattice script (tevol_lattice.m:168-170)   */
     int32_t precision;     /* HQT_FP64 or HQT_MIXED                         */
-    int32_t diag_every;    /* >0: vortex count every diag_every steps       */
+    int32_t diag_every;    /* >0: vortex count (and, with hqt_diag.obs, the
+                              observables) every diag_every steps           */
     int32_t apply_filter;  /* 1: the 2/3 Fourier filter each step (:142)    */
 } hqt_params;
 
@@ -75,6 +76,10 @@ typedef struct {
     int32_t  reserved;
     int32_t *records;          /* in: caller buffer, 4*capacity int32 laid out
                                   as (step, n, np, nm) per record; may be NULL */
+    double  *obs;              /* in: caller buffer, 3*capacity doubles, the
+                                  observables (Q, E_kin, N_O) of
+                                  hqt_observables_device per record; may be
+                                  NULL (no observables taken)                 */
 } hqt_diag;
 
 /* Version of this ABI (HQT_ABI_VERSION). */
@@ -141,6 +146,19 @@ int hqt_count_vortices(hqt_ctx *ctx, const double *O, int32_t *n,
                        int32_t *np, int32_t *nm);
 int hqt_count_vortices_device(hqt_ctx *ctx, const void *dO, int32_t *n,
                               int32_t *np, int32_t *nm);
+
+/* Global observables of a DEVICE state (no counterpart in the reference,
+ * whose scripts compute no global charge or energy in the loop): obs[0] = Q =
+ * sum rhoi(:,:,nz) dx dy, the boundary charge that the continuity update
+ * rhoi = rhoi - k2(:,:,nz) (tevol_driven_cluster.m:128) conserves exactly in
+ * exact arithmetic; obs[1] = E_kin = sum |u|^2/2 dx dy with u the
+ * density-weighted boundary velocity of scripts/analysis/movie_show.m:93-94
+ * (see hqt_boundary_velocity_device), the field whose spectrum the analysis
+ * takes; obs[2] = N_O = sum |O|^2 dx dy of O = func_Lz(Z1)(:,:,nz).  dx =
+ * Lx/nx, dy = Ly/ny.  Sums are compensated (TwoSum) FP64 in a fixed order:
+ * deterministic, and the precision of the sum does not depend on nx*ny. */
+int hqt_observables_device(hqt_ctx *ctx, const void *dZ1, const void *drhoi,
+                           double *obs);
 
 /* Kinetic-energy spectrum of the boundary superflow of a device O
  * (interleaved complex [nx,ny]), after scripts/analysis/movie_show.m:93-94,

@@ -450,6 +450,24 @@ def boundary_fields(op: Operators, Z1: np.ndarray):
     return O, vx, vy, n
 
 
+def observables(op: Operators, Z1: np.ndarray, rhoi: np.ndarray):
+    """Global observables of a state, build-defined (the reference computes no
+    global charge or energy in its loop): ``Q = sum rhoi(:,:,nz) dx dy``, the
+    boundary charge that the update ``rhoi = rhoi - k2(:,:,nz)``
+    (``tevol_driven_cluster.m:128``) conserves in exact arithmetic (``k2`` is
+    a spectral divergence, whose plane sum vanishes); ``E_kin = sum |u|^2/2
+    dx dy`` of the velocity of :func:`boundary_velocity`; ``N_O = sum |O|^2
+    dx dy``.  Sums are exact-rounded (``math.fsum``)."""
+    import math
+    O = boundary_order_parameter(op, Z1)
+    vx, vy = boundary_velocity(O, op.Lx_len, op.Ly_len)
+    area = (op.Lx_len / op.nx) * (op.Ly_len / op.ny)
+    q = area * math.fsum(np.asarray(rhoi)[:, :, -1].ravel())
+    e = area * math.fsum((0.5 * (vx * vx + vy * vy)).ravel())
+    n = area * math.fsum((O.real ** 2 + O.imag ** 2).ravel())
+    return q, e, n
+
+
 def energy_spectrum(O: np.ndarray, Lx: float, Ly: float):
     """Incompressible/compressible kinetic-energy spectrum of the boundary flow.
 

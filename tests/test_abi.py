@@ -28,7 +28,7 @@ def test_every_declared_symbol_is_exported(hqt):
 
 
 def test_abi_version(hqt):
-    assert hqt._lib.load().hqt_abi_version() == 1
+    assert hqt._lib.load().hqt_abi_version() == 2
 
 
 def test_struct_layout_matches_c(hqt, tmp_path):

@@ -353,3 +353,35 @@ def test_mixed_precision_driven_301(hqt, cuda, dev):
             "Z3_abs": float(np.max(np.abs(m[2] - f[2])) / np.max(np.abs(f[1])))}
     print("mixed vs fp64 after 100 steps (301^2x21):", errs)
     assert max(errs.values()) < 1e-8, errs
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 64, 21), (301, 301, 9), (53, 48, 8)])
+def test_observables_parity(hqt, oracle, dev, nx, ny, nz):
+    """Q, E_kin, N_O (compensated FP64 sums) against the oracle's exactly
+    rounded sums on the same state."""
+    to_d, from_d = dev
+    L = 0.5 * nx
+    state = driven_state(hqt, nx, ny, nz, noise="complex", amp=0.05)
+    op = oracle.build_operators(nx, ny, nz, L)
+    want = oracle.observables(op, state[0], state[4])
+    with hqt.Simulation(nx, ny, nz, Lx=L) as sim:
+        got = sim.observables_device(to_d(state[0]), to_d(state[4]))
+    for k, w in zip(("Q", "E_kin", "N_O"), want):
+        assert abs(got[k] - w) <= 1e-12 * abs(w), (k, got[k], w)
+
+
+def test_observable_records_in_loop(hqt, dev):
+    """With records, every diag_every steps the step records (Q, E_kin, N_O)
+    of the state at that step; the charge stays conserved to roundoff."""
+    to_d, from_d = dev
+    nx, nz, L = 48, 12, 24.0
+    state = driven_state(hqt, nx, nx, nz, noise="complex", amp=0.05)
+    with hqt.Simulation(nx, nx, nz, Lx=L, vy=VY7, diag_every=3) as sim:
+        t = [to_d(a) for a in state]
+        q0 = sim.observables_device(t[0], t[4])
+        info = sim.step_device(*t, nsteps=6, records=4)
+        last = sim.observables_device(t[0], t[4])
+    assert info.observables.shape == (2, 3)
+    assert list(info.records[:, 0]) == [3, 6]
+    assert tuple(info.observables[1]) == (last["Q"], last["E_kin"], last["N_O"])
+    assert abs(info.observables[1, 0] - q0["Q"]) < 1e-12 * abs(q0["Q"])
