@@ -122,29 +122,31 @@ class ClockSampler:
 
 
 def oracle_rate(w, nsteps_cap: int, budget_s: float):
-    """Site-updates/s of the CPU FP64 oracle on a bounded sample of the
-    workload (whole RK4 steps, up to nsteps_cap or budget_s seconds)."""
+    """Site-updates/s of the CPU FP64 restatement of the step in C + OpenMP
+    (oracle/hqt_step_omp.c: the reference's dense fourdif/chebdif operators,
+    all host cores) on a bounded sample of the workload: whole RK4 steps, up
+    to nsteps_cap or budget_s seconds, after one untimed step."""
+    import subprocess
     sys.path.insert(0, str(ROOT / "oracle"))
     import hqt_oracle as oracle
+    if not (ROOT / "oracle" / "libhqt_oracle_omp.so").exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "-s"], check=True)
     hqt = importlib.import_module(PKG)
     prof = hqt.seed.stationary_profile(w["mu"], w["vy"])
     st = hqt.seed.init_driven(w["nx"], w["ny"], w["nz"], prof, noise=w["noise"],
                               amplitude=w["amp"], seed=w["seed"])
     op = oracle.build_operators(w["nx"], w["ny"], w["nz"], w["L"])
-    s = oracle.OracleState(*st)
+    s, _, _ = oracle.omp_run(op, oracle.OracleState(*st), 1, w["dt"], w["mu"], w["vy"],
+                             w["remove_winding"])
     t0 = time.perf_counter()
     n = 0
     while n < max(1, nsteps_cap):
-        s, _ = oracle.rk4_step(op, s, w["dt"], w["mu"], w["vy"], w["remove_winding"])
+        s, _, _ = oracle.omp_run(op, s, 1, w["dt"], w["mu"], w["vy"], w["remove_winding"])
         n += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    try:
-        from threadpoolctl import threadpool_info
-        cores = max(i.get("num_threads", 1) for i in threadpool_info()) or 1
-    except Exception:
-        cores = os.cpu_count() or 1
+    cores = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or os.cpu_count() or 1
     sites = w["nx"] * w["ny"] * w["nz"]
     return sites * n / dt, n, dt, cores
 
@@ -206,9 +208,9 @@ def run_reference(args, w, ws, rank):
     rate, n, dt, cores = oracle_rate(w, args.steps + args.warmup, budget)
     host = host_cpu()
     sample = (f"{n} RK4 steps of the {w['nx']}x{w['ny']}x{w['nz']} workload, CPU FP64 "
-              f"oracle (NumPy restatement of the reference step, dense fourdif/chebdif "
-              f"operators), {cores} BLAS threads, {dt:.1f} s on {host['cpu_model']} "
-              f"({host['nproc']} logical cores)")
+              f"restatement of the reference step in C + OpenMP (dense fourdif/chebdif "
+              f"operators as the reference applies them), {cores} threads, {dt:.1f} s on "
+              f"{host['cpu_model']} ({host['nproc']} logical cores)")
     line = {"metric": "RK4 site-updates/s", "value": rate, "unit": "site-updates/s",
             "n_gpus": args.gpus, "steps": n, "warmup": 0,
             "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
@@ -373,8 +375,9 @@ def run_ours(args, w, ws, rank, local):
         rate, n, dt_s, cores = oracle_rate(w, 8, 20.0)
         host = host_cpu()
         cpu = {"value": rate, "unit": "site-updates/s", "cores": cores, "kind": "port",
-               "sample": f"{n} RK4 steps of {nx}x{ny}x{nz} on the CPU FP64 oracle "
-                         f"(NumPy restatement, dense fourdif/chebdif), {dt_s:.1f} s",
+               "sample": f"{n} RK4 steps of {nx}x{ny}x{nz}, CPU FP64 restatement in C + "
+                         f"OpenMP (dense fourdif/chebdif as the reference applies them), "
+                         f"{cores} threads, {dt_s:.1f} s",
                **host}
     sim.close()
     if rank == 0:

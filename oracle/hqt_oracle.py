@@ -141,15 +141,17 @@ def filter_mask(nx: int, ny: int) -> np.ndarray:
     Restates ``scripts/simulation/tevol_driven_cluster.m:27-31``:
     ``fx(round(round(nx/3)):round(nx/3*2)) = 1`` with 1-based MATLAB indices.
     """
-    fx = np.zeros(nx, dtype=bool)
-    lo = int(matlab_round(matlab_round(nx / 3)))
-    hi = int(matlab_round(nx / 3 * 2))
-    fx[lo - 1:hi] = True
-    fy = np.zeros(ny, dtype=bool)
-    lo = int(matlab_round(matlab_round(ny / 3)))
-    hi = int(matlab_round(ny / 3 * 2))
-    fy[lo - 1:hi] = True
-    return fx[:, None] | fy[None, :]
+    return filter_band(nx)[:, None] | filter_band(ny)[None, :]
+
+
+def filter_band(n: int) -> np.ndarray:
+    """``fx(round(round(n/3)):round(n/3*2)) = 1`` (1-based) of
+    ``tevol_driven_cluster.m:27-29`` along one axis of ``n >= 2`` points."""
+    f = np.zeros(n, dtype=bool)
+    lo = int(matlab_round(matlab_round(n / 3)))
+    hi = int(matlab_round(n / 3 * 2))
+    f[lo - 1:hi] = True
+    return f
 
 
 def ff(x: np.ndarray, mask: np.ndarray) -> np.ndarray:
@@ -656,3 +658,65 @@ def vortex_structure_factor(Phi: np.ndarray, Lx: float, Ly: float):
         Sn = np.where(cnt > 0, sn / np.maximum(cnt, 1), 0.0)
     k_bin = (np.arange(nb) + 0.5) * dk
     return k_bin, Sc, Sn, vort, spacing
+
+
+# ---------------------------------------------------------------------------
+# The same step in C + OpenMP (oracle/hqt_step_omp.c, built by oracle/Makefile)
+# ---------------------------------------------------------------------------
+_OMP_LIB = None
+
+
+def omp_library():
+    """ctypes handle of ``oracle/libhqt_oracle_omp.so`` (``make -C oracle``)."""
+    global _OMP_LIB
+    if _OMP_LIB is None:
+        import ctypes
+        from pathlib import Path
+        path = Path(__file__).resolve().parent / "libhqt_oracle_omp.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} is not built: run `make -C oracle`")
+        lib = ctypes.CDLL(str(path))
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.hqt_omp_run.restype = ctypes.c_int
+        lib.hqt_omp_run.argtypes = ([ctypes.c_int] * 3 + [ctypes.c_double] + [dp] * 9
+                                    + [dp] * 5 + [ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_double,
+                                                  ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_int)])
+        _OMP_LIB = lib
+    return _OMP_LIB
+
+
+def filter_matrices(n: int):
+    """Real and imaginary parts of the circulant ``W = F^-1 diag(m) F`` with
+    ``m`` the kept modes of ``tevol_driven_cluster.m:27-31`` along one axis
+    (``ff`` keeps mode (kx, ky) iff both indices are outside the band)."""
+    m = (~filter_band(n)).astype(np.float64)
+    W = np.fft.ifft(m[:, None] * np.fft.fft(np.eye(n), axis=0), axis=0)
+    return np.ascontiguousarray(W.real), np.ascontiguousarray(W.imag)
+
+
+def omp_run(op: Operators, s: OracleState, nsteps: int, h: float, mu: float, vy: float,
+            remove_winding: bool = True, apply_filter: bool = True):
+    """``nsteps`` steps of :func:`rk4_step` in C + OpenMP on all host cores.
+
+    Returns ``(state, windings, bad_step)``: ``bad_step`` is 0, or the 1-based
+    step at which a NaN appeared (the run stops there, like :func:`run`)."""
+    import ctypes
+    lib = omp_library()
+    dp = ctypes.POINTER(ctypes.c_double)
+    Rx, Ix = filter_matrices(op.nx)
+    Ry, Iy = filter_matrices(op.ny)
+    mats = [np.ascontiguousarray(a, dtype=np.float64) for a in
+            (op.Lx, op.Ly, op.Lz, op.Lz1, op.zz, Rx, Ix, Ry, Iy)]
+    Z1 = np.asfortranarray(s.Z1, dtype=np.complex128).copy(order="F")
+    Z2, Z3, Z4, rh = (np.asfortranarray(a, dtype=np.float64).copy(order="F")
+                      for a in (s.Z2, s.Z3, s.Z4, s.rhoi))
+    w = np.zeros(max(nsteps, 1), dtype=np.int32)
+    ptr = lambda a: a.ctypes.data_as(dp)
+    bad = lib.hqt_omp_run(op.nx, op.ny, op.nz, op.Ly_len, *[ptr(a) for a in mats],
+                          ptr(Z1), ptr(Z2), ptr(Z3), ptr(Z4), ptr(rh), int(nsteps),
+                          float(h), float(mu), float(vy), int(bool(remove_winding)),
+                          int(bool(apply_filter)), w.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    nrun = bad if bad else nsteps
+    return OracleState(Z1, Z2, Z3, Z4, rh), [int(v) for v in w[:nrun]], int(bad)
