@@ -28,7 +28,7 @@ EXPORTS = [
     "hqt_set_stream", "hqt_step", "hqt_step_device", "hqt_rhs_device",
     "hqt_filter_device", "hqt_boundary_order_parameter_device",
     "hqt_winding_device", "hqt_count_vortices", "hqt_count_vortices_device",
-    "hqt_profile", "hqt_profile_report",
+    "hqt_profile", "hqt_profile_report", "hqt_config_report",
     "hqt_count_vortices_field_noalloc", "hqt_noalloc_last_error",
     "hqt_energy_spectrum_device", "hqt_boundary_velocity_device", "hqt_observables_device",
     "hqt_find_vortices_device", "hqt_vortex_structure_factor_device",
@@ -42,7 +42,8 @@ class hqt_params(Structure):
                 ("Lx", c_double), ("Ly", c_double), ("mu", c_double),
                 ("vy", c_double), ("dt", c_double),
                 ("remove_winding", c_int32), ("precision", c_int32),
-                ("diag_every", c_int32), ("apply_filter", c_int32)]
+                ("diag_every", c_int32), ("apply_filter", c_int32),
+                ("autotune", c_int32)]
 
 
 class hqt_diag(Structure):
@@ -101,6 +102,7 @@ def load() -> ctypes.CDLL:
         "hqt_count_vortices_device": (c_int, [c_void_p, c_void_p, ip, ip, ip]),
         "hqt_profile": (c_int, [c_void_p, c_int]),
         "hqt_profile_report": (c_int, [c_void_p, ctypes.c_char_p, c_int64]),
+        "hqt_config_report": (c_int, [c_void_p, ctypes.c_char_p, c_int64]),
         "hqt_count_vortices_field_noalloc": (c_int, [c_void_p, c_int32, c_int32,
                                                      c_int32, ip, ip, ip, c_void_p]),
         "hqt_noalloc_last_error": (c_char_p, []),

@@ -47,6 +47,9 @@ class Simulation:
     ``nz`` Chebyshev points, box lengths ``Lx, Ly`` (``L0, L``), chemical
     potential ``mu``, drive ``vy`` (boundary value ``A_y = -vy``), time step
     ``dt`` (``h``), ``remove_winding`` (driven script) and ``apply_filter``.
+    ``autotune`` times the line-pass geometries (transform engine per axis,
+    lines per block) at creation and keeps the fastest
+    (:meth:`config_report` shows the choice).
     """
 
     def __init__(self, nx: int, ny: int | None = None, nz: int = 21,
@@ -54,7 +57,7 @@ class Simulation:
                  mu: float = 6.0, vy: float = 0.0, dt: float = 0.02,
                  remove_winding: bool = True, precision: str = "fp64",
                  diag_every: int = 0, apply_filter: bool = True,
-                 device: int = 0):
+                 device: int = 0, autotune: bool = False):
         ny = nx if ny is None else ny
         Lx = (nx - 1) / 2 if Lx is None else Lx
         Ly = Lx if Ly is None else Ly
@@ -65,7 +68,7 @@ class Simulation:
                                       float(Ly), float(mu), float(vy),
                                       float(dt), int(bool(remove_winding)),
                                       prec, int(diag_every),
-                                      int(bool(apply_filter)))
+                                      int(bool(apply_filter)), int(bool(autotune)))
         self._lib = _lib.load()
         ctx = ctypes.c_void_p()
         code = self._lib.hqt_create(ctypes.byref(self.params), self.device,
@@ -204,6 +207,13 @@ class Simulation:
         """Reset the launch counters; with ``enable`` every launch is timed
         with CUDA events (outside the step graph)."""
         self._check(self._lib.hqt_profile(self._ctx, int(bool(enable))))
+
+    def config_report(self) -> dict:
+        """The line-pass geometry in use (and the autotuner's timings)."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.hqt_config_report(self._ctx, buf, len(buf)))
+        return json.loads(buf.value.decode())
 
     def profile_report(self) -> dict:
         import json

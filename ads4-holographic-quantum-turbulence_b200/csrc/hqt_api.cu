@@ -15,7 +15,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -116,6 +119,7 @@ struct hqt_ctx {
     std::vector<long long> prof_count;
     std::vector<double> prof_ms;
     long long launches = 0;
+    std::string tune_json;  // launch geometry and, when tuned, the candidates timed
     std::vector<void *> allocs;
     std::string err;
 };
@@ -1003,6 +1007,217 @@ void use_internal_state(hqt_ctx *c) {
     c->cay = c->ay;
 }
 
+// ---------------------------------------------------------------- autotuner
+// Launch geometry of the line passes: the transform engine per axis
+// (prime-factor tensor-core engine, compile-time Stockham engine, runtime-plan
+// engine) and the lines per block of the runtime-plan engine.
+struct LineGeom {
+    bool px, py, cx, cy;
+    int NBx_rhs, NBx_2, TXy_rhs, TXy_2, TXy_filt;
+};
+
+LineGeom get_geom(const hqt_ctx *c) {
+    return LineGeom{c->px, c->py, c->cx, c->cy, c->NBx_rhs, c->NBx_2,
+                    c->TXy_rhs, c->TXy_2, c->TXy_filt};
+}
+
+void set_geom(hqt_ctx *c, const LineGeom &g) {
+    c->px = g.px;
+    c->py = g.py;
+    c->cx = g.cx;
+    c->cy = g.cy;
+    c->NBx_rhs = g.NBx_rhs;
+    c->NBx_2 = g.NBx_2;
+    c->TXy_rhs = g.TXy_rhs;
+    c->TXy_2 = g.TXy_2;
+    c->TXy_filt = g.TXy_filt;
+    c->fused_convert = c->mixed && c->p.apply_filter && c->px && c->py;
+}
+
+bool same_geom(const LineGeom &a, const LineGeom &b) {
+    return a.px == b.px && a.py == b.py && a.cx == b.cx && a.cy == b.cy &&
+           a.NBx_rhs == b.NBx_rhs && a.NBx_2 == b.NBx_2 && a.TXy_rhs == b.TXy_rhs &&
+           a.TXy_2 == b.TXy_2 && a.TXy_filt == b.TXy_filt;
+}
+
+const char *engine_name(bool p, bool ct) { return p ? "prime-factor" : ct ? "stockham" : "runtime"; }
+
+std::string geom_json(const LineGeom &g) {
+    char b[256];
+    std::snprintf(b, sizeof(b),
+                  "{\"x_engine\": \"%s\", \"y_engine\": \"%s\", \"NBx_rhs\": %d, \"NBx_2\": %d, "
+                  "\"TXy_rhs\": %d, \"TXy_2\": %d, \"TXy_filt\": %d}",
+                  engine_name(g.px, g.cx), engine_name(g.py, g.cy), g.NBx_rhs, g.NBx_2,
+                  g.TXy_rhs, g.TXy_2, g.TXy_filt);
+    return b;
+}
+
+std::mutex g_tune_mu;
+std::map<std::string, LineGeom> g_tune_cache;
+bool g_tune_file_read = false;
+
+// The tuning cache file (HQT_TUNE_CACHE): one line per tuned configuration,
+// "<key> px py cx cy NBx_rhs NBx_2 TXy_rhs TXy_2 TXy_filt".
+void tune_file_read_locked() {
+    if (g_tune_file_read) return;
+    g_tune_file_read = true;
+    const char *path = std::getenv("HQT_TUNE_CACHE");
+    if (!path) return;
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream in(line);
+        std::string key;
+        int v[9];
+        if (!(in >> key)) continue;
+        bool ok = true;
+        for (int &x : v) ok = ok && static_cast<bool>(in >> x);
+        if (!ok) continue;
+        g_tune_cache[key] = LineGeom{v[0] != 0, v[1] != 0, v[2] != 0, v[3] != 0, v[4],
+                                     v[5], v[6], v[7], v[8]};
+    }
+}
+
+void tune_file_append(const std::string &key, const LineGeom &g) {
+    const char *path = std::getenv("HQT_TUNE_CACHE");
+    if (!path) return;
+    std::ofstream f(path, std::ios::app);
+    f << key << ' ' << g.px << ' ' << g.py << ' ' << g.cx << ' ' << g.cy << ' ' << g.NBx_rhs
+      << ' ' << g.NBx_2 << ' ' << g.TXy_rhs << ' ' << g.TXy_2 << ' ' << g.TXy_filt << '\n';
+}
+
+// A geometry from a cache could name an engine this build lacks for the length.
+bool geom_valid(const hqt_ctx *c, const LineGeom &g) {
+    if ((g.px && !pfa_length(c->nx)) || (g.py && !pfa_length(c->ny))) return false;
+    if ((g.cx && !ct_supported(c->nx)) || (g.cy && !ct_supported(c->ny))) return false;
+    const size_t lim = 227 * 1024 - 1024;
+    const int v[5] = {g.NBx_rhs, g.NBx_2, g.TXy_rhs, g.TXy_2, g.TXy_filt};
+    for (int x : v)
+        if (x < 1 || x > 32) return false;
+    return std::max({smem_x(c->nx, 3, g.NBx_rhs), smem_x(c->ny, 4, g.TXy_rhs),
+                     smem_x(c->nx, 2, g.NBx_2), smem_x(c->ny, 2, g.TXy_2),
+                     smem_x(c->ny, 2, 3 * g.TXy_filt)}) <= lim;
+}
+
+int prestep(hqt_ctx *c);
+
+// Mean time of one eager step (ms) with geometry g on the internal state.
+int time_geom(hqt_ctx *c, const LineGeom &g, double *ms) {
+    set_geom(c, g);
+    use_internal_state(c);
+    drop_graph(c);
+    RC(prestep(c));
+    for (int i = 0; i < 2; ++i) RC(enqueue_step(c));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, c->stream));
+    constexpr int kSteps = 3;
+    int r = HQT_OK;
+    for (int i = 0; i < kSteps && r == HQT_OK; ++i) r = enqueue_step(c);
+    cudaEventRecord(b, c->stream);
+    const cudaError_t e = cudaEventSynchronize(b);
+    float t = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (r != HQT_OK) return r;
+    if (e != cudaSuccess) return fail(c, HQT_ECUDA, std::string("tuning: ") + cudaGetErrorString(e));
+    *ms = t / kSteps;
+    return HQT_OK;
+}
+
+// Choose the line-pass geometry by timing whole steps: every engine pairing
+// this build has for (nx, ny), and for the runtime-plan engine its
+// shared-memory heuristic and half of it.  Results are cached per process
+// (and in the file named by HQT_TUNE_CACHE) under the grid, precision and
+// step options.  The internal state is used as scratch and the step counter
+// reset afterwards.
+int autotune(hqt_ctx *c) {
+    char kb[160];
+    std::snprintf(kb, sizeof(kb), "dev%d:%dx%dx%d:%s:f%d:w%d", c->device, c->nx, c->ny, c->nz,
+                  c->mixed ? "mixed" : "fp64", c->p.apply_filter, c->p.remove_winding);
+    const std::string key = kb;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_file_read_locked();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end() && geom_valid(c, it->second)) {
+            set_geom(c, it->second);
+            c->tune_json = "{\"autotuned\": true, \"cached\": true, \"key\": \"" + key +
+                           "\", \"chosen\": " + geom_json(it->second) + "}";
+            return HQT_OK;
+        }
+    }
+    const LineGeom base = get_geom(c);
+    std::vector<LineGeom> cand;
+    std::vector<std::pair<bool, bool>> ex, ey;  // (prime-factor, stockham)
+    if (pfa_length(c->nx)) ex.push_back({true, false});
+    if (ct_supported(c->nx)) ex.push_back({false, true});
+    ex.push_back({false, false});
+    if (pfa_length(c->ny)) ey.push_back({true, false});
+    if (ct_supported(c->ny)) ey.push_back({false, true});
+    ey.push_back({false, false});
+    for (auto x : ex)
+        for (auto y : ey) {
+            LineGeom g = base;
+            g.px = x.first;
+            g.cx = x.second;
+            g.py = y.first;
+            g.cy = y.second;
+            cand.push_back(g);
+            const bool rx = !g.px && !g.cx, ry = !g.py && !g.cy;
+            if (rx || ry) {  // the runtime engine's batching, halved
+                LineGeom h = g;
+                if (rx) {
+                    h.NBx_rhs = std::max(1, g.NBx_rhs / 2);
+                    h.NBx_2 = std::max(1, g.NBx_2 / 2);
+                }
+                if (ry) {
+                    h.TXy_rhs = std::max(1, g.TXy_rhs / 2);
+                    h.TXy_2 = std::max(1, g.TXy_2 / 2);
+                    h.TXy_filt = std::max(1, g.TXy_filt / 2);
+                }
+                if (!same_geom(h, g)) cand.push_back(h);
+            }
+        }
+    std::string list;
+    double best = 1e300;
+    LineGeom chosen = base;
+    for (const LineGeom &g : cand) {
+        if (!geom_valid(c, g)) continue;
+        double ms = 0.0;
+        RC(time_geom(c, g, &ms));
+        list += (list.empty() ? "" : ", ") + std::string("{\"geometry\": ") + geom_json(g) +
+                ", \"ms_per_step\": " + std::to_string(ms) + "}";
+        if (ms < best) {
+            best = ms;
+            chosen = g;
+        }
+    }
+    set_geom(c, chosen);
+    drop_graph(c);
+    // leave the context as created: zero state and status, no launches counted
+    DevStatus s0{};
+    s0.first_bad_step = LLONG_MAX;
+    CK(cudaMemcpyAsync(c->st, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream));
+    const size_t V = (size_t)c->vol;
+    CK(cudaMemsetAsync(c->psi, 0, sizeof(double2) * V, c->stream));
+    CK(cudaMemsetAsync(c->at, 0, sizeof(double) * V, c->stream));
+    CK(cudaMemsetAsync(c->ax, 0, sizeof(double) * V, c->stream));
+    CK(cudaMemsetAsync(c->ay, 0, sizeof(double) * V, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->launches = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = chosen;
+        tune_file_append(key, chosen);
+    }
+    c->tune_json = "{\"autotuned\": true, \"cached\": false, \"key\": \"" + key +
+                   "\", \"chosen\": " + geom_json(chosen) + ", \"candidates\": [" + list + "]}";
+    return HQT_OK;
+}
+
 // signed integer wavenumbers of an n-point transform (even n: [0:n/2-1, -n/2:-1])
 void signed_k(int n, double scale, std::vector<double> &k) {
     k.resize(n);
@@ -1548,6 +1763,11 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     use_internal_state(c);
     c->prof_count.assign(K_NKINDS, 0);
     c->prof_ms.assign(K_NKINDS, 0.0);
+    c->tune_json = "{\"autotuned\": false, \"chosen\": " + geom_json(get_geom(c)) + "}";
+    if (p.autotune && !std::getenv("HQT_LINE_ENGINE")) {
+        const int r = autotune(c);
+        if (r != HQT_OK) return bail(r);
+    }
     *out = c;
     return HQT_OK;
 }
@@ -1657,6 +1877,13 @@ int hqt_profile(hqt_ctx *c, int enable) {
     c->prof_ms.assign(K_NKINDS, 0.0);
     c->launches = 0;
     c->prof_on = enable != 0;
+    return HQT_OK;
+}
+
+int hqt_config_report(hqt_ctx *c, char *buf, int64_t len) {
+    if (!c || !buf || len <= 0) return HQT_EINVAL;
+    if ((int64_t)c->tune_json.size() + 1 > len) return fail(c, HQT_EINVAL, "report buffer too small");
+    std::memcpy(buf, c->tune_json.c_str(), c->tune_json.size() + 1);
     return HQT_OK;
 }
 

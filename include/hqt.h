@@ -63,6 +63,10 @@ typedef struct {
     int32_t diag_every;    /* >0: vortex count (and, with hqt_diag.obs, the
                               observables) every diag_every steps           */
     int32_t apply_filter;  /* 1: the 2/3 Fourier filter each step (:142)    */
+    int32_t autotune;      /* 1: hqt_create times the line-pass geometries
+                              (transform engine per axis, lines per block)
+                              and keeps the fastest; cached per process and
+                              in the file named by HQT_TUNE_CACHE           */
 } hqt_params;
 
 /* Per-call diagnostics. */
@@ -268,6 +272,12 @@ int hqt_ensemble_step_device(hqt_ensemble *ens, void *const *dZ1, void *const *d
  * with the kernel launches issued since the last reset and the summed event
  * times per kernel kind. */
 int hqt_profile(hqt_ctx *ctx, int enable);
+
+/* JSON object with the context's line-pass geometry ("chosen": transform
+ * engine per axis, lines per block) and, when hqt_params.autotune was set,
+ * the candidates timed (ms per step) and whether the choice came from the
+ * cache.  No counterpart in the reference. */
+int hqt_config_report(hqt_ctx *ctx, char *buf, int64_t len);
 int hqt_profile_report(hqt_ctx *ctx, char *buf, int64_t len);
 
 #ifdef __cplusplus
