@@ -1,5 +1,6 @@
 // hqt_z_impl.cuh -- launchers of the column kernels for one column length
 // HQT_ZN (each hqt_z<N>.cu defines HQT_ZN and includes this file).
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -47,6 +48,14 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 2>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 3>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 4>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 1, true>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 2, true>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 3, true>);
+    opt((const void *)k_zstage<double, double, double, HQT_ZN, 4, true>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 1, true>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 2, true>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 3, true>);
+    opt((const void *)k_zstage<double, double, float, HQT_ZN, 4, true>);
     opt((const void *)k_zcons_tc<HQT_ZN>);
     return e;
 }
@@ -54,15 +63,15 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
 // One fused launch per stage (hqt_zfused.cuh): persistent blocks of kZWarps
 // warps, as many as fit on the device at once, each looping over tiles of
 // kZTile columns.
-template <typename TD, int M> static int z_stage_grid(long long plane) {
+template <typename TD, int M, bool SPLIT> static int z_stage_grid(long long plane) {
     static int per_sm = 0, nsm = 0;
     if (per_sm == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_zstage<double, double, TD, HQT_ZN, M>, kZThreads,
-            zf_smem_bytes<double, double, TD, HQT_ZN>());
+            &per_sm, k_zstage<double, double, TD, HQT_ZN, M, SPLIT>, kZThreads,
+            zf_smem_bytes<double, double, TD, HQT_ZN, SPLIT>());
         if (per_sm < 1) per_sm = 1;
     }
     const long long tiles = (plane + kZTile - 1) / kZTile;
@@ -70,33 +79,51 @@ template <typename TD, int M> static int z_stage_grid(long long plane) {
     return (int)(tiles < full ? tiles : full);
 }
 
-template <typename TD>
-static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> &a,
-                                 const ZHost &h, cudaStream_t s) {
-    const ZOps<double, HQT_ZN> op = make_zops(h);
-    constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN>();
+// HQT_ZSPLIT=1 selects the split-region variant of the stage kernel.
+static bool z_split() {
+    static const int v = [] {
+        const char *e = std::getenv("HQT_ZSPLIT");
+        return (e && e[0] == '1') ? 1 : 0;
+    }();
+    return v != 0;
+}
+
+template <typename TD, bool SPLIT>
+static cudaError_t z_stage_fused_v(int mode, const ZStageArgs<double, double, TD> &a,
+                                   const ZOps<double, HQT_ZN> &op, cudaStream_t s) {
+    constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN, SPLIT>();
     switch (mode) {
 #define HQT_ZS(M)                                                                            \
     case M:                                                                                  \
-        k_zstage<double, double, TD, HQT_ZN, M>                                              \
-            <<<z_stage_grid<TD, M>(a.plane), kZThreads, smem, s>>>(a, op);                          \
+        k_zstage<double, double, TD, HQT_ZN, M, SPLIT>                                       \
+            <<<z_stage_grid<TD, M, SPLIT>(a.plane), kZThreads, smem, s>>>(a, op);            \
         break;
         HQT_ZS(1)
         HQT_ZS(2)
         HQT_ZS(3)
         HQT_ZS(4)
 #undef HQT_ZS
-        case 0:
-            if constexpr (std::is_same<TD, double>::value) {
-                k_zstage<double, double, double, HQT_ZN, 0>
-                    <<<z_stage_grid<double, 0>(a.plane), kZThreads, smem, s>>>(a, op);
-                break;
-            }
-            return cudaErrorInvalidValue;
         default:
             return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template <typename TD>
+static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> &a,
+                                 const ZHost &h, cudaStream_t s) {
+    const ZOps<double, HQT_ZN> op = make_zops(h);
+    if (mode == 0) {
+        if constexpr (std::is_same<TD, double>::value) {
+            constexpr size_t smem = zf_smem_bytes<double, double, double, HQT_ZN>();
+            k_zstage<double, double, double, HQT_ZN, 0>
+                <<<z_stage_grid<double, 0, false>(a.plane), kZThreads, smem, s>>>(a, op);
+            return cudaGetLastError();
+        }
+        return cudaErrorInvalidValue;
+    }
+    return z_split() ? z_stage_fused_v<TD, true>(mode, a, op, s)
+                     : z_stage_fused_v<TD, false>(mode, a, op, s);
 }
 
 template <>

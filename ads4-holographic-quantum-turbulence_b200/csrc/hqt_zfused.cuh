@@ -84,7 +84,11 @@ template <typename V> struct ZTileF {
     __device__ __forceinline__ ZTileF<V> cols(int c) const { return ZTileF<V>{p, c0 + c}; }
 };
 
-template <typename TD, int NZP> struct ZfLayout {
+// SPLIT: the gauge-phase and Psi-phase inputs get separate regions (Gg, Gp)
+// instead of sharing G, so the Psi-phase inputs of a tile can be requested
+// one phase ahead (at the end of the previous tile) and the gauge-phase
+// inputs of the next tile right after this tile's gauge phase.
+template <typename TD, int NZP, bool SPLIT = false> struct ZfLayout {
     static constexpr int L = ZmDims<NZP>::LV * kZTile;
     static constexpr int c = L * 16, r = L * 8;  // complex / pair, real (double)
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
@@ -98,15 +102,16 @@ template <typename TD, int NZP> struct ZfLayout {
     static constexpr int pAT = 0, pDAT = r, pLAP = 2 * r, pDIV = 2 * r + dc;
     static constexpr int pZP = ((pDIV + dr + 15) / 16) * 16, pKP = pZP + c;
     static constexpr int psz = pKP + c;
-    static constexpr int oV = oG + mx(gsz, psz);
+    static constexpr int oGP = SPLIT ? oG + ((gsz + 15) / 16) * 16 : oG;  // Psi-phase region
+    static constexpr int oV = SPLIT ? oGP + psz : oG + mx(gsz, psz);
     // V: dp then S1 (Psi phase); g and S of the gauge phase
     static constexpr int oVG = oV, oVS = oV + c;
     static constexpr int bytes = oV + 2 * c;
 };
 
-template <typename T, typename TS, typename TD, int NZP>
+template <typename T, typename TS, typename TD, int NZP, bool SPLIT = false>
 __host__ __device__ constexpr int zf_smem_bytes() {
-    return ZfLayout<TD, NZP>::bytes;
+    return ZfLayout<TD, NZP, SPLIT>::bytes;
 }
 
 // ---- staging of levels 0..nz-1 of the tile starting at site0 --------------
@@ -169,13 +174,13 @@ __device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double
 
 // T = TS = double (state and arithmetic); TD = double or float (derivative
 // fields of the line passes).
-template <typename T, typename TS, typename TD, int NZP, int MODE>
-__global__ void __launch_bounds__(kZThreads, 3)
+template <typename T, typename TS, typename TD, int NZP, int MODE, bool SPLIT = false>
+__global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
     k_zstage(const __grid_constant__ ZStageArgs<T, TS, TD> a,
              const __grid_constant__ ZOps<T, NZP> op) {
     static_assert(std::is_same<T, double>::value && std::is_same<TS, double>::value,
                   "FP64 columns");
-    using Lay = ZfLayout<TD, NZP>;
+    using Lay = ZfLayout<TD, NZP, SPLIT>;
     using D = ZmDims<NZP>;
     constexpr int MT = D::MT, KS = D::KS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
@@ -213,17 +218,17 @@ __global__ void __launch_bounds__(kZThreads, 3)
     const ZTileF<double2> AXY{reinterpret_cast<double2 *>(sm + Lay::oAXY)};
     const ZTileF<C2<TD>> DXP{reinterpret_cast<C2<TD> *>(sm + Lay::oDXP)};
     const ZTileF<C2<TD>> DYP{reinterpret_cast<C2<TD> *>(sm + Lay::oDYP)};
-    unsigned char *gr = sm + Lay::oG;
+    unsigned char *gr = sm + Lay::oG, *gp = sm + Lay::oGP;
     const ZTileF<C2<TD>> DT{reinterpret_cast<C2<TD> *>(gr + Lay::gDT)};
     const ZTileF<C2<TD>> BF{reinterpret_cast<C2<TD> *>(gr + Lay::gBF)};
     const ZTileF<double2> ZA{reinterpret_cast<double2 *>(gr + Lay::gZA)};
     const ZTileF<double2> KA{reinterpret_cast<double2 *>(gr + Lay::gKA)};
-    const ZTileF<T> AT{reinterpret_cast<T *>(gr + Lay::pAT)};
-    const ZTileF<T> DAT{reinterpret_cast<T *>(gr + Lay::pDAT)};
-    const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(gr + Lay::pLAP)};
-    const ZTileF<TD> DIV{reinterpret_cast<TD *>(gr + Lay::pDIV)};
-    const ZTileF<double2> ZP{reinterpret_cast<double2 *>(gr + Lay::pZP)};
-    const ZTileF<double2> KP{reinterpret_cast<double2 *>(gr + Lay::pKP)};
+    const ZTileF<T> AT{reinterpret_cast<T *>(gp + Lay::pAT)};
+    const ZTileF<T> DAT{reinterpret_cast<T *>(gp + Lay::pDAT)};
+    const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(gp + Lay::pLAP)};
+    const ZTileF<TD> DIV{reinterpret_cast<TD *>(gp + Lay::pDIV)};
+    const ZTileF<double2> ZP{reinterpret_cast<double2 *>(gp + Lay::pZP)};
+    const ZTileF<double2> KP{reinterpret_cast<double2 *>(gp + Lay::pKP)};
     const ZTileF<double2> VC{reinterpret_cast<double2 *>(sm + Lay::oV)};
     const ZTileF<double2> VG{reinterpret_cast<double2 *>(sm + Lay::oVG)};
     const ZTileF<double2> VS{reinterpret_cast<double2 *>(sm + Lay::oVS)};
@@ -245,6 +250,17 @@ __global__ void __launch_bounds__(kZThreads, 3)
         }
     };
 
+    auto stage_psi = [&](long long site0) {
+        zf_real<NZP, T>(AT, a.at, nz, P, site0, tid);
+        zf_real<NZP, T>(DAT, a.dat, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, tid);
+        zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, tid);
+        if (MODE >= 1) {
+            zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, tid);
+            if (kReadK) zf_real<NZP, double2>(KP, a.kpsi, nz, P, site0, tid);
+        }
+    };
+
     // this warp's columns of every tile field
     const auto PSw = PS.cols(cw), AXYw = AXY.cols(cw), VCw = VC.cols(cw), VGw = VG.cols(cw),
                VSw = VS.cols(cw);
@@ -254,13 +270,23 @@ __global__ void __launch_bounds__(kZThreads, 3)
         stage_gauge((long long)blockIdx.x * kZTile);
     }
     cp_commit();
+    // SPLIT: commit groups per tile are (gauge of the next tile), (main of the
+    // next tile), (Psi of the next tile); the Psi group of a tile is the one
+    // left outstanding while its gauge phase runs
+    if (SPLIT) {
+        if ((long long)blockIdx.x < ntiles) stage_psi((long long)blockIdx.x * kZTile);
+        cp_commit();
+    }
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long site0 = tile * kZTile;
         const long long next = tile + gridDim.x;
         const long long sw0 = site0 + cw;   // this warp's first column
         const long long site = sw0 + q;     // this lane's column in C layout
-        cp_wait<0>();
+        if (SPLIT)
+            cp_wait<1>();  // main and gauge inputs; the Psi inputs may be in flight
+        else
+            cp_wait<0>();
         __syncthreads();  // every thread's copies are in
 
         // ---- F3, F4: both gauge components at once -------------------------
@@ -336,16 +362,13 @@ __global__ void __launch_bounds__(kZThreads, 3)
                 }
             }
         }
-        __syncthreads();  // every warp is done with G: the Psi inputs refill it
+        __syncthreads();  // every warp is done with G: it refills
 
         // ---- Psi ---------------------------------------------------------------
-        zf_real<NZP, T>(AT, a.at, nz, P, site0, tid);
-        zf_real<NZP, T>(DAT, a.dat, nz, P, site0, tid);
-        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, tid);
-        zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, tid);
-        if (MODE >= 1) {
-            zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, tid);
-            if (kReadK) zf_real<NZP, double2>(KP, a.kpsi, nz, P, site0, tid);
+        if (SPLIT) {  // the next tile's gauge inputs (its Psi inputs came earlier)
+            if (next < ntiles) stage_gauge(next * kZTile);
+        } else {
+            stage_psi(site0);
         }
         cp_commit();
         {  // dp = Lz Psi
@@ -354,7 +377,10 @@ __global__ void __launch_bounds__(kZThreads, 3)
 #pragma unroll
             for (int m = 0; m < MT; ++m) VC(8 * m + g, cw + q) = make_double2(c[m][0], c[m][1]);
         }
-        cp_wait<0>();
+        if (SPLIT)
+            cp_wait<1>();  // this tile's Psi inputs; the next gauge group may be in flight
+        else
+            cp_wait<0>();
         __syncthreads();  // every thread's copies are in
         // boundary row of F2: kb = Lz(nz,:) div A of column q, in every lane
         T kb = T(0);
@@ -447,8 +473,13 @@ __global__ void __launch_bounds__(kZThreads, 3)
                     a.wrho[sl] = a.zrho[sl] - (TS(1) / TS(6)) * (a.krho[sl] + k);
             }
         }
-        __syncthreads();  // every warp is done with G: the next tile refills it
-        if (next < ntiles) stage_gauge(next * kZTile);
+        __syncthreads();  // every warp is done with G (Gp): the next tile refills it
+        if (next < ntiles) {
+            if (SPLIT)
+                stage_psi(next * kZTile);
+            else
+                stage_gauge(next * kZTile);
+        }
         cp_commit();
     }
     cp_wait<0>();

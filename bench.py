@@ -236,7 +236,9 @@ def run_ours(args, w, ws, rank, local):
     state = hqt.seed.init_driven(nx, ny, nz, prof, noise=w["noise"], amplitude=w["amp"],
                                  seed=w["seed"] + rank)
     sim = hqt.Simulation(nx, ny, nz, Lx=w["L"], Ly=w["L"], mu=w["mu"], vy=w["vy"],
-                         dt=w["dt"], remove_winding=w["remove_winding"], device=dev)
+                         dt=w["dt"], remove_winding=w["remove_winding"], device=dev,
+                         autotune=True)
+    geometry = sim.config_report()
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)  # graph capture needs a non-default stream
     T = [api.to_device(a, dev) for a in state]
@@ -273,7 +275,7 @@ def run_ours(args, w, ws, rank, local):
         Tm = [api.to_device(a, dev) for a in state]
         with hqt.Simulation(nx, ny, nz, Lx=w["L"], Ly=w["L"], mu=w["mu"], vy=w["vy"],
                             dt=w["dt"], remove_winding=w["remove_winding"], device=dev,
-                            precision="mixed") as simm:
+                            precision="mixed", autotune=True) as simm:
             simm.step_device(*Tm, nsteps=max(args.warmup, 3))
             torch.cuda.synchronize()
             if ws > 1:
@@ -388,6 +390,7 @@ def run_ours(args, w, ws, rank, local):
                 "data": "synthetic (Newton stationary profile + seeded complex noise)",
                 "config": bench_config(args.workload, w, ws),
                 "gpu_launches": launches, "roofline": roofline,
+                "line_geometry": geometry.get("chosen"),
                 "step_hbm": {"alg_bytes_per_site": STEP_BYTES_FP64, "achieved_gbs": step_gbs,
                              "frac": step_gbs / peak},
                 "kernel_breakdown": breakdown, "mixed_precision": mixed,
@@ -417,7 +420,8 @@ def run_ensemble(args, ws, rank, local):
                                   amplitude=r["amp"], seed=r["seed"])
         sims.append(hqt.Simulation(r["nx"], r["ny"], r["nz"], Lx=r["L"], Ly=r["L"],
                                    mu=r["mu"], vy=r["vy"], dt=r["dt"],
-                                   remove_winding=r["remove_winding"], device=local))
+                                   remove_winding=r["remove_winding"], device=local,
+                                   autotune=True))
         T.append([api.to_device(a, local) for a in st])
     ens = hqt.Ensemble(sims)
     ens.step_device(T, nsteps=max(args.warmup, 3))
