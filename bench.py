@@ -237,7 +237,7 @@ def run_ours(args, w, ws, rank, local):
                                  seed=w["seed"] + rank)
     sim = hqt.Simulation(nx, ny, nz, Lx=w["L"], Ly=w["L"], mu=w["mu"], vy=w["vy"],
                          dt=w["dt"], remove_winding=w["remove_winding"], device=dev,
-                         autotune=True)
+                         autotune=not args.no_autotune)
     geometry = sim.config_report()
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)  # graph capture needs a non-default stream
@@ -275,7 +275,7 @@ def run_ours(args, w, ws, rank, local):
         Tm = [api.to_device(a, dev) for a in state]
         with hqt.Simulation(nx, ny, nz, Lx=w["L"], Ly=w["L"], mu=w["mu"], vy=w["vy"],
                             dt=w["dt"], remove_winding=w["remove_winding"], device=dev,
-                            precision="mixed", autotune=True) as simm:
+                            precision="mixed", autotune=not args.no_autotune) as simm:
             simm.step_device(*Tm, nsteps=max(args.warmup, 3))
             torch.cuda.synchronize()
             if ws > 1:
@@ -421,7 +421,7 @@ def run_ensemble(args, ws, rank, local):
         sims.append(hqt.Simulation(r["nx"], r["ny"], r["nz"], Lx=r["L"], Ly=r["L"],
                                    mu=r["mu"], vy=r["vy"], dt=r["dt"],
                                    remove_winding=r["remove_winding"], device=local,
-                                   autotune=True))
+                                   autotune=not args.no_autotune))
         T.append([api.to_device(a, local) for a in st])
     ens = hqt.Ensemble(sims)
     ens.step_device(T, nsteps=max(args.warmup, 3))
@@ -487,6 +487,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-array leg")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision variant")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default line-pass geometry (no tuning launches)")
     args = ap.parse_args()
     sys.path.insert(0, str(ROOT))
     if args.workload == "ensemble32":
