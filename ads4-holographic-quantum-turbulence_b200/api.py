@@ -199,6 +199,10 @@ class Simulation:
         code = self._lib.hqt_step_device(self._ctx, *ptrs, int(nsteps),
                                          ctypes.byref(d))
         info = self._info(d, buf)
+        if code == _lib.HQT_ENONFINITE:
+            err = NonfiniteEvolution(code, self._lib.hqt_last_error(self._ctx).decode())
+            err.info = info
+            raise err
         self._check(code)
         return info
 

@@ -79,12 +79,28 @@ template <typename TD, int M, bool SPLIT> static int z_stage_grid(long long plan
     return (int)(tiles < full ? tiles : full);
 }
 
-// HQT_ZSPLIT=1 selects the split-region variant of the stage kernel.
-static bool z_split() {
-    static const int v = [] {
+// The split-region stage kernel (separate shared regions for the gauge- and
+// Psi-phase inputs, each requested a phase ahead) when it keeps at least two
+// blocks per SM: at nz <= 21 it does (87 KB of tiles) and measured 136 vs
+// 165 us per stage at 301x301x21; at nz = 25 and 33 it would hold one block
+// per SM.  HQT_ZSPLIT=0/1 forces either variant (for measurements).
+template <typename TD> static bool z_use_split() {
+    static int v = -1;
+    if (v < 0) {
         const char *e = std::getenv("HQT_ZSPLIT");
-        return (e && e[0] == '1') ? 1 : 0;
-    }();
+        if (e && (e[0] == '0' || e[0] == '1')) {
+            v = e[0] == '1';
+        } else {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm, k_zstage<double, double, TD, HQT_ZN, 2, true>, kZThreads,
+                    zf_smem_bytes<double, double, TD, HQT_ZN, true>()) != cudaSuccess) {
+                cudaGetLastError();
+                per_sm = 0;
+            }
+            v = per_sm >= 2;
+        }
+    }
     return v != 0;
 }
 
@@ -122,8 +138,8 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
         }
         return cudaErrorInvalidValue;
     }
-    return z_split() ? z_stage_fused_v<TD, true>(mode, a, op, s)
-                     : z_stage_fused_v<TD, false>(mode, a, op, s);
+    return z_use_split<TD>() ? z_stage_fused_v<TD, true>(mode, a, op, s)
+                             : z_stage_fused_v<TD, false>(mode, a, op, s);
 }
 
 template <>

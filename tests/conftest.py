@@ -58,3 +58,10 @@ def cuda(hqt):
     import torch
     torch.cuda.init()
     return torch
+
+
+@pytest.fixture(scope="session")
+def dev(cuda, hqt):
+    """(to_device, from_device) of the package's API."""
+    api = importlib.import_module(hqt.__name__ + ".api")
+    return api.to_device, api.from_device

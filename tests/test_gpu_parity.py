@@ -40,13 +40,6 @@ def random_fields(nx, ny, nz, seed, amp=1.0):
     return Z1, 6.0 + smooth(s), 0.3 * smooth(s), 0.3 * smooth(s)
 
 
-@pytest.fixture(scope="module")
-def dev(cuda, hqt):
-    from importlib import import_module
-    api = import_module(hqt.__name__ + ".api")
-    return api.to_device, api.from_device
-
-
 GRIDS = [(33, 33, 10), (64, 64, 21), (48, 40, 17), (30, 22, 12), (53, 59, 8),
          (128, 96, 25), (301, 40, 8)]
 

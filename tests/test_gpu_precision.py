@@ -70,7 +70,7 @@ def run(hqt, state, cfg, prec, marks, engine=None):
     return obs0, out
 
 
-def compare(a, b, q0, gauge_fields):
+def compare(a, b, gauge_fields):
     """Deviation of run a from run b (both dicts of one mark)."""
     fa, fb = a["fields"], b["fields"]
     gauge = np.linalg.norm(fb[1].ravel())
@@ -97,8 +97,8 @@ def report(hqt, name, state, cfg, marks, alt_engine, gauge_fields):
     rows = []
     for k in marks:
         r = {"config": name, "steps": k,
-             "mixed_vs_fp64": compare(m[k], f[k], q0f, gauge_fields),
-             "fp64_engine_spread": compare(g[k], f[k], q0f, gauge_fields),
+             "mixed_vs_fp64": compare(m[k], f[k], gauge_fields),
+             "fp64_engine_spread": compare(g[k], f[k], gauge_fields),
              "charge_drift": {"fp64": (f[k]["obs"]["Q"] - q0f["Q"]) / abs(q0f["Q"]),
                               "mixed": (m[k]["obs"]["Q"] - q0m["Q"]) / abs(q0m["Q"])},
              "alt_engine": alt_engine}
@@ -112,19 +112,23 @@ def report(hqt, name, state, cfg, marks, alt_engine, gauge_fields):
 
 
 def check(rows):
-    short, long_ = rows[0], rows[-1]
-    mv = short["mixed_vs_fp64"]
-    assert max(mv["field"].values()) <= 1e-6, mv["field"]
-    assert max(mv["spectrum_rel_l2"].values()) <= 1e-6
-    assert abs(mv["Q_rel"]) <= 1e-6 and abs(mv["E_kin_rel"]) <= 1e-6
-    mv, sp = long_["mixed_vs_fp64"], long_["fp64_engine_spread"]
-    bar = max(1e-6, 10 * max(sp["field"].values()))
-    assert max(mv["field"].values()) <= bar, (mv["field"], sp["field"])
-    sbar = max(1e-6, 10 * max(sp["spectrum_rel_l2"].values()))
-    assert max(mv["spectrum_rel_l2"].values()) <= sbar
-    # the charge is conserved to roundoff in both precisions
-    assert abs(long_["charge_drift"]["fp64"]) <= 1e-12
-    assert abs(long_["charge_drift"]["mixed"]) <= 1e-6
+    """The 1e-6 field bar after 100 steps; everything else, at every mark,
+    within 10x of the FP64 engine spread or 1e-6, whichever is larger (the
+    spectrum measures the fluctuations about the mean flow, so its relative
+    deviation is the field's divided by their small size)."""
+    short = rows[0]
+    assert max(short["mixed_vs_fp64"]["field"].values()) <= 1e-6, short["mixed_vs_fp64"]["field"]
+    for r in rows:
+        mv, sp = r["mixed_vs_fp64"], r["fp64_engine_spread"]
+        bar = max(1e-6, 10 * max(sp["field"].values()))
+        assert max(mv["field"].values()) <= bar, (r["steps"], mv["field"], sp["field"])
+        sbar = max(1e-6, 10 * max(sp["spectrum_rel_l2"].values()))
+        assert max(mv["spectrum_rel_l2"].values()) <= sbar, (r["steps"], mv, sp)
+        ebar = max(1e-6, 10 * abs(sp["E_kin_rel"]))
+        assert abs(mv["E_kin_rel"]) <= ebar
+        # the charge is conserved to roundoff in both precisions
+        assert abs(r["charge_drift"]["fp64"]) <= 1e-12
+        assert abs(r["charge_drift"]["mixed"]) <= 1e-6
 
 
 def test_mixed_precision_driven301(hqt, cuda):
