@@ -197,7 +197,10 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     using D = PfaDims<P, Q>;
     using L_t = PfaLines<T, P, Q>;
     constexpr int H = (P - 1) / 2;
-    PfaWarp<T, P, Q> w;
+    // stage-A fragments out of registers: in FP64 the column-pair phase
+    // holds four spectra per lane, and the kernel drops from 253 to 166
+    // registers; in FP32 the 3xTF32 hi/lo fragments are 48 registers
+    PfaWarp<T, P, Q, true> w;
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);

@@ -1,6 +1,5 @@
 // hqt_z_impl.cuh -- launchers of the column kernels for one column length
 // HQT_ZN (each hqt_z<N>.cu defines HQT_ZN and includes this file).
-#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -48,14 +47,6 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 2>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 3>);
     opt((const void *)k_zstage<double, double, float, HQT_ZN, 4>);
-    opt((const void *)k_zstage<double, double, double, HQT_ZN, 1, true>);
-    opt((const void *)k_zstage<double, double, double, HQT_ZN, 2, true>);
-    opt((const void *)k_zstage<double, double, double, HQT_ZN, 3, true>);
-    opt((const void *)k_zstage<double, double, double, HQT_ZN, 4, true>);
-    opt((const void *)k_zstage<double, double, float, HQT_ZN, 1, true>);
-    opt((const void *)k_zstage<double, double, float, HQT_ZN, 2, true>);
-    opt((const void *)k_zstage<double, double, float, HQT_ZN, 3, true>);
-    opt((const void *)k_zstage<double, double, float, HQT_ZN, 4, true>);
     opt((const void *)k_zcons_tc<HQT_ZN>);
     return e;
 }
@@ -63,15 +54,15 @@ template <> cudaError_t z_init<HQT_ZN>(int max_smem) {
 // One fused launch per stage (hqt_zfused.cuh): persistent blocks of kZWarps
 // warps, as many as fit on the device at once, each looping over tiles of
 // kZTile columns.
-template <typename TD, int M, bool SPLIT> static int z_stage_grid(long long plane) {
+template <typename TD, int M> static int z_stage_grid(long long plane) {
     static int per_sm = 0, nsm = 0;
     if (per_sm == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, k_zstage<double, double, TD, HQT_ZN, M, SPLIT>, kZThreads,
-            zf_smem_bytes<double, double, TD, HQT_ZN, SPLIT>());
+            &per_sm, k_zstage<double, double, TD, HQT_ZN, M>, kZThreads,
+            zf_smem_bytes<double, double, TD, HQT_ZN>());
         if (per_sm < 1) per_sm = 1;
     }
     const long long tiles = (plane + kZTile - 1) / kZTile;
@@ -79,40 +70,15 @@ template <typename TD, int M, bool SPLIT> static int z_stage_grid(long long plan
     return (int)(tiles < full ? tiles : full);
 }
 
-// The split-region stage kernel (separate shared regions for the gauge- and
-// Psi-phase inputs, each requested a phase ahead) when it keeps at least two
-// blocks per SM: at nz <= 21 it does (87 KB of tiles) and measured 136 vs
-// 165 us per stage at 301x301x21; at nz = 25 and 33 it would hold one block
-// per SM.  HQT_ZSPLIT=0/1 forces either variant (for measurements).
-template <typename TD> static bool z_use_split() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = std::getenv("HQT_ZSPLIT");
-        if (e && (e[0] == '0' || e[0] == '1')) {
-            v = e[0] == '1';
-        } else {
-            int per_sm = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    &per_sm, k_zstage<double, double, TD, HQT_ZN, 2, true>, kZThreads,
-                    zf_smem_bytes<double, double, TD, HQT_ZN, true>()) != cudaSuccess) {
-                cudaGetLastError();
-                per_sm = 0;
-            }
-            v = per_sm >= 2;
-        }
-    }
-    return v != 0;
-}
-
-template <typename TD, bool SPLIT>
+template <typename TD>
 static cudaError_t z_stage_fused_v(int mode, const ZStageArgs<double, double, TD> &a,
                                    const ZOps<double, HQT_ZN> &op, cudaStream_t s) {
-    constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN, SPLIT>();
+    constexpr size_t smem = zf_smem_bytes<double, double, TD, HQT_ZN>();
     switch (mode) {
 #define HQT_ZS(M)                                                                            \
     case M:                                                                                  \
-        k_zstage<double, double, TD, HQT_ZN, M, SPLIT>                                       \
-            <<<z_stage_grid<TD, M, SPLIT>(a.plane), kZThreads, smem, s>>>(a, op);            \
+        k_zstage<double, double, TD, HQT_ZN, M>                                              \
+            <<<z_stage_grid<TD, M>(a.plane), kZThreads, smem, s>>>(a, op);            \
         break;
         HQT_ZS(1)
         HQT_ZS(2)
@@ -133,13 +99,12 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
         if constexpr (std::is_same<TD, double>::value) {
             constexpr size_t smem = zf_smem_bytes<double, double, double, HQT_ZN>();
             k_zstage<double, double, double, HQT_ZN, 0>
-                <<<z_stage_grid<double, 0, false>(a.plane), kZThreads, smem, s>>>(a, op);
+                <<<z_stage_grid<double, 0>(a.plane), kZThreads, smem, s>>>(a, op);
             return cudaGetLastError();
         }
         return cudaErrorInvalidValue;
     }
-    return z_use_split<TD>() ? z_stage_fused_v<TD, true>(mode, a, op, s)
-                             : z_stage_fused_v<TD, false>(mode, a, op, s);
+    return z_stage_fused_v<TD>(mode, a, op, s);
 }
 
 template <>

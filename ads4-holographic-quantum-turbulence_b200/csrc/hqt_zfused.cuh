@@ -84,11 +84,14 @@ template <typename V> struct ZTileF {
     __device__ __forceinline__ ZTileF<V> cols(int c) const { return ZTileF<V>{p, c0 + c}; }
 };
 
-// SPLIT: the gauge-phase and Psi-phase inputs get separate regions (Gg, Gp)
-// instead of sharing G, so the Psi-phase inputs of a tile can be requested
-// one phase ahead (at the end of the previous tile) and the gauge-phase
-// inputs of the next tile right after this tile's gauge phase.
-template <typename TD, int NZP, bool SPLIT = false> struct ZfLayout {
+// The gauge-phase and Psi-phase inputs have separate regions (Gg, Gp), so
+// the Psi-phase inputs of a tile are requested one phase ahead (at the end of
+// the previous tile) and the gauge-phase inputs of the next tile right after
+// this tile's gauge phase.  (A shared G region, one fewer region and three
+// blocks per SM instead of two at nz = 21, left both loads exposed: 165
+// against 136 us per stage at 301x301x21, 0.99 against 0.92 ms at
+// 512x512x25.)
+template <typename TD, int NZP> struct ZfLayout {
     static constexpr int L = ZmDims<NZP>::LV * kZTile;
     static constexpr int c = L * 16, r = L * 8;  // complex / pair, real (double)
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
@@ -102,16 +105,16 @@ template <typename TD, int NZP, bool SPLIT = false> struct ZfLayout {
     static constexpr int pAT = 0, pDAT = r, pLAP = 2 * r, pDIV = 2 * r + dc;
     static constexpr int pZP = ((pDIV + dr + 15) / 16) * 16, pKP = pZP + c;
     static constexpr int psz = pKP + c;
-    static constexpr int oGP = SPLIT ? oG + ((gsz + 15) / 16) * 16 : oG;  // Psi-phase region
-    static constexpr int oV = SPLIT ? oGP + psz : oG + mx(gsz, psz);
+    static constexpr int oGP = oG + ((gsz + 15) / 16) * 16;  // Psi-phase region
+    static constexpr int oV = oGP + psz;
     // V: dp then S1 (Psi phase); g and S of the gauge phase
     static constexpr int oVG = oV, oVS = oV + c;
     static constexpr int bytes = oV + 2 * c;
 };
 
-template <typename T, typename TS, typename TD, int NZP, bool SPLIT = false>
+template <typename T, typename TS, typename TD, int NZP>
 __host__ __device__ constexpr int zf_smem_bytes() {
-    return ZfLayout<TD, NZP, SPLIT>::bytes;
+    return ZfLayout<TD, NZP>::bytes;
 }
 
 // ---- staging of levels 0..nz-1 of the tile starting at site0 --------------
@@ -174,13 +177,13 @@ __device__ __forceinline__ void zm_pair(const double (&A)[MT][KS], ZTileF<double
 
 // T = TS = double (state and arithmetic); TD = double or float (derivative
 // fields of the line passes).
-template <typename T, typename TS, typename TD, int NZP, int MODE, bool SPLIT = false>
-__global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
+template <typename T, typename TS, typename TD, int NZP, int MODE>
+__global__ void __launch_bounds__(kZThreads, 2)
     k_zstage(const __grid_constant__ ZStageArgs<T, TS, TD> a,
              const __grid_constant__ ZOps<T, NZP> op) {
     static_assert(std::is_same<T, double>::value && std::is_same<TS, double>::value,
                   "FP64 columns");
-    using Lay = ZfLayout<TD, NZP, SPLIT>;
+    using Lay = ZfLayout<TD, NZP>;
     using D = ZmDims<NZP>;
     constexpr int MT = D::MT, KS = D::KS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
@@ -270,23 +273,18 @@ __global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
         stage_gauge((long long)blockIdx.x * kZTile);
     }
     cp_commit();
-    // SPLIT: commit groups per tile are (gauge of the next tile), (main of the
-    // next tile), (Psi of the next tile); the Psi group of a tile is the one
-    // left outstanding while its gauge phase runs
-    if (SPLIT) {
-        if ((long long)blockIdx.x < ntiles) stage_psi((long long)blockIdx.x * kZTile);
-        cp_commit();
-    }
+    // commit groups per tile: (gauge of the next tile), (main of the next
+    // tile), (Psi of the next tile); the Psi group of a tile is the one left
+    // outstanding while its gauge phase runs
+    if ((long long)blockIdx.x < ntiles) stage_psi((long long)blockIdx.x * kZTile);
+    cp_commit();
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long site0 = tile * kZTile;
         const long long next = tile + gridDim.x;
         const long long sw0 = site0 + cw;   // this warp's first column
         const long long site = sw0 + q;     // this lane's column in C layout
-        if (SPLIT)
-            cp_wait<1>();  // main and gauge inputs; the Psi inputs may be in flight
-        else
-            cp_wait<0>();
+        cp_wait<1>();     // main and gauge inputs; the Psi inputs may be in flight
         __syncthreads();  // every thread's copies are in
 
         // ---- F3, F4: both gauge components at once -------------------------
@@ -362,14 +360,11 @@ __global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
                 }
             }
         }
-        __syncthreads();  // every warp is done with G: it refills
+        __syncthreads();  // every warp is done with Gg: it refills
 
         // ---- Psi ---------------------------------------------------------------
-        if (SPLIT) {  // the next tile's gauge inputs (its Psi inputs came earlier)
-            if (next < ntiles) stage_gauge(next * kZTile);
-        } else {
-            stage_psi(site0);
-        }
+        // the next tile's gauge inputs (this tile's Psi inputs came earlier)
+        if (next < ntiles) stage_gauge(next * kZTile);
         cp_commit();
         {  // dp = Lz Psi
             double c[MT][2];
@@ -377,10 +372,7 @@ __global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
 #pragma unroll
             for (int m = 0; m < MT; ++m) VC(8 * m + g, cw + q) = make_double2(c[m][0], c[m][1]);
         }
-        if (SPLIT)
-            cp_wait<1>();  // this tile's Psi inputs; the next gauge group may be in flight
-        else
-            cp_wait<0>();
+        cp_wait<1>();     // this tile's Psi inputs; the next gauge group may be in flight
         __syncthreads();  // every thread's copies are in
         // boundary row of F2: kb = Lz(nz,:) div A of column q, in every lane
         T kb = T(0);
@@ -473,13 +465,8 @@ __global__ void __launch_bounds__(kZThreads, SPLIT ? 2 : 3)
                     a.wrho[sl] = a.zrho[sl] - (TS(1) / TS(6)) * (a.krho[sl] + k);
             }
         }
-        __syncthreads();  // every warp is done with G (Gp): the next tile refills it
-        if (next < ntiles) {
-            if (SPLIT)
-                stage_psi(next * kZTile);
-            else
-                stage_gauge(next * kZTile);
-        }
+        __syncthreads();  // every warp is done with Gp: the next tile refills it
+        if (next < ntiles) stage_psi(next * kZTile);
         cp_commit();
     }
     cp_wait<0>();

@@ -74,3 +74,29 @@ def state_sketches(Z1, Z2, Z3, Z4, rhoi) -> dict:
     """Sketches of the five fields; rhoi by its boundary plane."""
     return dict(Z1=sketch(Z1), Z2=sketch(Z2), Z3=sketch(Z3), Z4=sketch(Z4),
                 rho=sketch(np.asarray(rhoi)[:, :, -1]))
+
+
+LATTICE128 = dict(nx=128, nz=25, L=32.0, mu=6.0, dt=0.02, vortices=26, seed=1,
+                  every=50, max_steps=3000)
+
+
+def lattice_state(prof, w):
+    """The vortex-lattice initial fields of ``seed.init_lattice`` for the
+    configuration ``w`` (bare atan2 imprint, as tevol_lattice.m:109-135)."""
+    import importlib
+    seed = importlib.import_module("ads4-holographic-quantum-turbulence_b200.seed")
+    rng = np.random.default_rng(w["seed"])
+    nv, L = w["vortices"], w["L"]
+    xs, ys = rng.uniform(0, L, nv), rng.uniform(0, L, nv)
+    q = np.r_[np.ones(nv // 2), -np.ones(nv - nv // 2)]
+    return seed.init_lattice(w["nx"], w["nx"], w["nz"], prof, L, L, xs, ys, q,
+                             periodic_images=0)
+
+
+def profile_from(d):
+    """A ``seed.StationaryProfile`` from its stored arrays."""
+    import importlib
+    seed = importlib.import_module("ads4-holographic-quantum-turbulence_b200.seed")
+    z = np.asarray(d["z"])
+    return seed.StationaryProfile(6.0, 0.0, z, np.asarray(d["Z1"]), np.asarray(d["Z2"]),
+                                  np.asarray(d["Vy1"]), np.asarray(d["rhoi"]), 0)
