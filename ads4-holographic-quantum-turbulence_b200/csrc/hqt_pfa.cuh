@@ -276,42 +276,24 @@ template <int P, int Q> struct PfaStageA<float, P, Q> {
     }
 };
 
-// RELOAD: the stage-A fragments are read from the (cached) table at every
-// stage A instead of staying in registers for the kernel's life, which frees
-// their registers for kernels whose other phases need many (the FP64 y pass).
-template <typename T, int P, int Q, bool RELOAD = false> struct PfaWarp {
+template <typename T, int P, int Q> struct PfaWarp {
     using D = PfaDims<P, Q>;
     static constexpr int N = D::N;
-    struct Held {
-        PfaStageA<T, P, Q> sa;
-    };
-    struct Table {
-        const T *frag;
-    };
-    typename std::conditional<RELOAD, Table, Held>::type st;
+    PfaStageA<T, P, Q> sa;
     int lane, g, q;
 
     __device__ __forceinline__ void init(const T *frag) {
         lane = threadIdx.x & 31;
         g = lane >> 2;
         q = lane & 3;
-        if constexpr (RELOAD)
-            st.frag = frag;
-        else
-            st.sa.init(frag, lane);
+        sa.init(frag, lane);
     }
 
     // Stage A along t for every column u of `in`; SIGN -1 forward, +1 inverse.
     // The result X(u, k) goes to put(u, k, re, im) for k = 0..Q-1.
     template <int SIGN, typename Put>
     __device__ __forceinline__ void stage_a(PfaBuf<T> in, Put put) const {
-        if constexpr (RELOAD) {
-            PfaStageA<T, P, Q> sa;
-            sa.init(st.frag, lane);
-            sa.template run<SIGN>(in, put, g, q);
-        } else {
-            st.sa.template run<SIGN>(in, put, g, q);
-        }
+        sa.template run<SIGN>(in, put, g, q);
     }
 
     // Stage B on the CUDA cores, a lane per column (line, k2), in the

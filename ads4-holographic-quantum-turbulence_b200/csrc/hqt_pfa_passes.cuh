@@ -197,10 +197,11 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     using D = PfaDims<P, Q>;
     using L_t = PfaLines<T, P, Q>;
     constexpr int H = (P - 1) / 2;
-    // stage-A fragments out of registers: in FP64 the column-pair phase
-    // holds four spectra per lane, and the kernel drops from 253 to 166
-    // registers; in FP32 the 3xTF32 hi/lo fragments are 48 registers
-    PfaWarp<T, P, Q, true> w;
+    // (Reloading the stage-A fragments at every stage A instead of holding
+    // them took the FP64 kernel from 253 to 166 registers and 8 to 11 warps
+    // per SM, but from 151 to 195 us per launch: the loads sit in front of
+    // every DMMA chain.)
+    PfaWarp<T, P, Q> w;
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
