@@ -300,7 +300,7 @@ int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
         return HQT_OK;
     }
     if (c->cy) {
-        const int nb = ct_lines(c->ny, 3);
+        const int nb = ct_lines_y(c->ny, 3);
         RC(ct_dispatch(c, c->ny, CT_Y_RHS, &a, dim3((c->nx + nb - 1) / nb, c->nz),
                        smem_x(c->ny, 3, nb)));
         return HQT_OK;
@@ -353,7 +353,7 @@ int launch_y_d1(hqt_ctx *c, FieldIn<double> in, const double *add_re, FieldOut<d
         return HQT_OK;
     }
     if (c->cy) {
-        const int nb = ct_lines(c->ny, 2);
+        const int nb = ct_lines_y(c->ny, 2);
         RC(ct_dispatch(c, c->ny, CT_Y_D1, &a, dim3((c->nx + nb - 1) / nb, nsl),
                        smem_x(c->ny, 2, nb)));
         return HQT_OK;
@@ -423,7 +423,7 @@ int launch_y_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *
         return HQT_OK;
     }
     if (c->cy) {
-        const int nb = ct_lines(c->ny, 3, sizeof(float2));
+        const int nb = ct_lines_y(c->ny, 3, sizeof(float2));
         RC(ct_dispatch(c, c->ny, CT_Y_RHS_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),
                        smem_x(c->ny, 3, nb, sizeof(float2))));
         return HQT_OK;
@@ -474,7 +474,7 @@ int launch_d1_32(hqt_ctx *c, bool along_x, const float *in, float *out) {
         return HQT_OK;
     }
     if (c->cy) {
-        const int nb = ct_lines(c->ny, 2, sizeof(float2));
+        const int nb = ct_lines_y(c->ny, 2, sizeof(float2));
         RC(ct_dispatch(c, c->ny, CT_Y_D1_F, &a, dim3((c->nx + nb - 1) / nb, c->nz),
                        smem_x(c->ny, 2, nb, sizeof(float2))));
         return HQT_OK;
@@ -544,7 +544,7 @@ int launch_filter(hqt_ctx *c, int nf, const FieldIn<double> *in, const FieldOut<
         if (c->py) {
             CK(pfa_launch_301(CT_FY, &a, c->nz, c->stream));
         } else if (c->cy) {
-            const int tx = ct_lines(c->ny, 6);
+            const int tx = ct_lines_y(c->ny, 6);
             RC(ct_dispatch(c, c->ny, CT_FY, &a, dim3((c->nx + tx - 1) / tx, c->nz),
                            smem_x(c->ny, 2, 3 * tx)));
         } else {

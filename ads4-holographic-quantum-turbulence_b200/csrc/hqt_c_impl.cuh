@@ -88,7 +88,7 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
         }
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
-            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(double2));
+            constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(double2));
             if (real_field_d1(a.in, a.out))
                 k_y_d1r_c<double, HQT_CN>
                     <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);
@@ -124,7 +124,7 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
         }
         case CT_Y_D1_F: {
             const YD1Args<float> &a = *(const YD1Args<float> *)args;
-            constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(float2));
+            constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(float2));
             if (real_field_d1(a.in, a.out))
                 k_y_d1r_c<float, HQT_CN>
                     <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);

@@ -69,10 +69,20 @@ constexpr int kTabTotal = tab_offset(16) + 16;
 
 // Lines per block of the compile-time line transforms: a block holds
 // (1 + nbuf*NB) lines of N complex values of esize bytes in about 54 KB of
-// shared memory,
-// so that four 128-thread blocks fit on an SM.
+// shared memory, so that four 128-thread blocks fit on an SM.
 __host__ __device__ constexpr int ct_lines(int N, int nbuf, int esize = 16) {
     const int v = ((54 * 1024) / esize / N - 1) / nbuf;
+    return v < 1 ? 1 : (v > 16 ? 16 : v);
+}
+// The same for the y passes, whose lines are NB adjacent columns: FP64 lines
+// of 256 points and more get about 108 KB (two blocks per SM), so that a
+// y-line load reads 64 contiguous bytes or more per row and the radix passes
+// have work for all threads.  Measured at 512x512x25 (FP64): y_rhs 984 ->
+// 859 us, filter_y 611 -> 451 us.  The x passes (contiguous lines) and the
+// FP32 passes were slower with the larger blocks and keep 54 KB.
+__host__ __device__ constexpr int ct_lines_y(int N, int nbuf, int esize = 16) {
+    const int budget = (esize == 16 && N >= 256 ? 108 : 54) * 1024;
+    const int v = (budget / esize / N - 1) / nbuf;
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
 

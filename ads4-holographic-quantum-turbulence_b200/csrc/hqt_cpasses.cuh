@@ -85,7 +85,7 @@ __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
-    constexpr int NB = ct_lines(N, 3, sizeof(C2<T>));
+    constexpr int NB = ct_lines_y(N, 3, sizeof(C2<T>));
     const int x0 = blockIdx.x * NB;
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -183,7 +183,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
-    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
+    constexpr int NB = ct_lines_y(N, 2, sizeof(C2<T>));
     const int x0 = blockIdx.x * NB;
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -235,7 +235,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1r_c(XD1Args<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
-    constexpr int NB = ct_lines(N, 2, sizeof(C2<T>));
+    constexpr int NB = ct_lines_y(N, 2, sizeof(C2<T>));
     const int x0 = blockIdx.x * 2 * NB;
     const int nr = min(2 * NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -298,7 +298,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
-    constexpr int TX = ct_lines(N, 6, sizeof(C2<T>));
+    constexpr int TX = ct_lines_y(N, 6, sizeof(C2<T>));
     constexpr int NB = 3 * TX;  // up to three fields of TX columns
     const int x0 = blockIdx.x * TX;
     const int valid = min(TX, a.nx - x0);

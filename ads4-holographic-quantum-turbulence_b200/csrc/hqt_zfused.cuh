@@ -483,7 +483,9 @@ __global__ void __launch_bounds__(kZThreads, 2)
 // the real fields (div A, cons, v, A_t) pack both sites into one pair tile
 // (x: site 8w+j, y: site 8w+4+j), so the real chain costs one product per 8
 // sites.  Lane (g, q) owns sites 8w+q and 8w+4+q at levels 8m+g.
-constexpr int kZConsTiles = 5;  // pair tiles: PA, PB, div A, two scratch
+// The input tiles (PA, PB, div A) are double-buffered: a tile's inputs are
+// requested while the previous tile computes.
+constexpr int kZConsTiles = 8;  // pair tiles: 2 x (PA, PB, div A), two scratch
 constexpr int kZConsSites = 2 * kZTile;
 template <int NZP>
 __host__ __device__ constexpr int zcons_smem_bytes() {
@@ -516,13 +518,12 @@ __global__ void __launch_bounds__(kZThreads)
         }
     }
     __syncthreads();
-    const ZTileF<double2> PA{sm}, PB{sm + L}, DV{sm + 2 * L}, V1{sm + 3 * L}, V2{sm + 4 * L};
-    const auto PAw = PA.cols(cw), PBw = PB.cols(cw), DVw = DV.cols(cw), V1w = V1.cols(cw),
-               V2w = V2.cols(cw);
+    const ZTileF<double2> V1{sm + 6 * L}, V2{sm + 7 * L};
+    const auto V1w = V1.cols(cw), V2w = V2.cols(cw);
     const long long ntiles = (P + kZConsSites - 1) / kZConsSites;
-#pragma unroll 1
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long site0 = tile * kZConsSites;
+    // inputs of the tile at site0 into buffer set b
+    auto fetch = [&](long long site0, int b) {
+        const ZTileF<double2> PA{sm + 3 * b * L}, PB{sm + (3 * b + 1) * L}, DV{sm + (3 * b + 2) * L};
         // site c of the tile -> pair column 4(c/8) + c%4, half (c/4)%2
 #pragma unroll
         for (int it = 0; it < (NZP * kZConsSites + kZThreads - 1) / kZThreads; ++it) {
@@ -534,9 +535,21 @@ __global__ void __launch_bounds__(kZThreads)
                 cp_async<8>(h ? &DV(l, pc).y : &DV(l, pc).x, a.divA + gi);
             }
         }
+    };
+    if ((long long)blockIdx.x < ntiles) fetch((long long)blockIdx.x * kZConsSites, 0);
+    cp_commit();
+    int buf = 0;
+#pragma unroll 1
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= 1) {
+        const long long site0 = tile * kZConsSites;
+        const long long next = tile + gridDim.x;
+        if (next < ntiles) fetch(next * kZConsSites, buf ^ 1);
         cp_commit();
-        cp_wait<0>();
+        cp_wait<1>();  // this tile's inputs; the next tile's may be in flight
         __syncthreads();
+        const ZTileF<double2> PA{sm + 3 * buf * L}, PB{sm + (3 * buf + 1) * L},
+            DV{sm + (3 * buf + 2) * L};
+        const auto PAw = PA.cols(cw), PBw = PB.cols(cw), DVw = DV.cols(cw);
         const long long sA = site0 + 8 * warp + q, sB = sA + 4;  // this lane's two sites
         const bool okA = sA < P, okB = sB < P;
         {  // cons (levels < nz-1 enter Lzr)
@@ -626,8 +639,9 @@ __global__ void __launch_bounds__(kZThreads)
                 a.ay[gb + sB] = -a.vy;
             }
         }
-        __syncthreads();  // every warp is done with the tiles: the next tile refills them
+        __syncthreads();  // every warp is done with this buffer set: it refills next
     }
+    cp_wait<0>();
 }
 
 }  // namespace hqt
