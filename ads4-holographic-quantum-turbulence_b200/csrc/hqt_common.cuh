@@ -75,13 +75,15 @@ __host__ __device__ constexpr int ct_lines(int N, int nbuf, int esize = 16) {
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
 // The same for the y passes, whose lines are NB adjacent columns: FP64 lines
-// of 256 points and more get about 108 KB (two blocks per SM), so that a
-// y-line load reads 64 contiguous bytes or more per row and the radix passes
-// have work for all threads.  Measured at 512x512x25 (FP64): y_rhs 984 ->
-// 859 us, filter_y 611 -> 451 us.  The x passes (contiguous lines) and the
-// FP32 passes were slower with the larger blocks and keep 54 KB.
+// of 512 points get about 108 KB (two blocks per SM; four lines instead of
+// one), so that a y-line load reads 64 contiguous bytes per row and the radix
+// passes have work for all threads.  Measured at 512x512x25 (FP64): y_rhs
+// 984 -> 835 us, filter_y 611 -> 445 us.  At 256 points (eight lines instead
+// of four) the 32-run ensemble was 9% slower, and the x passes (contiguous
+// lines) and the FP32 passes were slower with the larger blocks: they keep
+// 54 KB.
 __host__ __device__ constexpr int ct_lines_y(int N, int nbuf, int esize = 16) {
-    const int budget = (esize == 16 && N >= 256 ? 108 : 54) * 1024;
+    const int budget = (esize == 16 && N >= 512 ? 108 : 54) * 1024;
     const int v = (budget / esize / N - 1) / nbuf;
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }
