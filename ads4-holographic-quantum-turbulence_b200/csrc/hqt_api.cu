@@ -47,6 +47,10 @@ struct hqt_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // side branch of a step: the A_t derivatives run beside stage 1's line
+    // passes (forked and joined with events on the launch stream)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int nx = 0, ny = 0, nz = 0, NZP = 0;
     long long plane = 0, vol = 0;
     FFTPlan planx{}, plany{};
@@ -698,13 +702,37 @@ int enqueue_convert(hqt_ctx *c) {
     return HQT_OK;
 }
 
+// Run launch() on the side stream, ordered after everything enqueued so far
+// on the launch stream; join_side() orders the launch stream after it.
+// Profiled (eager, event-timed) steps stay on one stream.
+template <typename F> int on_side(hqt_ctx *c, F launch) {
+    if (c->prof_on) return launch();
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    const int r = launch();
+    c->stream = main;
+    RC(r);
+    CK(cudaEventRecord(c->ev_join, c->side));
+    return HQT_OK;
+}
+int join_side(hqt_ctx *c) {
+    if (c->prof_on) return HQT_OK;
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return HQT_OK;
+}
+
 int enqueue_stages_mixed(hqt_ctx *c) {
     double2 *psi = c->cpsi;
     double *at = c->cat, *ax = c->cax, *ay = c->cay;
     // with fused_convert the previous step's filter (or prestep) left them
     if (!c->fused_convert) RC(enqueue_convert(c));
-    RC(launch_d1_32(c, true, c->at32, c->dxat32));
-    RC(launch_d1_32(c, false, c->at32, c->dyat32));
+    // the A_t derivatives beside stage 1's line passes
+    RC(on_side(c, [&]() -> int {
+        RC(launch_d1_32(c, true, c->at32, c->dxat32));
+        return launch_d1_32(c, false, c->at32, c->dyat32);
+    }));
     for (int s = 1; s <= 4; ++s) {
         const int yi = (s == 3) ? 1 : 0, ni = (s == 2) ? 1 : 0;
         const int y32 = (s == 1) ? 2 : yi;
@@ -749,6 +777,7 @@ int enqueue_stages_mixed(hqt_ctx *c) {
         a.way = ay;
         a.wrho = c->rho;
         a.slice_mean = c->slice_mean;
+        if (s == 1) RC(join_side(c));
         RC(launch_zstage_mixed(c, s, a));
     }
     return HQT_OK;
@@ -760,11 +789,14 @@ int enqueue_step(hqt_ctx *c) {
     if (c->mixed) {
         RC(enqueue_stages_mixed(c));
     } else {
-    // A_t is frozen during the four stages: its horizontal derivatives once
-    RC(launch_x_d1(c, FieldIn<double>{nullptr, at, nullptr},
-                   FieldOut<double>{nullptr, c->dxat, nullptr}));
-    RC(launch_y_d1(c, FieldIn<double>{nullptr, at, nullptr}, nullptr,
-                   FieldOut<double>{nullptr, c->dyat, nullptr}));
+    // A_t is frozen during the four stages: its horizontal derivatives once,
+    // beside stage 1's line passes (which do not read them)
+    RC(on_side(c, [&]() -> int {
+        RC(launch_x_d1(c, FieldIn<double>{nullptr, at, nullptr},
+                       FieldOut<double>{nullptr, c->dxat, nullptr}));
+        return launch_y_d1(c, FieldIn<double>{nullptr, at, nullptr}, nullptr,
+                           FieldOut<double>{nullptr, c->dyat, nullptr});
+    }));
     for (int s = 1; s <= 4; ++s) {
         // stage s reads Y[(s-2)&1] (the state itself at s = 1) and writes the
         // next stage input to the other buffer
@@ -806,6 +838,7 @@ int enqueue_step(hqt_ctx *c) {
         a.wax = ax;
         a.way = ay;
         a.wrho = c->rho;
+        if (s == 1) RC(join_side(c));
         switch (s) {
             case 1: RC(launch_zstage<1>(c, a)); break;
             case 2: RC(launch_zstage<2>(c, a)); break;
@@ -1565,6 +1598,12 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         return bail(HQT_ECUDA);
     }
     c->stream = c->own_stream;
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        c->err = "stream or event creation failed";
+        return bail(HQT_ECUDA);
+    }
 
     // radial operators: Lz = 2*chebdif(nz,1), Lz1 = inv(Lz(1:nz-1,1:nz-1))
     {
@@ -1782,6 +1821,10 @@ void hqt_destroy(hqt_ctx *c) {
         cudaEventDestroy(e.b);
     }
     for (void *q : c->allocs) cudaFree(q);
+    if (c->side) cudaStreamSynchronize(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
