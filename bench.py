@@ -40,6 +40,9 @@ WORKLOADS = {
                   remove_winding=True, noise="complex", amp=1e-3, seed=0),
     "lattice512": dict(nx=512, ny=512, nz=25, L=128.0, mu=6.0, vy=0.0, dt=0.02,
                        remove_winding=False, noise="complex", amp=1e-3, seed=1),
+    # the large single run's grid: 1024x1024x33, L = 256, dt = 0.01
+    "large1024": dict(nx=1024, ny=1024, nz=33, L=256.0, mu=6.0, vy=0.0, dt=0.01,
+                      remove_winding=True, noise="complex", amp=1e-3, seed=2),
 }
 
 # The batched-ensemble workload: 32 independent runs, grids {128,192,256}^2,
