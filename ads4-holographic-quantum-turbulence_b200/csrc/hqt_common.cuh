@@ -82,8 +82,14 @@ __host__ __device__ constexpr int ct_lines(int N, int nbuf, int esize = 16) {
 // of four) the 32-run ensemble was 9% slower, and the x passes (contiguous
 // lines) and the FP32 passes were slower with the larger blocks: they keep
 // 54 KB.
+// At 1024 points 128 KB holds two FP64 lines of the y pass (one line left a
+// warp's y load 32 rows wide), and 108 KB four FP32 lines.
 __host__ __device__ constexpr int ct_lines_y(int N, int nbuf, int esize = 16) {
-    const int budget = (esize == 16 && N >= 512 ? 108 : 54) * 1024;
+    const int budget = (esize == 16 && N >= 1024   ? 128
+                        : esize == 16 && N >= 512 ? 108
+                        : esize == 8 && N >= 1024 ? 108
+                                                  : 54) *
+                       1024;
     const int v = (budget / esize / N - 1) / nbuf;
     return v < 1 ? 1 : (v > 16 ? 16 : v);
 }

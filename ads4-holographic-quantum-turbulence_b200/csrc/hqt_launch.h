@@ -69,7 +69,7 @@ cudaError_t z_misc(const ZColArgs<double> &a, const ZHost &h, int grid, int thre
 // Compile-time column lengths of this build; a run uses the smallest >= nz.
 #define HQT_NZP_LIST(X) X(8) X(12) X(16) X(17) X(21) X(25) X(33)
 // Line lengths with compile-time transforms; other lengths use hqt_fft.cuh.
-#define HQT_CN_LIST(X) X(33) X(64) X(128) X(192) X(256) X(301) X(512)
+#define HQT_CN_LIST(X) X(33) X(64) X(128) X(192) X(256) X(301) X(512) X(1024)
 
 namespace hqt {
 #define HQT_ZDECL(N)                                                                       \

@@ -41,7 +41,7 @@ def random_fields(nx, ny, nz, seed, amp=1.0):
 
 
 GRIDS = [(33, 33, 10), (64, 64, 21), (48, 40, 17), (30, 22, 12), (53, 59, 8),
-         (128, 96, 25), (301, 40, 8)]
+         (128, 96, 25), (301, 40, 8), (1024, 24, 5), (20, 1024, 5), (512, 36, 6)]
 
 
 @pytest.mark.parametrize("nx,ny,nz", GRIDS)
