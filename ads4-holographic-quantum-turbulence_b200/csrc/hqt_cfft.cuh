@@ -85,13 +85,45 @@ template <> struct BigTab<float> {
 };
 
 constexpr int kCtThreads = 128;
+
+// Shared-memory view of the compile-time engine's buffers.  When N is a
+// multiple of G = 128 bytes / element (8 complex doubles, 16 complex floats),
+// element e of the dynamic shared memory lives at e XOR ((e/G) mod G) XOR
+// ((e/G^2) mod G): a permutation inside each 128-byte row, so accesses to
+// consecutive elements stay conflict-free, while the strided writes of the
+// first Stockham pass (butterfly j writes (j*R + k)*NB + b: rows R*NB
+// elements apart) spread over the banks instead of hitting the same ones
+// (8- and 16-way conflicts at R = 8, 16 with one line per block).  Buffers
+// start at multiples of N, so the permutation stays inside each buffer.
+template <typename T, int N> __host__ __device__ constexpr bool ct_swizzled() {
+    return N % (128 / (int)sizeof(C2<T>)) == 0;
+}
+template <typename T, int N> struct CtView {
+    int base;
+    __device__ __forceinline__ C2<T> &operator[](int i) const {
+        int e = base + i;
+        if constexpr (ct_swizzled<T, N>()) {
+            constexpr int G = 128 / (int)sizeof(C2<T>);
+            e ^= ((e / G) & (G - 1)) ^ ((e / (G * G)) & (G - 1));
+        }
+        return reinterpret_cast<C2<T> *>(g_smem)[e];
+    }
+};
+template <typename T, int N> __device__ __forceinline__ CtView<T, N> ctv(int buf) {
+    return CtView<T, N>{buf};
+}
+
+// the twiddle table into buffer `roots`
+template <typename T, int N>
+__device__ __forceinline__ void ct_load_roots(int roots, const C2<T> *g) {
+    const CtView<T, N> s = ctv<T, N>(roots);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = g[i];
+}
 constexpr int kCtKB = 6;  // output pairs per warp task of a large odd radix
 
 template <typename T, int N, int NB, int R, int Ns>
 __device__ __forceinline__ void ct_small(int src, int dst, int roots, int sign) {
-    const C2<T> *S = sptr<T>(src);
-    C2<T> *D = sptr<T>(dst);
-    const C2<T> *W = sptr<T>(roots);
+    const CtView<T, N> S = ctv<T, N>(src), D = ctv<T, N>(dst), W = ctv<T, N>(roots);
     constexpr int nR = N / R;
     constexpr int TOTAL = NB * nR;
     constexpr int qs = N / (Ns * R);
@@ -118,9 +150,7 @@ __device__ __forceinline__ void ct_small(int src, int dst, int roots, int sign) 
 
 template <typename T, int N, int NB, int R, int Ns>
 __device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
-    C2<T> *S = sptr<T>(src);
-    C2<T> *D = sptr<T>(dst);
-    const C2<T> *W = sptr<T>(roots);
+    const CtView<T, N> S = ctv<T, N>(src), D = ctv<T, N>(dst), W = ctv<T, N>(roots);
     constexpr int nR = N / R;
     constexpr int M = (R - 1) / 2;
     constexpr int qs = N / (Ns * R);
@@ -246,8 +276,7 @@ __device__ __forceinline__ int ct_fft(int a, int b, int roots) {
 // dst = m(k) src over the batch (order 1: i*s1*k, order 2: s2*k^2)
 template <typename T, int N, int NB, int ORDER>
 __device__ __forceinline__ void ct_deriv(int dst, int src, T s1, T s2) {
-    const C2<T> *S = sptr<T>(src);
-    C2<T> *D = sptr<T>(dst);
+    const CtView<T, N> S = ctv<T, N>(src), D = ctv<T, N>(dst);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int e = t / NB;
         const T kk = T(2 * e < N ? e : (2 * e > N ? e - N : 0));

@@ -14,7 +14,7 @@ namespace hqt {
 // x lines: NB consecutive (y, z) rows, contiguous in global memory
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cx_load(int buf, int valid, F get) {
-    C2<T> *s = sptr<T>(buf);
+    const CtView<T, N> s = ctv<T, N>(buf);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int b = t / N, e = t - b * N;
         s[e * NB + b] = (b < valid) ? get(t) : mk2<T>(T(0), T(0));
@@ -22,7 +22,7 @@ __device__ __forceinline__ void cx_load(int buf, int valid, F get) {
 }
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cx_store(int buf, int valid, F put) {
-    const C2<T> *s = sptr<T>(buf);
+    const CtView<T, N> s = ctv<T, N>(buf);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int b = t / N, e = t - b * N;
         if (b < valid) put(t, s[e * NB + b]);
@@ -31,7 +31,7 @@ __device__ __forceinline__ void cx_store(int buf, int valid, F put) {
 // y lines: NB adjacent columns of one z slice; element (y, b) at y*NB + b
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zoff, F get) {
-    C2<T> *s = sptr<T>(buf);
+    const CtView<T, N> s = ctv<T, N>(buf);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int y = t / NB, b = t - y * NB;
         s[t] = (b < valid) ? get(zoff + (long long)y * nx + b) : mk2<T>(T(0), T(0));
@@ -39,7 +39,7 @@ __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zo
 }
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long zoff, F put) {
-    const C2<T> *s = sptr<T>(buf);
+    const CtView<T, N> s = ctv<T, N>(buf);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int y = t / NB, b = t - y * NB;
         if (b < valid) put(zoff + (long long)y * nx + b, s[t]);
@@ -53,7 +53,7 @@ __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
     const long long g0 = (long long)L0 * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     cx_load<T, N, NB>(A, valid, [&](int t) { return a.psi[g0 + t]; });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -90,7 +90,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     // Psi: d_y and d_yy
     cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return a.psi[g]; });
     __syncthreads();
@@ -117,7 +117,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     __syncthreads();
     const int SE = ct_fft<T, N, NB, -1>(C, F1, R);      // E spectrum in C or F1
     {
-        C2<T> *sc = sptr<T>(SC), *se = sptr<T>(SE);
+        const CtView<T, N> sc = ctv<T, N>(SC), se = ctv<T, N>(SE);
         const T h = T(0.5);
         for (int t = threadIdx.x; t < (N / 2 + 1) * NB; t += kCtThreads) {
             const int b = t % NB, k = t / NB;
@@ -151,7 +151,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     const int F3 = (P1 == SC) ? F2 : SC;
     const int P2 = ct_fft<T, N, NB, +1>(SE, F3, R);
     {
-        const C2<T> *s1 = sptr<T>(P1), *s2 = sptr<T>(P2);
+        const CtView<T, N> s1 = ctv<T, N>(P1), s2 = ctv<T, N>(P2);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
             const int y = t / NB, b = t - y * NB;
             if (b < valid) {
@@ -171,7 +171,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     cx_load<T, N, NB>(A, valid, [&](int t) { return load_field(a.in, g0 + t); });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -188,7 +188,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
     const int valid = min(NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return load_field(a.in, g); });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -213,7 +213,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1r_c(XD1Args<T> a) {
     constexpr int R = 0, A = N, B = N + NB * N;
     const T *src = a.in.re + (long long)L0 * N;
     T *dst = a.out.re + (long long)L0 * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     cx_load<T, N, NB>(A, valid, [&](int t) {
         const int j = t / N, e = t - j * N;
         const int r0 = 2 * j, r1 = r0 + 1;
@@ -240,9 +240,9 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     const int nr = min(2 * NB, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     {  // the layout of cy_load: element (y, j) at y*NB + j
-        C2<T> *sa = sptr<T>(A);
+        const CtView<T, N> sa = ctv<T, N>(A);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
             const int y = t / NB, j = t - y * NB;
             const int r0 = 2 * j, r1 = r0 + 1;
@@ -255,7 +255,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
     __syncthreads();
     const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
-    const C2<T> *sr = sptr<T>(r);
+    const CtView<T, N> sr = ctv<T, N>(r);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int y = t / NB, j = t - y * NB;
         const int r0 = 2 * j, r1 = r0 + 1;
@@ -273,7 +273,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     const int w = a.st ? a.st->winding : 0;
     for (int f = 0; f < a.nf; ++f) {
         cx_load<T, N, NB>(A, valid, [&](int t) {
@@ -304,9 +304,9 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     const int valid = min(TX, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     {
-        C2<T> *s = sptr<T>(A);
+        const CtView<T, N> s = ctv<T, N>(A);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
             const int bb = t % NB, y = t / NB;
             const int f = bb / TX, b = bb % TX;
@@ -317,7 +317,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
     {
-        C2<T> *s = sptr<T>(X);
+        const CtView<T, N> s = ctv<T, N>(X);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
             const int bb = t % NB, ky = t / NB;
             const int kx = x0 + min(bb % TX, valid - 1);
@@ -328,7 +328,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     }
     __syncthreads();
     const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
-    const C2<T> *s = sptr<T>(r);
+    const CtView<T, N> s = ctv<T, N>(r);
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int bb = t % NB, y = t / NB;
         const int f = bb / TX, b = bb % TX;
@@ -343,7 +343,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
     const int valid = min(NB, a.nlines - L0);
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
-    load_roots<T>(R, a.roots, N);
+    ct_load_roots<T, N>(R, a.roots);
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
     int mybad = 0;

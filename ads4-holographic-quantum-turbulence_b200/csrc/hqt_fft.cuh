@@ -57,9 +57,9 @@ template <int BITS> __host__ __device__ constexpr int bitrev(int i) {
 }
 
 // Power-of-two radix: iterative radix-2 DIT on bit-reversed registers.
-template <typename T, int R>
-__device__ __forceinline__ void dft_pow2_store(C2<T> (&v)[R], C2<T> *D, int a0,
-                                               int ks, int sign) {
+template <typename T, int R, typename DV>
+__device__ __forceinline__ void dft_pow2_store(C2<T> (&v)[R], DV D, int a0, int ks,
+                                               int sign) {
     constexpr int LOG = Log2<R>::v;
     constexpr int off = tab_offset(R);
 #pragma unroll
@@ -100,9 +100,9 @@ __device__ __forceinline__ void dft_pow2_store(C2<T> (&v)[R], C2<T> *D, int a0,
 
 // Odd prime radix: X[k] = x0 + sum_j a_j cos(2pi jk/R) -+ i sum_j b_j sin(..),
 // a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}; outputs k and R-k share the sums.
-template <typename T, int R>
-__device__ __forceinline__ void dft_odd_store(C2<T> (&v)[R], C2<T> *D, int a0,
-                                              int ks, int sign) {
+template <typename T, int R, typename DV>
+__device__ __forceinline__ void dft_odd_store(C2<T> (&v)[R], DV D, int a0, int ks,
+                                              int sign) {
     constexpr int M = (R - 1) / 2;
     constexpr int off = tab_offset(R);
 #pragma unroll
@@ -137,9 +137,9 @@ __device__ __forceinline__ void dft_odd_store(C2<T> (&v)[R], C2<T> *D, int a0,
     }
 }
 
-template <typename T, int R>
-__device__ __forceinline__ void dft_store(C2<T> (&v)[R], C2<T> *D, int a0, int ks,
-                                          int sign) {
+// D: a shared-memory pointer, or a view with the same subscript (CtView)
+template <typename T, int R, typename DV>
+__device__ __forceinline__ void dft_store(C2<T> (&v)[R], DV D, int a0, int ks, int sign) {
     if constexpr ((R & (R - 1)) == 0)
         dft_pow2_store<T, R>(v, D, a0, ks, sign);
     else
