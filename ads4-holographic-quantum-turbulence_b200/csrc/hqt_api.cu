@@ -112,6 +112,9 @@ struct hqt_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+    // programmatic dependent launch of the step's kernels (HQT_PDL=0 turns
+    // it off); cleared if a step graph with it cannot be built
+    bool pdl = true;
     // profiling: CUDA events around every launch (graphs are bypassed)
     bool prof_on = false;
     bool capturing = false;
@@ -129,6 +132,7 @@ struct hqt_ctx {
 };
 
 static thread_local std::string g_create_err;
+thread_local bool hqt::g_pdl = false;
 
 namespace {
 
@@ -673,9 +677,11 @@ int launch_zcol_misc(hqt_ctx *c, const double *at, double *dat, const double2 *p
 
 int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
     Prof pr(c, K_WIND, 2);
-    k_wind_partial<<<kPartials, kRedThreads, 0, c->stream>>>(O, c->nx, c->ny, c->partial);
+    (void)klaunch(k_wind_partial, dim3(kPartials), dim3(kRedThreads), 0, c->stream, O, c->nx, c->ny,
+                  c->partial);
     CK(cudaGetLastError());
-    k_wind_final<<<1, kRedThreads, 0, c->stream>>>(c->partial, kPartials, c->ny, c->st, out);
+    (void)klaunch(k_wind_final, dim3(1), dim3(kRedThreads), 0, c->stream, c->partial, kPartials,
+                  c->ny, c->st, out);
     CK(cudaGetLastError());
     return HQT_OK;
 }
@@ -689,15 +695,15 @@ int launch_winding(hqt_ctx *c, const double2 *O, int *out) {
 // slice means of the state and its FP32 stage-1 copies (mixed precision)
 int enqueue_convert(hqt_ctx *c) {
     Prof pr(c, K_CONVERT, 3);
-    k_slice_partials<<<dim3(kSliceChunks, c->nz), kRedThreads, 0, c->stream>>>(
-        c->cpsi, c->cat, c->cax, c->cay, c->plane, c->slice_partial);
+    (void)klaunch(k_slice_partials, dim3(kSliceChunks, c->nz), dim3(kRedThreads), 0, c->stream,
+                  c->cpsi, c->cat, c->cax, c->cay, c->plane, c->slice_partial);
     CK(cudaGetLastError());
-    k_slice_finalize<<<(5 * c->nz + 127) / 128, 128, 0, c->stream>>>(
-        c->slice_partial, c->nz, c->plane, c->slice_mean);
+    (void)klaunch(k_slice_finalize, dim3((5 * c->nz + 127) / 128), dim3(128), 0, c->stream,
+                  c->slice_partial, c->nz, c->plane, c->slice_mean);
     CK(cudaGetLastError());
-    k_state_to_f32<<<592, 256, 0, c->stream>>>(c->cpsi, c->cat, c->cax, c->cay, c->plane,
-                                              c->vol, c->slice_mean, c->ypsi32[2], c->at32,
-                                              c->yax32[2], c->yay32[2]);
+    (void)klaunch(k_state_to_f32, dim3(592), dim3(256), 0, c->stream, c->cpsi, c->cat, c->cax,
+                  c->cay, c->plane, c->vol, c->slice_mean, c->ypsi32[2], c->at32, c->yax32[2],
+                  c->yay32[2]);
     CK(cudaGetLastError());
     return HQT_OK;
 }
@@ -783,7 +789,15 @@ int enqueue_stages_mixed(hqt_ctx *c) {
     return HQT_OK;
 }
 
+// Sets g_pdl for the launches made while it lives.
+struct PdlScope {
+    bool old;
+    explicit PdlScope(bool on) : old(g_pdl) { g_pdl = on; }
+    ~PdlScope() { g_pdl = old; }
+};
+
 int enqueue_step(hqt_ctx *c) {
+    const PdlScope pdl_scope(c->pdl);
     double2 *psi = c->cpsi;
     double *at = c->cat, *ax = c->cax, *ay = c->cay;
     if (c->mixed) {
@@ -860,12 +874,13 @@ int enqueue_step(hqt_ctx *c) {
         RC(launch_filter(c, 3, in, out, c->p.remove_winding != 0, true, c->fused_convert));
     } else if (c->p.remove_winding) {
         Prof pr(c, K_PHASE);
-        k_phase_multiply<<<592, 256, 0, c->stream>>>(psi, c->nx, c->ny, c->vol, c->st);
+        (void)klaunch(k_phase_multiply, dim3(592), dim3(256), 0, c->stream, psi, c->nx, c->ny,
+                      c->vol, c->st);
         CK(cudaGetLastError());
     }
     {
         Prof pr(c, K_STEP_END);
-        k_step_end<<<1, 32, 0, c->stream>>>(c->st);
+        (void)klaunch(k_step_end, dim3(1), dim3(32), 0, c->stream, c->st);
         CK(cudaGetLastError());
     }
     return HQT_OK;
@@ -921,8 +936,20 @@ int build_graph(hqt_ctx *c) {
     if (c->gexec && std::memcmp(key, c->graph_key, sizeof(key)) == 0) return HQT_OK;
     drop_graph(c);
     CK(cudaGraphCreate(&c->graph, 0));
-    RC(add_guarded_step(c, c->graph));
-    CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+    int r = add_guarded_step(c, c->graph);
+    cudaError_t e = (r == HQT_OK) ? cudaGraphInstantiate(&c->gexec, c->graph, 0) : cudaSuccess;
+    if (c->pdl && (r != HQT_OK || e != cudaSuccess)) {
+        // programmatic edges refused inside the conditional body: build the
+        // step again with plain stream order
+        cudaGetLastError();
+        drop_graph(c);
+        c->pdl = false;
+        CK(cudaGraphCreate(&c->graph, 0));
+        r = add_guarded_step(c, c->graph);
+        e = (r == HQT_OK) ? cudaGraphInstantiate(&c->gexec, c->graph, 0) : cudaSuccess;
+    }
+    RC(r);
+    CK(e);
     std::memcpy(c->graph_key, key, sizeof(key));
     return HQT_OK;
 }
@@ -1748,6 +1775,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     c->cy = ct_supported(p.ny);
     c->px = pfa_length(p.nx);
     c->py = pfa_length(p.ny);
+    if (const char *env = std::getenv("HQT_PDL")) c->pdl = std::string(env) != "0";
     if (const char *env = std::getenv("HQT_LINE_ENGINE")) {
         // "runtime" forces the runtime-plan engine, "stockham" the
         // compile-time Stockham engine (the tests cover all three)
@@ -1925,8 +1953,10 @@ int hqt_profile(hqt_ctx *c, int enable) {
 
 int hqt_config_report(hqt_ctx *c, char *buf, int64_t len) {
     if (!c || !buf || len <= 0) return HQT_EINVAL;
-    if ((int64_t)c->tune_json.size() + 1 > len) return fail(c, HQT_EINVAL, "report buffer too small");
-    std::memcpy(buf, c->tune_json.c_str(), c->tune_json.size() + 1);
+    const std::string rep =
+        std::string("{\"pdl\": ") + (c->pdl ? "true" : "false") + ", " + c->tune_json.substr(1);
+    if ((int64_t)rep.size() + 1 > len) return fail(c, HQT_EINVAL, "report buffer too small");
+    std::memcpy(buf, rep.c_str(), rep.size() + 1);
     return HQT_OK;
 }
 
@@ -2183,14 +2213,28 @@ int build_ensemble_graph(hqt_ensemble *e) {
     std::vector<const void *> key;
     for (hqt_ctx *c : e->m) key.insert(key.end(), {c->cpsi, c->cat, c->cax, c->cay});
     if (e->gexec && key == e->key) return HQT_OK;
-    drop_ensemble_graph(e);
-    EK(cudaGraphCreate(&e->graph, 0));
-    for (size_t i = 0; i < e->m.size(); ++i) {
-        hqt_ctx *c = e->m[i];
-        const int r = add_guarded_step(c, e->graph);
-        if (r != HQT_OK) return efail(e, r, "member " + std::to_string(i) + ": " + c->err);
+    for (int attempt = 0;; ++attempt) {
+        drop_ensemble_graph(e);
+        EK(cudaGraphCreate(&e->graph, 0));
+        int r = HQT_OK;
+        size_t i = 0;
+        for (; i < e->m.size() && r == HQT_OK; ++i) r = add_guarded_step(e->m[i], e->graph);
+        const cudaError_t ce =
+            (r == HQT_OK) ? cudaGraphInstantiate(&e->gexec, e->graph, 0) : cudaSuccess;
+        bool any_pdl = false;
+        for (hqt_ctx *c : e->m) any_pdl = any_pdl || c->pdl;
+        if ((r != HQT_OK || ce != cudaSuccess) && attempt == 0 && any_pdl) {
+            // programmatic edges refused inside the conditional bodies: build
+            // every member's step again with plain stream order
+            cudaGetLastError();
+            for (hqt_ctx *c : e->m) c->pdl = false;
+            continue;
+        }
+        if (r != HQT_OK)
+            return efail(e, r, "member " + std::to_string(i - 1) + ": " + e->m[i - 1]->err);
+        EK(ce);
+        break;
     }
-    EK(cudaGraphInstantiate(&e->gexec, e->graph, 0));
     e->key = key;
     return HQT_OK;
 }

@@ -71,65 +71,71 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
     constexpr int T = kCtThreads;
     switch (kind) {
         case CT_X_RHS:
-            k_x_rhs_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const XRhsArgs<double> *)args);
+            (void)klaunch(k_x_rhs_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const XRhsArgs<double> *)args);
             break;
         case CT_Y_RHS:
-            k_y_rhs_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<double> *)args);
+            (void)klaunch(k_y_rhs_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const YRhsArgs<double> *)args);
             break;
         case CT_X_D1: {
             const XD1Args<double> &a = *(const XD1Args<double> *)args;
             constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(double2));
             if (real_field_d1(a.in, a.out))
-                k_x_d1r_c<double, HQT_CN>
-                    <<<(a.nlines + nb2 - 1) / nb2, T, smem, s>>>(a);
+                (void)klaunch(k_x_d1r_c<double, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2), dim3(T),
+                              smem, s, a);
             else
-                k_x_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(a);
+                (void)klaunch(k_x_d1_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
             break;
         }
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
             constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(double2));
             if (real_field_d1(a.in, a.out))
-                k_y_d1r_c<double, HQT_CN>
-                    <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);
+                (void)klaunch(k_y_d1r_c<double, HQT_CN>, dim3((a.nx + nb2 - 1) / nb2, grid.y),
+                              dim3(T), smem, s, a);
             else
-                k_y_d1_c<double, HQT_CN><<<grid, T, smem, s>>>(a);
+                (void)klaunch(k_y_d1_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
             break;
         }
         case CT_FX_FWD:
-            k_x_filt_fwd_c<double, HQT_CN>
-                <<<grid, T, smem, s>>>(*(const XFiltFwdArgs<double> *)args);
+            (void)klaunch(k_x_filt_fwd_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const XFiltFwdArgs<double> *)args);
             break;
         case CT_FY:
-            k_y_filt_c<double, HQT_CN><<<grid, T, smem, s>>>(*(const YFiltArgs<double> *)args);
+            (void)klaunch(k_y_filt_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const YFiltArgs<double> *)args);
             break;
         case CT_FX_INV:
-            k_x_filt_inv_c<double, HQT_CN>
-                <<<grid, T, smem, s>>>(*(const XFiltInvArgs<double> *)args);
+            (void)klaunch(k_x_filt_inv_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const XFiltInvArgs<double> *)args);
             break;
         case CT_X_RHS_F:
-            k_x_rhs_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const XRhsArgs<float> *)args);
+            (void)klaunch(k_x_rhs_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const XRhsArgs<float> *)args);
             break;
         case CT_Y_RHS_F:
-            k_y_rhs_c<float, HQT_CN><<<grid, T, smem, s>>>(*(const YRhsArgs<float> *)args);
+            (void)klaunch(k_y_rhs_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s,
+                          *(const YRhsArgs<float> *)args);
             break;
         case CT_X_D1_F: {
             const XD1Args<float> &a = *(const XD1Args<float> *)args;
             constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(float2));
             if (real_field_d1(a.in, a.out))
-                k_x_d1r_c<float, HQT_CN><<<(a.nlines + nb2 - 1) / nb2, T, smem, s>>>(a);
+                (void)klaunch(k_x_d1r_c<float, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2), dim3(T),
+                              smem, s, a);
             else
-                k_x_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(a);
+                (void)klaunch(k_x_d1_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
             break;
         }
         case CT_Y_D1_F: {
             const YD1Args<float> &a = *(const YD1Args<float> *)args;
             constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(float2));
             if (real_field_d1(a.in, a.out))
-                k_y_d1r_c<float, HQT_CN>
-                    <<<dim3((a.nx + nb2 - 1) / nb2, grid.y), T, smem, s>>>(a);
+                (void)klaunch(k_y_d1r_c<float, HQT_CN>, dim3((a.nx + nb2 - 1) / nb2, grid.y),
+                              dim3(T), smem, s, a);
             else
-                k_y_d1_c<float, HQT_CN><<<grid, T, smem, s>>>(a);
+                (void)klaunch(k_y_d1_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
             break;
         }
         default:
@@ -154,64 +160,75 @@ cudaError_t pfa_launch_301(int kind, const void *args, int nlines, cudaStream_t 
     };
     switch (kind) {
         case CT_X_RHS:
-            k_x_rhs_pfa<double, P, Q><<<grid, 32, smem, s>>>(*(const XRhsArgs<double> *)args);
+            (void)klaunch(k_x_rhs_pfa<double, P, Q>, dim3(grid), dim3(32), smem, s,
+                          *(const XRhsArgs<double> *)args);
             break;
         case CT_Y_RHS: {
             const YRhsArgs<double> &a = *(const YRhsArgs<double> *)args;
-            k_y_rhs_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
+            (void)klaunch(k_y_rhs_pfa<double, P, Q>, dim3(ygrid(a.nx, nlines)), dim3(32), smem, s,
+                          a);
             break;
         }
         case CT_X_D1: {
             const XD1Args<double> &a = *(const XD1Args<double> *)args;
             if (real_field_d1(a.in, a.out))
-                k_x_d1r_pfa<double, P, Q><<<rgrid, 32, smem, s>>>(a);
+                (void)klaunch(k_x_d1r_pfa<double, P, Q>, dim3(rgrid), dim3(32), smem, s, a);
             else
-                k_x_d1_pfa<double, P, Q><<<grid, 32, smem, s>>>(a);
+                (void)klaunch(k_x_d1_pfa<double, P, Q>, dim3(grid), dim3(32), smem, s, a);
             break;
         }
         case CT_Y_D1: {
             const YD1Args<double> &a = *(const YD1Args<double> *)args;
             if (real_field_d1(a.in, a.out))
-                k_y_d1r_pfa<double, P, Q><<<yrgrid(a.nx, nlines), 32, smem, s>>>(a);
+                (void)klaunch(k_y_d1r_pfa<double, P, Q>, dim3(yrgrid(a.nx, nlines)), dim3(32), smem,
+                              s, a);
             else
-                k_y_d1_pfa<double, P, Q><<<ygrid(a.nx, nlines), 32, smem, s>>>(a);
+                (void)klaunch(k_y_d1_pfa<double, P, Q>, dim3(ygrid(a.nx, nlines)), dim3(32), smem,
+                              s, a);
             break;
         }
         case CT_X_RHS_F:
-            k_x_rhs_pfa<float, P, Q><<<grid, 32, smem32, s>>>(*(const XRhsArgs<float> *)args);
+            (void)klaunch(k_x_rhs_pfa<float, P, Q>, dim3(grid), dim3(32), smem32, s,
+                          *(const XRhsArgs<float> *)args);
             break;
         case CT_Y_RHS_F: {
             const YRhsArgs<float> &a = *(const YRhsArgs<float> *)args;
-            k_y_rhs_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
+            (void)klaunch(k_y_rhs_pfa<float, P, Q>, dim3(ygrid(a.nx, nlines)), dim3(32), smem32, s,
+                          a);
             break;
         }
         case CT_X_D1_F: {
             const XD1Args<float> &a = *(const XD1Args<float> *)args;
             if (real_field_d1(a.in, a.out))
-                k_x_d1r_pfa<float, P, Q><<<rgrid, 32, smem32, s>>>(a);
+                (void)klaunch(k_x_d1r_pfa<float, P, Q>, dim3(rgrid), dim3(32), smem32, s, a);
             else
-                k_x_d1_pfa<float, P, Q><<<grid, 32, smem32, s>>>(a);
+                (void)klaunch(k_x_d1_pfa<float, P, Q>, dim3(grid), dim3(32), smem32, s, a);
             break;
         }
         case CT_Y_D1_F: {
             const YD1Args<float> &a = *(const YD1Args<float> *)args;
             if (real_field_d1(a.in, a.out))
-                k_y_d1r_pfa<float, P, Q><<<yrgrid(a.nx, nlines), 32, smem32, s>>>(a);
+                (void)klaunch(k_y_d1r_pfa<float, P, Q>, dim3(yrgrid(a.nx, nlines)), dim3(32),
+                              smem32, s, a);
             else
-                k_y_d1_pfa<float, P, Q><<<ygrid(a.nx, nlines), 32, smem32, s>>>(a);
+                (void)klaunch(k_y_d1_pfa<float, P, Q>, dim3(ygrid(a.nx, nlines)), dim3(32), smem32,
+                              s, a);
             break;
         }
         case CT_FX_FWD:
-            k_x_filt_fwd_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XFiltFwdArgs<double> *)args);
+            (void)klaunch(k_x_filt_fwd_pfa<P, Q>, dim3(grid), dim3(32), smem, s,
+                          *(const XFiltFwdArgs<double> *)args);
             break;
         case CT_FY: {
             const YFiltArgs<double> &a = *(const YFiltArgs<double> *)args;
-            k_y_filt_pfa<P, Q>
-                <<<dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines, a.nf), 32, smem, s>>>(a);
+            (void)klaunch(k_y_filt_pfa<P, Q>,
+                          dim3((a.nx + kPfaLines - 1) / kPfaLines, nlines, a.nf), dim3(32), smem, s,
+                          a);
             break;
         }
         case CT_FX_INV:
-            k_x_filt_inv_pfa<P, Q><<<grid, 32, smem, s>>>(*(const XFiltInvArgs<double> *)args);
+            (void)klaunch(k_x_filt_inv_pfa<P, Q>, dim3(grid), dim3(32), smem, s,
+                          *(const XFiltInvArgs<double> *)args);
             break;
         default:
             return cudaErrorInvalidValue;

@@ -95,6 +95,20 @@ __host__ __device__ constexpr int ct_lines_y(int N, int nbuf, int esize = 16) {
 }
 
 #ifdef __CUDACC__
+// Programmatic dependent launch.  A kernel of the step is launched with
+// programmatic stream serialization (klaunch in hqt_launch.h), so it may be
+// scheduled before the kernel before it in the stream has finished and its
+// writes are flushed.  Each such kernel calls pdl_wait() before it touches
+// any global memory that another kernel of the step writes or reads; only
+// its preamble (operator fragments and twiddles from tables written at
+// context creation, zeroed shared memory) runs before the wait, which
+// returns once every prerequisite grid has completed and its writes are
+// visible.  A no-op in a kernel launched without the attribute.  No kernel
+// triggers its dependents early (griddepcontrol.launch_dependents): at
+// 301x301x21 that made the step graph 1.83 -> 2.17 ms, the early blocks
+// sitting on SM resources while they wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // angle(a./b) as atan2 of a*conj(b) (same argument; |b|^2 > 0 only rescales),
 // with every product and sum rounded on its own so that all count paths give
 // the same bits.

@@ -54,6 +54,7 @@ __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
     constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
     const long long g0 = (long long)L0 * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     cx_load<T, N, NB>(A, valid, [&](int t) { return a.psi[g0 + t]; });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -91,6 +92,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N, C = N + 2 * NB * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     // Psi: d_y and d_yy
     cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return a.psi[g]; });
     __syncthreads();
@@ -172,6 +174,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1_c(XD1Args<T> a) {
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     cx_load<T, N, NB>(A, valid, [&](int t) { return load_field(a.in, g0 + t); });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -189,6 +192,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     cy_load<T, N, NB>(A, valid, a.nx, zoff, [&](long long g) { return load_field(a.in, g); });
     __syncthreads();
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
@@ -214,6 +218,7 @@ __global__ void HQT_CT_BOUNDS k_x_d1r_c(XD1Args<T> a) {
     const T *src = a.in.re + (long long)L0 * N;
     T *dst = a.out.re + (long long)L0 * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     cx_load<T, N, NB>(A, valid, [&](int t) {
         const int j = t / N, e = t - j * N;
         const int r0 = 2 * j, r1 = r0 + 1;
@@ -241,6 +246,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     {  // the layout of cy_load: element (y, j) at y*NB + j
         const CtView<T, N> sa = ctv<T, N>(A);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
@@ -274,6 +280,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     const int w = a.st ? a.st->winding : 0;
     for (int f = 0; f < a.nf; ++f) {
         cx_load<T, N, NB>(A, valid, [&](int t) {
@@ -305,6 +312,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     {
         const CtView<T, N> s = ctv<T, N>(A);
         for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
@@ -344,6 +352,7 @@ __global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
     constexpr int R = 0, A = N, B = N + NB * N;
     const long long g0 = (long long)L0 * N;
     ct_load_roots<T, N>(R, a.roots);
+    pdl_wait();
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
     int mybad = 0;

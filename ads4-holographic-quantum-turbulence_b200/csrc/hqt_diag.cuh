@@ -17,6 +17,7 @@ constexpr int kRedThreads = 256;
 // partial[blockIdx.x] = sum over this block's sites of angle(O(x,y+1)/O(x,y))
 __global__ void __launch_bounds__(kRedThreads)
     k_wind_partial(const double2 *O, int nx, int ny, double *partial) {
+    pdl_wait();
     __shared__ double sh[kRedThreads];
     const long long n = (long long)nx * ny;
     double acc = 0.0;
@@ -43,6 +44,7 @@ __device__ __forceinline__ double round_half_away(double v) {
 
 __global__ void __launch_bounds__(kRedThreads)
     k_wind_final(const double *partial, int nparts, int ny, DevStatus *st, int *out) {
+    pdl_wait();
     __shared__ double sh[kRedThreads];
     double acc = 0.0;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += partial[i];
@@ -92,6 +94,7 @@ __global__ void __launch_bounds__(kRedThreads)
 // Psi *= exp(-2 pi i y w / ny) over all z (winding removal without filter).
 __global__ void k_phase_multiply(double2 *psi, int nx, int ny, long long vol,
                                  const DevStatus *st) {
+    pdl_wait();
     const int w = st->winding;
     if (w == 0) return;
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
@@ -113,6 +116,7 @@ constexpr int kSliceChunks = 32;
 __global__ void __launch_bounds__(kRedThreads)
     k_slice_partials(const double2 *psi, const double *at, const double *ax,
                      const double *ay, long long plane, double *partial) {
+    pdl_wait();
     __shared__ double sh[5][kRedThreads];
     const long long off = (long long)blockIdx.y * plane;
     const long long per = (plane + kSliceChunks - 1) / kSliceChunks;
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 __global__ void k_slice_finalize(const double *partial, int nz, long long plane, double *mean) {
+    pdl_wait();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (z, field)
     if (t >= 5 * nz) return;
     const int z = t / 5, f = t % 5;
@@ -154,6 +159,7 @@ __global__ void k_state_to_f32(const double2 *psi, const double *at, const doubl
                                const double *ay, long long plane, long long vol,
                                const double *mean, float2 *psi32, float *at32, float *ax32,
                                float *ay32) {
+    pdl_wait();
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < vol;
          s += (long long)gridDim.x * blockDim.x) {
         const double *m = mean + 5 * (s / plane);
@@ -187,6 +193,7 @@ __global__ void k_step_guard(cudaGraphConditionalHandle h, const DevStatus *st) 
 }
 
 __global__ void k_step_end(DevStatus *st) {
+    pdl_wait();
     if (threadIdx.x == 0 && blockIdx.x == 0) st->step += 1;
 }
 

@@ -38,54 +38,54 @@ cudaError_t fft_init(const double *tc, const double *ts, int ntab, int max_smem)
 
 
 cudaError_t launch_x_rhs(const XRhsArgs<double> &a, int grid, size_t smem, cudaStream_t s) {
-    k_x_rhs<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_rhs<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_rhs(const YRhsArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_rhs<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_rhs<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_x_d1(const XD1Args<double> &a, int grid, size_t smem, cudaStream_t s) {
-    k_x_d1<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_d1<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_d1(const YD1Args<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_d1<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_d1<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_x_filt_fwd(const XFiltFwdArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s) {
-    k_x_filt_fwd<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_filt_fwd<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_filt(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_filt<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_filt<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_x_filt_inv(const XFiltInvArgs<double> &a, int grid, size_t smem,
                               cudaStream_t s) {
-    k_x_filt_inv<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_filt_inv<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_x_rhs_f(const XRhsArgs<float> &a, int grid, size_t smem, cudaStream_t s) {
-    k_x_rhs<float><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_rhs<float>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_rhs_f(const YRhsArgs<float> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_rhs<float><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_rhs<float>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_x_d1_f(const XD1Args<float> &a, int grid, size_t smem, cudaStream_t s) {
-    k_x_d1<float><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_x_d1<float>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_d1_f(const YD1Args<float> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_d1<float><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_d1<float>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 cudaError_t launch_y_fwd(const YFiltArgs<double> &a, dim3 grid, size_t smem, cudaStream_t s) {
-    k_y_fwd<double><<<grid, 128, smem, s>>>(a);
+    (void)klaunch(k_y_fwd<double>, dim3(grid), dim3(128), smem, s, a);
     return cudaGetLastError();
 }
 

@@ -1,8 +1,35 @@
 // hqt_launch.h -- host entry points of the kernel translation units.
 #pragma once
+#include <cuda_runtime.h>
+
+#include <utility>
+
 #include "hqt_args.h"
 
 namespace hqt {
+
+// Launches of the step's kernels carry programmatic stream serialization
+// while g_pdl is set (the context sets it on its own thread while it
+// enqueues or captures a step): a kernel's blocks may then be scheduled
+// before the previous kernel in the stream has finished, and wait for it in
+// pdl_wait() (hqt_common.cuh).  Every kernel launched through klaunch calls
+// pdl_wait() before its first access to memory that other kernels touch.
+extern thread_local bool g_pdl;
+template <typename... P, typename... A>
+cudaError_t klaunch(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                    A &&...args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = g_pdl ? 1u : 0u;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 
 // Radial operators on the host (row-major): Lz (nz x nz), Lz1 ((nz-1)^2), zz.
 struct ZHost {

@@ -132,6 +132,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_rhs(XRhsArgs<T> a) {
     const int R = 0, A = n, B = n + a.NB * n, C = n + 2 * a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     // ---- Psi ----
     xl_load<T>(A, n, nb, [&](int t) { return a.psi[g0 + t]; });
     __syncthreads();
@@ -175,6 +176,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_rhs(YRhsArgs<T> a) {
     const int R = 0, A0 = n, A1 = n + a.TX * n, A2 = n + 2 * a.TX * n;
     const int P = n, Q = n + 2 * a.TX * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     // ---- Psi: d_y and d_yy ----
     yl_load<T>(A0, n, nb, a.nx, zoff, [&](long long g) { return a.psi[g]; });
     __syncthreads();
@@ -268,6 +270,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_d1(XD1Args<T> a) {
     const int R = 0, A = n, B = n + a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     xl_load<T>(A, n, nb, [&](int t) { return load_field(a.in, g0 + t); });
     __syncthreads();
     int X = fft_run<T>(A, B, R, a.plan, nb, -1);
@@ -285,6 +288,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_d1(YD1Args<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const int R = 0, A = n, B = n + a.TX * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     yl_load<T>(A, n, nb, a.nx, zoff, [&](long long g) { return load_field(a.in, g); });
     __syncthreads();
     int X = fft_run<T>(A, B, R, a.plan, nb, -1);
@@ -309,6 +313,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_fwd(XFiltFwdArgs<T
     const int R = 0, A = n, B = n + a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     const int w = a.st ? a.st->winding : 0;
     for (int f = 0; f < a.nf; ++f) {
         xl_load<T>(A, n, nb, [&](int t) {
@@ -339,6 +344,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_filt(YFiltArgs<T> a) {
     const int nbl = nb * a.nf;
     const int R = 0, A = n, B = n + a.TX * a.nf * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     const int tot = nbl * n;
     {
         C2<T> *s = sptr<T>(A);
@@ -379,6 +385,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_inv(XFiltInvArgs<T
     const int R = 0, A = n, B = n + a.NB * n;
     const long long g0 = (long long)L0 * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
     int mybad = 0;
@@ -410,6 +417,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_fwd(YFiltArgs<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const int R = 0, A = n, B = n + a.TX * n;
     load_roots<T>(R, a.roots, n);
+    pdl_wait();
     for (int f = 0; f < a.nf; ++f) {
         C2<T> *spec = a.spec[f];
         yl_load<T>(A, n, nb, a.nx, zoff, [&](long long g) { return spec[g]; });

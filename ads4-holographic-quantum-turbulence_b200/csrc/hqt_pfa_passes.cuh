@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const L_t L(min(kPfaLines, a.nx - x0));
@@ -405,6 +407,7 @@ __global__ void __launch_bounds__(32) k_x_d1_pfa(const __grid_constant__ XD1Args
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -430,6 +433,7 @@ __global__ void __launch_bounds__(32) k_y_d1_pfa(const __grid_constant__ YD1Args
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const L_t L(min(kPfaLines, a.nx - x0));
@@ -465,6 +469,7 @@ __global__ void __launch_bounds__(32) k_x_d1r_pfa(const __grid_constant__ XD1Arg
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int R0 = blockIdx.x * kPfaRealLines;
     const int nr = min(kPfaRealLines, a.nlines - R0);  // real lines inside the grid
     const L_t L((nr + 1) / 2);
@@ -502,6 +507,7 @@ __global__ void __launch_bounds__(32) k_y_d1r_pfa(const __grid_constant__ YD1Arg
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int x0 = blockIdx.x * kPfaRealLines;
     const int nr = min(kPfaRealLines, a.nx - x0);  // columns inside the grid
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
@@ -549,6 +555,7 @@ __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ X
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));
@@ -601,6 +608,7 @@ __global__ void __launch_bounds__(32) k_y_filt_pfa(const __grid_constant__ YFilt
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int x0 = blockIdx.x * kPfaLines;
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     L_t L(min(kPfaLines, a.nx - x0));
@@ -663,6 +671,7 @@ __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ X
     w.init(pfa_frag<T>());
     T cs[2][P];
     pfa_twiddles<T, P>(cs);
+    pdl_wait();
     const int L0 = blockIdx.x * kPfaLines;
     const long long g0 = (long long)L0 * N;
     const L_t L(min(kPfaLines, a.nlines - L0));

@@ -77,8 +77,8 @@ static cudaError_t z_stage_fused_v(int mode, const ZStageArgs<double, double, TD
     switch (mode) {
 #define HQT_ZS(M)                                                                            \
     case M:                                                                                  \
-        k_zstage<double, double, TD, HQT_ZN, M>                                              \
-            <<<z_stage_grid<TD, M>(a.plane), kZThreads, smem, s>>>(a, op);            \
+        (void)klaunch(k_zstage<double, double, TD, HQT_ZN, M>,                               \
+                      dim3(z_stage_grid<TD, M>(a.plane)), dim3(kZThreads), smem, s, a, op); \
         break;
         HQT_ZS(1)
         HQT_ZS(2)
@@ -98,8 +98,9 @@ static cudaError_t z_stage_fused(int mode, const ZStageArgs<double, double, TD> 
     if (mode == 0) {
         if constexpr (std::is_same<TD, double>::value) {
             constexpr size_t smem = zf_smem_bytes<double, double, double, HQT_ZN>();
-            k_zstage<double, double, double, HQT_ZN, 0>
-                <<<z_stage_grid<double, 0>(a.plane), kZThreads, smem, s>>>(a, op);
+            (void)klaunch(k_zstage<double, double, double, HQT_ZN, 0>,
+                          dim3(z_stage_grid<double, 0>(a.plane)), dim3(kZThreads), smem, s, a,
+                          op);
             return cudaGetLastError();
         }
         return cudaErrorInvalidValue;
@@ -134,7 +135,8 @@ cudaError_t z_cons<HQT_ZN>(const ZConsArgs<double> &a, const ZHost &h, cudaStrea
     const long long tiles = (a.plane + kZConsSites - 1) / kZConsSites;
     const long long full = (long long)per_sm * (nsm > 0 ? nsm : 1);
     const ZOps<double, HQT_ZN> op = make_zops(h);
-    k_zcons_tc<HQT_ZN><<<(int)(tiles < full ? tiles : full), kZThreads, smem, s>>>(a, op);
+    (void)klaunch(k_zcons_tc<HQT_ZN>, dim3((int)(tiles < full ? tiles : full)), dim3(kZThreads),
+                  smem, s, a, op);
     return cudaGetLastError();
 }
 
@@ -142,7 +144,7 @@ template <>
 cudaError_t z_misc<HQT_ZN>(const ZColArgs<double> &a, const ZHost &h, int grid, int threads,
                            cudaStream_t s) {
     const ZOps<double, HQT_ZN> op = make_zops(h);
-    k_zcol_misc<double, HQT_ZN><<<grid, threads, 0, s>>>(a, op);
+    (void)klaunch(k_zcol_misc<double, HQT_ZN>, dim3(grid), dim3(threads), 0, s, a, op);
     return cudaGetLastError();
 }
 

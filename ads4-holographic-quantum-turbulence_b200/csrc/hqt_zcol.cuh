@@ -24,6 +24,7 @@ namespace hqt {
 
 template <typename T, int NZP>
 __global__ void __launch_bounds__(128, 4) k_zcol_misc(ZColArgs<T> a, ZOps<T, NZP> op) {
+    pdl_wait();
     const long long site = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (site >= a.plane) return;
     const int nz = a.nz;

@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(kZThreads, 2)
         lzr[m] = i < NZP ? op.lzb[i < NZP ? i : 0] : 0.0;
     }
     __syncthreads();
+    pdl_wait();
 
     const ZTileF<double2> PS{reinterpret_cast<double2 *>(sm + Lay::oPS)};
     const ZTileF<double2> AXY{reinterpret_cast<double2 *>(sm + Lay::oAXY)};
@@ -518,6 +519,7 @@ __global__ void __launch_bounds__(kZThreads)
         }
     }
     __syncthreads();
+    pdl_wait();
     const ZTileF<double2> V1{sm + 6 * L}, V2{sm + 7 * L};
     const auto V1w = V1.cols(cw), V2w = V2.cols(cw);
     const long long ntiles = (P + kZConsSites - 1) / kZConsSites;

@@ -241,13 +241,13 @@ def run_ours(args, w, ws, rank, local):
     sim = hqt.Simulation(nx, ny, nz, Lx=w["L"], Ly=w["L"], mu=w["mu"], vy=w["vy"],
                          dt=w["dt"], remove_winding=w["remove_winding"], device=dev,
                          autotune=not args.no_autotune)
-    geometry = sim.config_report()
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)  # graph capture needs a non-default stream
     T = [api.to_device(a, dev) for a in state]
     # warm-up (also captures the step graph)
     sim.step_device(*T, nsteps=max(args.warmup, 3))
     torch.cuda.synchronize()
+    geometry = sim.config_report()  # after the graph build (which may clear "pdl")
     pr = torch.cuda.get_device_properties(dev)
     pci = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
     if ws > 1:
@@ -394,6 +394,7 @@ def run_ours(args, w, ws, rank, local):
                 "config": bench_config(args.workload, w, ws),
                 "gpu_launches": launches, "roofline": roofline,
                 "line_geometry": geometry.get("chosen"),
+                "programmatic_dependent_launch": geometry.get("pdl"),
                 "step_hbm": {"alg_bytes_per_site": STEP_BYTES_FP64, "achieved_gbs": step_gbs,
                              "frac": step_gbs / peak},
                 "kernel_breakdown": breakdown, "mixed_precision": mixed,
