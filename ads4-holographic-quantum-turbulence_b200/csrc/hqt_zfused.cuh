@@ -91,8 +91,14 @@ template <typename V> struct ZTileF {
 // blocks per SM instead of two at nz = 21, left both loads exposed: 165
 // against 136 us per stage at 301x301x21, 0.99 against 0.92 ms at
 // 512x512x25.)
+// The staged input fields are read at levels < nz (pointwise terms, with
+// clamped indices) and < KP (the mma operand), so they hold KP levels; the
+// V fields are written at every output level 8m+g < MP and hold LV.  At
+// nz = 25 (KP = 28, MP = 32) that is 103.5 KB instead of 116 KB: two blocks
+// per SM instead of one.
 template <typename TD, int NZP> struct ZfLayout {
-    static constexpr int L = ZmDims<NZP>::LV * kZTile;
+    static constexpr int L = ZmDims<NZP>::KP * kZTile;   // staged fields
+    static constexpr int LV = ZmDims<NZP>::LV * kZTile;  // V fields
     static constexpr int c = L * 16, r = L * 8;  // complex / pair, real (double)
     static constexpr int dc = L * (int)sizeof(C2<TD>), dr = L * (int)sizeof(TD);
     static constexpr int mx(int a, int b) { return a > b ? a : b; }
@@ -108,8 +114,8 @@ template <typename TD, int NZP> struct ZfLayout {
     static constexpr int oGP = oG + ((gsz + 15) / 16) * 16;  // Psi-phase region
     static constexpr int oV = oGP + psz;
     // V: dp then S1 (Psi phase); g and S of the gauge phase
-    static constexpr int oVG = oV, oVS = oV + c;
-    static constexpr int bytes = oV + 2 * c;
+    static constexpr int oVG = oV, oVS = oV + LV * 16;
+    static constexpr int bytes = oV + 2 * LV * 16;
 };
 
 template <typename T, typename TS, typename TD, int NZP>

@@ -136,6 +136,9 @@ def run_oracle(oracle, nx, ny, nz, L, state, nsteps, dt, mu, vy, remove_winding=
     (33, 10, 16.0, VY7, "reference", True),     # smoke-test grid, driven
     (64, 21, 50.0, 0.0, "complex", True),       # CPU-runnable config
     (48, 17, 30.0, VY7, "complex", False),      # lattice script: no winding removal
+    (40, 25, 20.0, VY7, "complex", True),       # 25 levels: trimmed staged tiles
+    (36, 23, 18.0, VY7, "complex", True),       # 23 levels in the 25-level kernel
+    (32, 33, 16.0, 0.0, "complex", True),       # 33 levels (large single run)
 ])
 def test_single_step_parity(hqt, oracle, nx, nz, L, vy, noise, rw, cuda):
     state = driven_state(hqt, nx, nx, nz, noise=noise, amp=1e-2, vy=vy)
