@@ -111,8 +111,13 @@ template <typename TD, int NZP> struct ZfLayout {
     static constexpr int pAT = 0, pDAT = r, pLAP = 2 * r, pDIV = 2 * r + dc;
     static constexpr int pZP = ((pDIV + dr + 15) / 16) * 16, pKP = pZP + c;
     static constexpr int psz = pKP + c;
-    static constexpr int oGP = oG + ((gsz + 15) / 16) * 16;  // Psi-phase region
-    static constexpr int oV = oGP + psz;
+    static constexpr int gsz16 = ((gsz + 15) / 16) * 16;
+    // separate Gg and Gp while two blocks still fit on an SM (228 KB, 1 KB
+    // reserved per block); otherwise (FP64 at nz = 33: 136 KB split, 97 KB
+    // shared) one G region that the two phases take in turn
+    static constexpr bool split = oG + gsz16 + psz + 2 * LV * 16 <= (228 / 2 - 1) * 1024;
+    static constexpr int oGP = split ? oG + gsz16 : oG;  // Psi-phase region
+    static constexpr int oV = split ? oGP + psz : oG + mx(gsz16, psz);
     // V: dp then S1 (Psi phase); g and S of the gauge phase
     static constexpr int oVG = oV, oVS = oV + LV * 16;
     static constexpr int bytes = oV + 2 * LV * 16;
@@ -283,15 +288,21 @@ __global__ void __launch_bounds__(kZThreads, 2)
     // commit groups per tile: (gauge of the next tile), (main of the next
     // tile), (Psi of the next tile); the Psi group of a tile is the one left
     // outstanding while its gauge phase runs
-    if ((long long)blockIdx.x < ntiles) stage_psi((long long)blockIdx.x * kZTile);
-    cp_commit();
+    if constexpr (Lay::split) {
+        if ((long long)blockIdx.x < ntiles) stage_psi((long long)blockIdx.x * kZTile);
+        cp_commit();
+    }
 #pragma unroll 1
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long site0 = tile * kZTile;
         const long long next = tile + gridDim.x;
         const long long sw0 = site0 + cw;   // this warp's first column
         const long long site = sw0 + q;     // this lane's column in C layout
-        cp_wait<1>();     // main and gauge inputs; the Psi inputs may be in flight
+        // main and gauge inputs; with split regions the Psi inputs may be in flight
+        if constexpr (Lay::split)
+            cp_wait<1>();
+        else
+            cp_wait<0>();
         __syncthreads();  // every thread's copies are in
 
         // ---- F3, F4: both gauge components at once -------------------------
@@ -370,8 +381,13 @@ __global__ void __launch_bounds__(kZThreads, 2)
         __syncthreads();  // every warp is done with Gg: it refills
 
         // ---- Psi ---------------------------------------------------------------
-        // the next tile's gauge inputs (this tile's Psi inputs came earlier)
-        if (next < ntiles) stage_gauge(next * kZTile);
+        // split: the next tile's gauge inputs (this tile's Psi inputs came
+        // earlier); shared G: this tile's Psi inputs over its gauge inputs
+        if constexpr (Lay::split) {
+            if (next < ntiles) stage_gauge(next * kZTile);
+        } else {
+            stage_psi(site0);
+        }
         cp_commit();
         {  // dp = Lz Psi
             double c[MT][2];
@@ -379,7 +395,12 @@ __global__ void __launch_bounds__(kZThreads, 2)
 #pragma unroll
             for (int m = 0; m < MT; ++m) VC(8 * m + g, cw + q) = make_double2(c[m][0], c[m][1]);
         }
-        cp_wait<1>();     // this tile's Psi inputs; the next gauge group may be in flight
+        // this tile's Psi inputs; with split regions the next gauge group may
+        // be in flight
+        if constexpr (Lay::split)
+            cp_wait<1>();
+        else
+            cp_wait<0>();
         __syncthreads();  // every thread's copies are in
         // boundary row of F2: kb = Lz(nz,:) div A of column q, in every lane
         T kb = T(0);
@@ -473,7 +494,12 @@ __global__ void __launch_bounds__(kZThreads, 2)
             }
         }
         __syncthreads();  // every warp is done with Gp: the next tile refills it
-        if (next < ntiles) stage_psi(next * kZTile);
+        if (next < ntiles) {
+            if constexpr (Lay::split)
+                stage_psi(next * kZTile);
+            else
+                stage_gauge(next * kZTile);
+        }
         cp_commit();
     }
     cp_wait<0>();
