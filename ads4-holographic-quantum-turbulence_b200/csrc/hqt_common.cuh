@@ -140,6 +140,17 @@ __device__ __forceinline__ int plaquette_class(const double2 *O, int nx, int ny,
 }
 #endif
 
+// Column kx of the x spectra survives the filter weight
+// (M(kx,ky) + M(-kx,-ky))/2 for some ky iff mx(kx) or mx(-kx) is nonzero.
+// The others form one range [dead0, dead1] (set up with the masks).  They
+// are zero after the y pass, so in every line engine the filter's x forward
+// pass does not store them, its y pass skips blocks made of them only, and
+// its x inverse reads them as zero (whatever a y pass of another engine
+// left there).
+__host__ __device__ constexpr bool filt_col_live(int kx, int dead0, int dead1) {
+    return kx < dead0 || kx > dead1;
+}
+
 // Status word shared by the step kernels (device memory).
 struct DevStatus {
     long long step;            // steps completed since the context was created

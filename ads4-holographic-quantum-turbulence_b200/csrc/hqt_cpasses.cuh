@@ -45,6 +45,31 @@ __device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long z
         if (b < valid) put(zoff + (long long)y * nx + b, s[t]);
     }
 }
+// cy_store whose put(g, v, x) also takes x = get(g), a global value of the
+// same element (an addend).  The reads of kCtRd elements are issued before
+// their writes: in one loop a read after a write could not move ahead of it
+// (the compiler cannot tell the arrays apart), which left every element's
+// read latency exposed.
+constexpr int kCtRd = 8;
+template <typename T, int N, int NB, typename X, typename G, typename F>
+__device__ __forceinline__ void cy_store_rd(int buf, int valid, int nx, long long zoff, G get,
+                                            F put) {
+    const CtView<T, N> s = ctv<T, N>(buf);
+    constexpr int TOT = N * NB;
+    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * kCtThreads) {
+        X x[kCtRd];
+#pragma unroll
+        for (int j = 0; j < kCtRd; ++j) {
+            const int t = t0 + j * kCtThreads, y = t / NB, b = t - y * NB;
+            if (t < TOT && b < valid) x[j] = get(zoff + (long long)y * nx + b);
+        }
+#pragma unroll
+        for (int j = 0; j < kCtRd; ++j) {
+            const int t = t0 + j * kCtThreads, y = t / NB, b = t - y * NB;
+            if (t < TOT && b < valid) put(zoff + (long long)y * nx + b, s[t], x[j]);
+        }
+    }
+}
 
 template <typename T, int N>
 __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
@@ -106,8 +131,9 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     __syncthreads();
     const int fr = (r1 == Y) ? C : Y;
     const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
-    cy_store<T, N, NB>(r2, valid, a.nx, zoff,
-                       [&](long long g, C2<T> v) { a.lap[g] = a.dxxpsi[g] + v; });
+    cy_store_rd<T, N, NB, C2<T>>(
+        r2, valid, a.nx, zoff, [&](long long g) { return a.dxxpsi[g]; },
+        [&](long long g, C2<T> v, C2<T> x) { a.lap[g] = x + v; });
     __syncthreads();
     // C = A_x + i A_y and E = d_x C, each transformed, then paired
     cy_load<T, N, NB>(A, valid, a.nx, zoff,
@@ -153,16 +179,14 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     const int F3 = (P1 == SC) ? F2 : SC;
     const int P2 = ct_fft<T, N, NB, +1>(SE, F3, R);
     {
-        const CtView<T, N> s1 = ctv<T, N>(P1), s2 = ctv<T, N>(P2);
-        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
-            const int y = t / NB, b = t - y * NB;
-            if (b < valid) {
-                const long long g = zoff + (long long)y * a.nx + b;
-                a.divA[g] = a.E[g].x + s1[t].x;
-                a.dxB[g] = a.dxxay[g] + s1[t].y;
-                a.dyB[g] = s2[t].x;
-            }
-        }
+        // x = (E.x, d_xx A_y) of the element
+        cy_store_rd<T, N, NB, C2<T>>(
+            P1, valid, a.nx, zoff, [&](long long g) { return mk2<T>(a.E[g].x, a.dxxay[g]); },
+            [&](long long g, C2<T> v, C2<T> x) {
+                a.divA[g] = x.x + v.x;
+                a.dxB[g] = x.y + v.y;
+            });
+        cy_store<T, N, NB>(P2, valid, a.nx, zoff, [&](long long g, C2<T> v) { a.dyB[g] = v.x; });
     }
 }
 
@@ -199,10 +223,16 @@ __global__ void HQT_CT_BOUNDS k_y_d1_c(YD1Args<T> a) {
     ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
     __syncthreads();
     const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
-    cy_store<T, N, NB>(r, valid, a.nx, zoff, [&](long long g, C2<T> v) {
-        if (a.add_re) v.x += a.add_re[g];
-        store_field(a.out, g, v);
-    });
+    if (a.add_re)
+        cy_store_rd<T, N, NB, T>(
+            r, valid, a.nx, zoff, [&](long long g) { return a.add_re[g]; },
+            [&](long long g, C2<T> v, T x) {
+                v.x += x;
+                store_field(a.out, g, v);
+            });
+    else
+        cy_store<T, N, NB>(r, valid, a.nx, zoff,
+                           [&](long long g, C2<T> v) { store_field(a.out, g, v); });
 }
 
 // First x / y derivative of a real field into a real field, two real lines
@@ -261,14 +291,30 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     ct_deriv<T, N, NB, 1>(X, X, a.s1, T(0));
     __syncthreads();
     const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
+    // the addends of kCtRd elements are read before their writes (cy_store_rd)
     const CtView<T, N> sr = ctv<T, N>(r);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
-        const int y = t / NB, j = t - y * NB;
-        const int r0 = 2 * j, r1 = r0 + 1;
-        const long long gy = zoff + (long long)y * a.nx;
-        const C2<T> v = sr[t];
-        if (r0 < nr) a.out.re[gy + r0] = v.x + (a.add_re ? a.add_re[gy + r0] : T(0));
-        if (r1 < nr) a.out.re[gy + r1] = v.y + (a.add_re ? a.add_re[gy + r1] : T(0));
+    constexpr int TOT = N * NB;
+    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * kCtThreads) {
+        C2<T> x[kCtRd];
+#pragma unroll
+        for (int i = 0; i < kCtRd; ++i) {
+            const int t = t0 + i * kCtThreads, y = t / NB, j = t - y * NB;
+            const int r0 = 2 * j, r1 = r0 + 1;
+            const long long gy = zoff + (long long)y * a.nx;
+            const bool in = t < TOT && a.add_re;
+            x[i] = mk2<T>(in && r0 < nr ? a.add_re[gy + r0] : T(0),
+                          in && r1 < nr ? a.add_re[gy + r1] : T(0));
+        }
+#pragma unroll
+        for (int i = 0; i < kCtRd; ++i) {
+            const int t = t0 + i * kCtThreads, y = t / NB, j = t - y * NB;
+            if (t >= TOT) continue;
+            const int r0 = 2 * j, r1 = r0 + 1;
+            const long long gy = zoff + (long long)y * a.nx;
+            const C2<T> v = sr[t];
+            if (r0 < nr) a.out.re[gy + r0] = v.x + x[i].x;
+            if (r1 < nr) a.out.re[gy + r1] = v.y + x[i].y;
+        }
     }
 }
 
@@ -298,7 +344,9 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
         __syncthreads();
         const int X = ct_fft<T, N, NB, -1>(A, B, R);
         C2<T> *spec = a.spec[f];
-        cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) { spec[g0 + t] = v; });
+        cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) {
+            if (filt_col_live(t % N, a.dead0, a.dead1)) spec[g0 + t] = v;
+        });
         __syncthreads();
     }
 }
@@ -311,6 +359,9 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     const int valid = min(TX, a.nx - x0);
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     constexpr int R = 0, A = N, B = N + NB * N;
+    bool live = false;
+    for (int b = 0; b < valid; ++b) live = live || filt_col_live(x0 + b, a.dead0, a.dead1);
+    if (!live) return;  // every column filtered out
     ct_load_roots<T, N>(R, a.roots);
     pdl_wait();
     {
@@ -358,7 +409,9 @@ __global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
     int mybad = 0;
     for (int f = 0; f < a.nf; ++f) {
         const C2<T> *spec = a.spec[f];
-        cx_load<T, N, NB>(A, valid, [&](int t) { return spec[g0 + t]; });
+        cx_load<T, N, NB>(A, valid, [&](int t) {
+            return filt_col_live(t % N, a.dead0, a.dead1) ? spec[g0 + t] : mk2<T>(T(0), T(0));
+        });
         __syncthreads();
         const int X = ct_fft<T, N, NB, +1>(A, B, R);
         cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) {

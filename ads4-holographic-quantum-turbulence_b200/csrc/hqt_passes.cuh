@@ -119,6 +119,31 @@ __device__ __forceinline__ void yl_store(int buf, int n, int nb, int nx, long lo
     }
 }
 
+// yl_store whose put(g, v, x) also takes x = get(g), an addend read from
+// global memory: the reads of kRdBatch elements are issued before their
+// writes (in one loop a read after a write could not move ahead of it, the
+// compiler not knowing the arrays apart, and each read's latency was exposed).
+constexpr int kRdBatch = 8;
+template <typename T, typename X, typename G, typename F>
+__device__ __forceinline__ void yl_store_rd(int buf, int n, int nb, int nx, long long zoff,
+                                            G get, F put) {
+    const C2<T> *s = sptr<T>(buf);
+    const int tot = n * nb, th = blockDim.x;
+    for (int t0 = threadIdx.x; t0 < tot; t0 += kRdBatch * th) {
+        X x[kRdBatch];
+#pragma unroll
+        for (int j = 0; j < kRdBatch; ++j) {
+            const int t = t0 + j * th, y = t / nb, b = t - y * nb;
+            if (t < tot) x[j] = get(zoff + (long long)y * nx + b);
+        }
+#pragma unroll
+        for (int j = 0; j < kRdBatch; ++j) {
+            const int t = t0 + j * th, y = t / nb, b = t - y * nb;
+            if (t < tot) put(zoff + (long long)y * nx + b, t, s[t], x[j]);
+        }
+    }
+}
+
 #define HQT_FFT_BOUNDS __launch_bounds__(128, 4)
 
 // ------------------------------------------------------------------------
@@ -190,8 +215,9 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_rhs(YRhsArgs<T> a) {
     __syncthreads();
     int fr = (r1 == Y) ? A2 : Y;
     int r2 = fft_run<T>(X, fr, R, a.plan, nb, +1);
-    yl_store<T>(r2, n, nb, a.nx, zoff,
-                [&](long long g, C2<T> v) { a.lap[g] = a.dxxpsi[g] + v; });
+    yl_store_rd<T, C2<T>>(
+        r2, n, nb, a.nx, zoff, [&](long long g) { return a.dxxpsi[g]; },
+        [&](long long g, int, C2<T> v, C2<T> x) { a.lap[g] = x + v; });
     __syncthreads();
     // ---- C = A_x + i A_y and E = d_x C as one batch of 2*nb lines ----
     const int nb2 = 2 * nb;
@@ -245,17 +271,18 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_rhs(YRhsArgs<T> a) {
     const int Xo = (X == P) ? Q : P;
     const int r3 = fft_run<T>(X, Xo, R, a.plan, nb2, +1);
     {
+        // element t = y*nb + b of the nb-line view; x = (E.x, d_xx A_y)
         const C2<T> *s = sptr<T>(r3);
-        const int tot = nb * n;
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            const int y = t / nb, b = t - y * nb;
-            const long long g = zoff + (long long)y * a.nx + b;
-            const C2<T> p1 = s[y * nb2 + b];
-            const C2<T> p2 = s[y * nb2 + nb + b];
-            a.divA[g] = a.E[g].x + p1.x;
-            a.dxB[g] = a.dxxay[g] + p1.y;
-            a.dyB[g] = p2.x;
-        }
+        yl_store_rd<T, C2<T>>(
+            r3, n, nb, a.nx, zoff, [&](long long g) { return mk2<T>(a.E[g].x, a.dxxay[g]); },
+            [&](long long g, int t, C2<T>, C2<T> x) {
+                const int y = t / nb, b = t - y * nb;
+                const C2<T> p1 = s[y * nb2 + b];
+                const C2<T> p2 = s[y * nb2 + nb + b];
+                a.divA[g] = x.x + p1.x;
+                a.dxB[g] = x.y + p1.y;
+                a.dyB[g] = p2.x;
+            });
     }
 }
 
@@ -296,10 +323,15 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_d1(YD1Args<T> a) {
     __syncthreads();
     const int Y = (X == A) ? B : A;
     const int r = fft_run<T>(X, Y, R, a.plan, nb, +1);
-    yl_store<T>(r, n, nb, a.nx, zoff, [&](long long g, C2<T> v) {
-        if (a.add_re) v.x += a.add_re[g];
-        store_field(a.out, g, v);
-    });
+    if (a.add_re)
+        yl_store_rd<T, T>(
+            r, n, nb, a.nx, zoff, [&](long long g) { return a.add_re[g]; },
+            [&](long long g, int, C2<T> v, T x) {
+                v.x += x;
+                store_field(a.out, g, v);
+            });
+    else
+        yl_store<T>(r, n, nb, a.nx, zoff, [&](long long g, C2<T> v) { store_field(a.out, g, v); });
 }
 
 // ------------------------------------------------------------------------
@@ -331,7 +363,9 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_fwd(XFiltFwdArgs<T
         __syncthreads();
         const int X = fft_run<T>(A, B, R, a.plan, nb, -1);
         C2<T> *spec = a.spec[f];
-        xl_store<T>(X, n, nb, [&](int t, C2<T> v) { spec[g0 + t] = v; });
+        xl_store<T>(X, n, nb, [&](int t, C2<T> v) {
+            if (filt_col_live(t % n, a.dead0, a.dead1)) spec[g0 + t] = v;
+        });
         __syncthreads();
     }
 }
@@ -343,6 +377,9 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_filt(YFiltArgs<T> a) {
     const long long zoff = (long long)blockIdx.y * a.ny * a.nx + x0;
     const int nbl = nb * a.nf;
     const int R = 0, A = n, B = n + a.TX * a.nf * n;
+    bool live = false;
+    for (int b = 0; b < nb; ++b) live = live || filt_col_live(x0 + b, a.dead0, a.dead1);
+    if (!live) return;  // every column filtered out
     load_roots<T>(R, a.roots, n);
     pdl_wait();
     const int tot = nbl * n;
@@ -391,7 +428,9 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_x_filt_inv(XFiltInvArgs<T
     int mybad = 0;
     for (int f = 0; f < a.nf; ++f) {
         const C2<T> *spec = a.spec[f];
-        xl_load<T>(A, n, nb, [&](int t) { return spec[g0 + t]; });
+        xl_load<T>(A, n, nb, [&](int t) {
+            return filt_col_live(t % n, a.dead0, a.dead1) ? spec[g0 + t] : mk2<T>(T(0), T(0));
+        });
         __syncthreads();
         const int X = fft_run<T>(A, B, R, a.plan, nb, +1);
         xl_store<T>(X, n, nb, [&](int t, C2<T> v) {

@@ -109,15 +109,6 @@ template <typename T, int P, int Q> struct PfaLines {
     }
 };
 
-// Column kx of the x spectra survives the filter weight
-// (M(kx,ky) + M(-kx,-ky))/2 for some ky iff mx(kx) or mx(-kx) is nonzero.
-// The others form one range [dead0, dead1] (set up with the masks); they
-// are zero after the y pass, so they are neither transformed along y nor
-// read back.
-__device__ __forceinline__ bool filt_col_live(int kx, int dead0, int dead1) {
-    return kx < dead0 || kx > dead1;
-}
-
 // cos/sin(2 pi j/P), j = 0..P-1, for the CUDA-core stage B
 template <typename T, int P> __device__ __forceinline__ void pfa_twiddles(T (&cs)[2][P]) {
 #pragma unroll

@@ -63,7 +63,12 @@ def test_rhs_parity(hqt, oracle, dev, nx, ny, nz):
 
 
 @pytest.mark.parametrize("nx,ny,nz", [(33, 33, 10), (64, 64, 21), (301, 301, 5),
-                                      (53, 59, 8), (30, 22, 12)])
+                                      (53, 59, 8), (30, 22, 12),
+                                      # x and y on different line engines: the
+                                      # x inverse must read the weight-zeroed
+                                      # columns as zero whatever the y pass did
+                                      (64, 301, 4), (40, 301, 3), (301, 64, 4),
+                                      (512, 48, 3), (48, 512, 3)])
 def test_filter_parity(hqt, oracle, cuda, nx, ny, nz):
     torch = cuda
     rng = np.random.default_rng(nx + ny)
