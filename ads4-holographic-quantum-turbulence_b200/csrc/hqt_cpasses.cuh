@@ -28,6 +28,23 @@ __device__ __forceinline__ void cx_store(int buf, int valid, F put) {
         if (b < valid) put(t, s[e * NB + b]);
     }
 }
+// (re, im) of two real fields into the x-line layout of cx_load by cp.async
+// (zero past `valid`); the caller commits and waits
+template <typename T, int N, int NB>
+__device__ __forceinline__ void cx_load_pair_async(int buf, int valid, long long g0, const T *re,
+                                                   const T *im) {
+    const CtView<T, N> s = ctv<T, N>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int b = t / N, e = t - b * N;
+        C2<T> &d = s[e * NB + b];
+        if (b < valid) {
+            cp_async<sizeof(T)>(&d.x, re + g0 + t);
+            cp_async<sizeof(T)>(&d.y, im + g0 + t);
+        } else {
+            d = mk2<T>(T(0), T(0));
+        }
+    }
+}
 // y lines: NB adjacent columns of one z slice; element (y, b) at y*NB + b
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zoff, F get) {
@@ -43,6 +60,36 @@ __device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long z
     for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
         const int y = t / NB, b = t - y * NB;
         if (b < valid) put(zoff + (long long)y * nx + b, s[t]);
+    }
+}
+// cy_load by cp.async of a complex field, or of the pair (re, im) of two
+// real fields (zero past `valid`); the caller commits and waits
+template <typename T, int N, int NB>
+__device__ __forceinline__ void cy_load_async(int buf, int valid, int nx, long long zoff,
+                                              const C2<T> *src) {
+    const CtView<T, N> s = ctv<T, N>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int y = t / NB, b = t - y * NB;
+        if (b < valid)
+            cp_async<sizeof(C2<T>)>(&s[t], src + zoff + (long long)y * nx + b);
+        else
+            s[t] = mk2<T>(T(0), T(0));
+    }
+}
+template <typename T, int N, int NB>
+__device__ __forceinline__ void cy_load_pair_async(int buf, int valid, int nx, long long zoff,
+                                                   const T *re, const T *im) {
+    const CtView<T, N> s = ctv<T, N>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        const int y = t / NB, b = t - y * NB;
+        C2<T> &d = s[t];
+        if (b < valid) {
+            const long long g = zoff + (long long)y * nx + b;
+            cp_async<sizeof(T)>(&d.x, re + g);
+            cp_async<sizeof(T)>(&d.y, im + g);
+        } else {
+            d = mk2<T>(T(0), T(0));
+        }
     }
 }
 // cy_store whose put(g, v, x) also takes x = get(g), a global value of the
@@ -90,21 +137,24 @@ __global__ void HQT_CT_BOUNDS k_x_rhs_c(XRhsArgs<T> a) {
     cx_store<T, N, NB>(r1, valid, [&](int t, C2<T> v) { a.dxpsi[g0 + t] = v; });
     ct_deriv<T, N, NB, 2>(X, X, a.s1, a.s2);
     __syncthreads();
+    // r1's buffer is free: C = A_x + i A_y comes into it while d_xx Psi is
+    // transformed and stored
+    cx_load_pair_async<T, N, NB>(r1, valid, g0, a.ax, a.ay);
+    cp_commit();
     const int fr = (r1 == Y) ? C : Y;
     const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
     cx_store<T, N, NB>(r2, valid, [&](int t, C2<T> v) { a.dxxpsi[g0 + t] = v; });
-    __syncthreads();
-    cx_load<T, N, NB>(A, valid, [&](int t) { return mk2<T>(a.ax[g0 + t], a.ay[g0 + t]); });
-    __syncthreads();
-    const int X2 = ct_fft<T, N, NB, -1>(A, B, R);
-    const int Y2 = (X2 == A) ? B : A;
+    cp_wait<0>();
+    __syncthreads();  // C is in; X and fr are free
+    const int X2 = ct_fft<T, N, NB, -1>(r1, X, R);
+    const int Y2 = (X2 == r1) ? X : r1;
     ct_deriv<T, N, NB, 1>(Y2, X2, a.s1, a.s2);
     __syncthreads();
-    const int r3 = ct_fft<T, N, NB, +1>(Y2, C, R);
+    const int r3 = ct_fft<T, N, NB, +1>(Y2, fr, R);
     cx_store<T, N, NB>(r3, valid, [&](int t, C2<T> v) { a.E[g0 + t] = v; });
     ct_deriv<T, N, NB, 2>(X2, X2, a.s1, a.s2);
     __syncthreads();
-    const int fr2 = (r3 == Y2) ? C : Y2;
+    const int fr2 = (r3 == Y2) ? fr : Y2;
     const int r4 = ct_fft<T, N, NB, +1>(X2, fr2, R);
     cx_store<T, N, NB>(r4, valid, [&](int t, C2<T> v) { a.dxxay[g0 + t] = v.y; });
 }
@@ -129,21 +179,26 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     cy_store<T, N, NB>(r1, valid, a.nx, zoff, [&](long long g, C2<T> v) { a.dypsi[g] = v; });
     ct_deriv<T, N, NB, 2>(X, X, a.s1, a.s2);
     __syncthreads();
+    // C = A_x + i A_y and E = d_x C, each transformed, then paired.  C comes
+    // into r1's buffer (free now) while d_yy Psi is transformed and stored,
+    // E into a third buffer while C is transformed.
+    cy_load_pair_async<T, N, NB>(r1, valid, a.nx, zoff, a.ax, a.ay);
+    cp_commit();
     const int fr = (r1 == Y) ? C : Y;
     const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
     cy_store_rd<T, N, NB, C2<T>>(
         r2, valid, a.nx, zoff, [&](long long g) { return a.dxxpsi[g]; },
         [&](long long g, C2<T> v, C2<T> x) { a.lap[g] = x + v; });
-    __syncthreads();
-    // C = A_x + i A_y and E = d_x C, each transformed, then paired
-    cy_load<T, N, NB>(A, valid, a.nx, zoff,
-                      [&](long long g) { return mk2<T>(a.ax[g], a.ay[g]); });
-    __syncthreads();
-    const int SC = ct_fft<T, N, NB, -1>(A, B, R);       // C spectrum in A or B
-    const int F1 = (SC == A) ? B : A;                   // free
-    cy_load<T, N, NB>(C, valid, a.nx, zoff, [&](long long g) { return a.E[g]; });
-    __syncthreads();
-    const int SE = ct_fft<T, N, NB, -1>(C, F1, R);      // E spectrum in C or F1
+    __syncthreads();  // X and fr are free
+    cy_load_async<T, N, NB>(fr, valid, a.nx, zoff, a.E);
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();  // C is in
+    const int SC = ct_fft<T, N, NB, -1>(r1, X, R);      // C spectrum in r1 or X
+    const int F1 = (SC == r1) ? X : r1;                 // free
+    cp_wait<0>();
+    __syncthreads();  // E is in
+    const int SE = ct_fft<T, N, NB, -1>(fr, F1, R);     // E spectrum in fr or F1
     {
         const CtView<T, N> sc = ctv<T, N>(SC), se = ctv<T, N>(SE);
         const T h = T(0.5);
