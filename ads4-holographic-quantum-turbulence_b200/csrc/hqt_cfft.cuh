@@ -19,7 +19,7 @@ struct CtPlan {
     int Ns[kMaxPass];
 };
 
-__host__ __device__ constexpr CtPlan ct_plan(int n) {
+__host__ __device__ constexpr CtPlan ct_plan(int n, int maxbits = 4) {
     CtPlan p{};
     int m = n, p2 = 0;
     while (m % 2 == 0) {
@@ -28,7 +28,7 @@ __host__ __device__ constexpr CtPlan ct_plan(int n) {
     }
     int k = 0;
     if (p2 > 0) {
-        const int npass = (p2 + 3) / 4;
+        const int npass = (p2 + maxbits - 1) / maxbits;
         int left = p2;
         for (int i = 0; i < npass; ++i) {
             const int bits = (left + (npass - i) - 1) / (npass - i);
@@ -50,6 +50,15 @@ __host__ __device__ constexpr CtPlan ct_plan(int n) {
     }
     return p;
 }
+
+// Largest power-of-two radix 2^maxbits of a pass: 8 in FP64, 16 in FP32.
+// An FP64 radix-16 butterfly (16 complex doubles in registers, plus
+// twiddles) overflowed the 128 registers of the pass kernels: spills and a
+// stack frame around every transform call.  With radix 8 at most (N = 256
+// as 8*8*4 instead of 16*16), the 256^2 x 21 step went from 2.22 to
+// 1.34 ms and the 32-run ensemble from 37.2 to 28.1 ms.
+template <typename T> __host__ __device__ constexpr int ct_maxbits() { return 3; }
+template <> __host__ __device__ constexpr int ct_maxbits<float>() { return 4; }
 
 __host__ __device__ constexpr bool ct_small_radix(int R) {
     return R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8 || R == 11 || R == 13 ||
@@ -245,7 +254,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
 
 template <typename T, int N, int NB, int P>
 __device__ __forceinline__ int ct_fft_from(int src, int dst, int roots, int sign) {
-    constexpr CtPlan pl = ct_plan(N);
+    constexpr CtPlan pl = ct_plan(N, ct_maxbits<T>());
     if constexpr (P >= pl.np) {
         return src;
     } else {
