@@ -19,7 +19,7 @@ struct CtPlan {
     int Ns[kMaxPass];
 };
 
-__host__ __device__ constexpr CtPlan ct_plan(int n, int maxbits = 4) {
+__host__ __device__ constexpr CtPlan ct_plan(int n, int maxbits) {
     CtPlan p{};
     int m = n, p2 = 0;
     while (m % 2 == 0) {
@@ -51,14 +51,14 @@ __host__ __device__ constexpr CtPlan ct_plan(int n, int maxbits = 4) {
     return p;
 }
 
-// Largest power-of-two radix 2^maxbits of a pass: 8 in FP64, 16 in FP32.
-// An FP64 radix-16 butterfly (16 complex doubles in registers, plus
-// twiddles) overflowed the 128 registers of the pass kernels: spills and a
-// stack frame around every transform call.  With radix 8 at most (N = 256
-// as 8*8*4 instead of 16*16), the 256^2 x 21 step went from 2.22 to
-// 1.34 ms and the 32-run ensemble from 37.2 to 28.1 ms.
-template <typename T> __host__ __device__ constexpr int ct_maxbits() { return 3; }
-template <> __host__ __device__ constexpr int ct_maxbits<float>() { return 4; }
+// Largest power-of-two radix of a pass: 2^3.  An FP64 radix-16 butterfly
+// (16 complex doubles in registers, plus twiddles) overflowed the 128
+// registers of the pass kernels: spills and a stack frame around every
+// transform call.  With radix 8 at most (N = 256 as 8*8*4 instead of
+// 16*16), the 256^2 x 21 step went from 2.22 to 1.34 ms and the 32-run
+// ensemble from 37.2 to 28.1 ms; in FP32 (mixed precision) the 1024^2 x 33
+// step went from 48.5 to 47.3 ms.
+constexpr int kCtMaxBits = 3;
 
 __host__ __device__ constexpr bool ct_small_radix(int R) {
     return R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8 || R == 11 || R == 13 ||
@@ -254,7 +254,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
 
 template <typename T, int N, int NB, int P>
 __device__ __forceinline__ int ct_fft_from(int src, int dst, int roots, int sign) {
-    constexpr CtPlan pl = ct_plan(N, ct_maxbits<T>());
+    constexpr CtPlan pl = ct_plan(N, kCtMaxBits);
     if constexpr (P >= pl.np) {
         return src;
     } else {
@@ -302,7 +302,7 @@ __device__ __forceinline__ void ct_deriv(int dst, int src, T s1, T s2) {
 
 // Host check: a plan this engine can instantiate.
 __host__ __device__ constexpr bool ct_plan_ok(int n) {
-    const CtPlan p = ct_plan(n);
+    const CtPlan p = ct_plan(n, kCtMaxBits);
     for (int i = 0; i < p.np; ++i)
         if (!ct_small_radix(p.R[i]) && (big_offset(p.R[i]) < 0 || (p.R[i] - 1) / 2 + 1 > 6 * kCtKB))
             return false;

@@ -290,7 +290,6 @@ __device__ __noinline__ int fft_run(int a, int b, int roots, FFTPlan plan, int n
             HQT_PASS(8)
             HQT_PASS(11)
             HQT_PASS(13)
-            HQT_PASS(16)
 #undef HQT_PASS
         default:
             bigodd_pass<T>(src, dst, roots, n, R, Ns, nb, sign);

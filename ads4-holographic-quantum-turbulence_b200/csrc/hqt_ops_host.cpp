@@ -115,9 +115,10 @@ FFTPlan make_plan(int n) {
         ++p2;
     }
     std::vector<int> rad;
-    // power-of-two part: ceil(p2/4) passes, bits spread evenly (16, 8, 4, 2)
+    // power-of-two part: ceil(p2/3) passes, bits spread evenly (8, 4, 2); a
+    // radix-16 pass held 16 complex values in registers and spilled in FP64
     if (p2 > 0) {
-        const int npass = (p2 + 3) / 4;
+        const int npass = (p2 + 2) / 3;
         int left = p2;
         for (int i = 0; i < npass; ++i) {
             const int bits = (left + (npass - i) - 1) / (npass - i);
