@@ -68,24 +68,34 @@ cudaError_t ct_init<HQT_CN>(const double *tc, const double *ts, int ntab, const 
 template <>
 cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem,
                               cudaStream_t s) {
-    constexpr int T = kCtThreads;
+    // block sizes: ct_threads of each kernel's NB (the expressions of the kernels)
+    constexpr int N = HQT_CN, ED = (int)sizeof(double2), EF = (int)sizeof(float2);
+    constexpr int TXR = ct_threads_n(N, ct_lines(N, 3, ED), ED);
+    constexpr int TYR = ct_threads_n(N, ct_lines_y(N, 3, ED), ED);
+    constexpr int TX2 = ct_threads_n(N, ct_lines(N, 2, ED), ED);
+    constexpr int TY2 = ct_threads_n(N, ct_lines_y(N, 2, ED), ED);
+    constexpr int TYF = ct_threads_n(N, 3 * ct_lines_y(N, 6, ED), ED);
+    constexpr int TXRf = ct_threads_n(N, ct_lines(N, 3, EF), EF);
+    constexpr int TYRf = ct_threads_n(N, ct_lines_y(N, 3, EF), EF);
+    constexpr int TX2f = ct_threads_n(N, ct_lines(N, 2, EF), EF);
+    constexpr int TY2f = ct_threads_n(N, ct_lines_y(N, 2, EF), EF);
     switch (kind) {
         case CT_X_RHS:
-            (void)klaunch(k_x_rhs_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_x_rhs_c<double, HQT_CN>, dim3(grid), dim3(TXR), smem, s,
                           *(const XRhsArgs<double> *)args);
             break;
         case CT_Y_RHS:
-            (void)klaunch(k_y_rhs_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_y_rhs_c<double, HQT_CN>, dim3(grid), dim3(TYR), smem, s,
                           *(const YRhsArgs<double> *)args);
             break;
         case CT_X_D1: {
             const XD1Args<double> &a = *(const XD1Args<double> *)args;
             constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(double2));
             if (real_field_d1(a.in, a.out))
-                (void)klaunch(k_x_d1r_c<double, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2), dim3(T),
-                              smem, s, a);
+                (void)klaunch(k_x_d1r_c<double, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2),
+                              dim3(TX2), smem, s, a);
             else
-                (void)klaunch(k_x_d1_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
+                (void)klaunch(k_x_d1_c<double, HQT_CN>, dim3(grid), dim3(TX2), smem, s, a);
             break;
         }
         case CT_Y_D1: {
@@ -93,39 +103,39 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
             constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(double2));
             if (real_field_d1(a.in, a.out))
                 (void)klaunch(k_y_d1r_c<double, HQT_CN>, dim3((a.nx + nb2 - 1) / nb2, grid.y),
-                              dim3(T), smem, s, a);
+                              dim3(TY2), smem, s, a);
             else
-                (void)klaunch(k_y_d1_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
+                (void)klaunch(k_y_d1_c<double, HQT_CN>, dim3(grid), dim3(TY2), smem, s, a);
             break;
         }
         case CT_FX_FWD:
-            (void)klaunch(k_x_filt_fwd_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_x_filt_fwd_c<double, HQT_CN>, dim3(grid), dim3(TX2), smem, s,
                           *(const XFiltFwdArgs<double> *)args);
             break;
         case CT_FY:
-            (void)klaunch(k_y_filt_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_y_filt_c<double, HQT_CN>, dim3(grid), dim3(TYF), smem, s,
                           *(const YFiltArgs<double> *)args);
             break;
         case CT_FX_INV:
-            (void)klaunch(k_x_filt_inv_c<double, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_x_filt_inv_c<double, HQT_CN>, dim3(grid), dim3(TX2), smem, s,
                           *(const XFiltInvArgs<double> *)args);
             break;
         case CT_X_RHS_F:
-            (void)klaunch(k_x_rhs_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_x_rhs_c<float, HQT_CN>, dim3(grid), dim3(TXRf), smem, s,
                           *(const XRhsArgs<float> *)args);
             break;
         case CT_Y_RHS_F:
-            (void)klaunch(k_y_rhs_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s,
+            (void)klaunch(k_y_rhs_c<float, HQT_CN>, dim3(grid), dim3(TYRf), smem, s,
                           *(const YRhsArgs<float> *)args);
             break;
         case CT_X_D1_F: {
             const XD1Args<float> &a = *(const XD1Args<float> *)args;
             constexpr int nb2 = 2 * ct_lines(HQT_CN, 2, sizeof(float2));
             if (real_field_d1(a.in, a.out))
-                (void)klaunch(k_x_d1r_c<float, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2), dim3(T),
-                              smem, s, a);
+                (void)klaunch(k_x_d1r_c<float, HQT_CN>, dim3((a.nlines + nb2 - 1) / nb2),
+                              dim3(TX2f), smem, s, a);
             else
-                (void)klaunch(k_x_d1_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
+                (void)klaunch(k_x_d1_c<float, HQT_CN>, dim3(grid), dim3(TX2f), smem, s, a);
             break;
         }
         case CT_Y_D1_F: {
@@ -133,9 +143,9 @@ cudaError_t ct_launch<HQT_CN>(int kind, const void *args, dim3 grid, size_t smem
             constexpr int nb2 = 2 * ct_lines_y(HQT_CN, 2, sizeof(float2));
             if (real_field_d1(a.in, a.out))
                 (void)klaunch(k_y_d1r_c<float, HQT_CN>, dim3((a.nx + nb2 - 1) / nb2, grid.y),
-                              dim3(T), smem, s, a);
+                              dim3(TY2f), smem, s, a);
             else
-                (void)klaunch(k_y_d1_c<float, HQT_CN>, dim3(grid), dim3(T), smem, s, a);
+                (void)klaunch(k_y_d1_c<float, HQT_CN>, dim3(grid), dim3(TY2f), smem, s, a);
             break;
         }
         default:

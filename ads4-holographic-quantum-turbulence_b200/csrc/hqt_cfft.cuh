@@ -93,7 +93,15 @@ template <> struct BigTab<float> {
     static __device__ __forceinline__ float s(int i) { return c_big_sin_f[i]; }
 };
 
-constexpr int kCtThreads = 128;
+// Threads of a pass block with NB lines of N points: 256 when a buffer of
+// the block holds 32 KB or more (the large FP64/FP32 y-pass blocks at 512
+// and 1024 points, two per SM), else 128.
+__host__ __device__ constexpr int ct_threads_n(int N, int NB, int esize) {
+    return (long long)NB * N * esize >= 32 * 1024 ? 256 : 128;
+}
+template <typename T, int N, int NB> __host__ __device__ constexpr int ct_threads() {
+    return ct_threads_n(N, NB, (int)sizeof(C2<T>));
+}
 
 // Shared-memory view of the compile-time engine's buffers.  When N is a
 // multiple of G = 128 bytes / element (8 complex doubles, 16 complex floats),
@@ -136,7 +144,7 @@ __device__ __forceinline__ void ct_small(int src, int dst, int roots, int sign) 
     constexpr int nR = N / R;
     constexpr int TOTAL = NB * nR;
     constexpr int qs = N / (Ns * R);
-    for (int t = threadIdx.x; t < TOTAL; t += kCtThreads) {
+    for (int t = threadIdx.x; t < TOTAL; t += ct_threads<T, N, NB>()) {
         const int b = t % NB;
         const int j = t / NB;
         const int m = (Ns == 1) ? 0 : j % Ns;
@@ -167,7 +175,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
     static_assert(off >= 0, "radix without a constant table");
     // phase 1: twiddle and fold in place
     constexpr int TOT1 = NB * nR * M;
-    for (int it = threadIdx.x; it < TOT1; it += kCtThreads) {
+    for (int it = threadIdx.x; it < TOT1; it += ct_threads<T, N, NB>()) {
         const int b = it % NB;
         const int rest = it / NB;
         const int j = rest % nR;
@@ -194,7 +202,7 @@ __device__ __forceinline__ void ct_big(int src, int dst, int roots, int sign) {
     constexpr int NG = (NBF + 31) / 32;           // butterfly groups
     const T sg = (sign < 0) ? T(1) : T(-1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int task = warp; task < NKB * NG; task += kCtThreads / 32) {
+    for (int task = warp; task < NKB * NG; task += ct_threads<T, N, NB>() / 32) {
         const int kb = task % NKB;
         const int bf = (task / NKB) * 32 + lane;
         if (bf >= NBF) continue;
@@ -286,7 +294,7 @@ __device__ __forceinline__ int ct_fft(int a, int b, int roots) {
 template <typename T, int N, int NB, int ORDER>
 __device__ __forceinline__ void ct_deriv(int dst, int src, T s1, T s2) {
     const CtView<T, N> S = ctv<T, N>(src), D = ctv<T, N>(dst);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int e = t / NB;
         const T kk = T(2 * e < N ? e : (2 * e > N ? e - N : 0));
         const C2<T> v = S[t];

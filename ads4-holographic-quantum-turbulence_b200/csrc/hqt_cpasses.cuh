@@ -9,13 +9,15 @@
 
 namespace hqt {
 
-#define HQT_CT_BOUNDS __launch_bounds__(kCtThreads, 4)
+// At most 256 threads (ct_threads) and 128 registers a thread: four
+// 128-thread or two 256-thread blocks per SM.
+#define HQT_CT_BOUNDS __launch_bounds__(256, 2)
 
 // x lines: NB consecutive (y, z) rows, contiguous in global memory
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cx_load(int buf, int valid, F get) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int b = t / N, e = t - b * N;
         s[e * NB + b] = (b < valid) ? get(t) : mk2<T>(T(0), T(0));
     }
@@ -23,7 +25,7 @@ __device__ __forceinline__ void cx_load(int buf, int valid, F get) {
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cx_store(int buf, int valid, F put) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int b = t / N, e = t - b * N;
         if (b < valid) put(t, s[e * NB + b]);
     }
@@ -34,7 +36,7 @@ template <typename T, int N, int NB>
 __device__ __forceinline__ void cx_load_pair_async(int buf, int valid, long long g0, const T *re,
                                                    const T *im) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int b = t / N, e = t - b * N;
         C2<T> &d = s[e * NB + b];
         if (b < valid) {
@@ -49,7 +51,7 @@ __device__ __forceinline__ void cx_load_pair_async(int buf, int valid, long long
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zoff, F get) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int y = t / NB, b = t - y * NB;
         s[t] = (b < valid) ? get(zoff + (long long)y * nx + b) : mk2<T>(T(0), T(0));
     }
@@ -57,7 +59,7 @@ __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zo
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_store(int buf, int valid, int nx, long long zoff, F put) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int y = t / NB, b = t - y * NB;
         if (b < valid) put(zoff + (long long)y * nx + b, s[t]);
     }
@@ -68,7 +70,7 @@ template <typename T, int N, int NB>
 __device__ __forceinline__ void cy_load_async(int buf, int valid, int nx, long long zoff,
                                               const C2<T> *src) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int y = t / NB, b = t - y * NB;
         if (b < valid)
             cp_async<sizeof(C2<T>)>(&s[t], src + zoff + (long long)y * nx + b);
@@ -80,7 +82,7 @@ template <typename T, int N, int NB>
 __device__ __forceinline__ void cy_load_pair_async(int buf, int valid, int nx, long long zoff,
                                                    const T *re, const T *im) {
     const CtView<T, N> s = ctv<T, N>(buf);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int y = t / NB, b = t - y * NB;
         C2<T> &d = s[t];
         if (b < valid) {
@@ -103,16 +105,16 @@ __device__ __forceinline__ void cy_store_rd(int buf, int valid, int nx, long lon
                                             F put) {
     const CtView<T, N> s = ctv<T, N>(buf);
     constexpr int TOT = N * NB;
-    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * kCtThreads) {
+    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * ct_threads<T, N, NB>()) {
         X x[kCtRd];
 #pragma unroll
         for (int j = 0; j < kCtRd; ++j) {
-            const int t = t0 + j * kCtThreads, y = t / NB, b = t - y * NB;
+            const int t = t0 + j * ct_threads<T, N, NB>(), y = t / NB, b = t - y * NB;
             if (t < TOT && b < valid) x[j] = get(zoff + (long long)y * nx + b);
         }
 #pragma unroll
         for (int j = 0; j < kCtRd; ++j) {
-            const int t = t0 + j * kCtThreads, y = t / NB, b = t - y * NB;
+            const int t = t0 + j * ct_threads<T, N, NB>(), y = t / NB, b = t - y * NB;
             if (t < TOT && b < valid) put(zoff + (long long)y * nx + b, s[t], x[j]);
         }
     }
@@ -202,7 +204,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     {
         const CtView<T, N> sc = ctv<T, N>(SC), se = ctv<T, N>(SE);
         const T h = T(0.5);
-        for (int t = threadIdx.x; t < (N / 2 + 1) * NB; t += kCtThreads) {
+        for (int t = threadIdx.x; t < (N / 2 + 1) * NB; t += ct_threads<T, N, NB>()) {
             const int b = t % NB, k = t / NB;
             const int kp = (N - k) % N;
             const C2<T> Cc = sc[k * NB + b], Cp = sc[kp * NB + b];
@@ -334,7 +336,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     pdl_wait();
     {  // the layout of cy_load: element (y, j) at y*NB + j
         const CtView<T, N> sa = ctv<T, N>(A);
-        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
             const int y = t / NB, j = t - y * NB;
             const int r0 = 2 * j, r1 = r0 + 1;
             const long long gy = zoff + (long long)y * a.nx;
@@ -349,11 +351,11 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
     // the addends of kCtRd elements are read before their writes (cy_store_rd)
     const CtView<T, N> sr = ctv<T, N>(r);
     constexpr int TOT = N * NB;
-    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * kCtThreads) {
+    for (int t0 = threadIdx.x; t0 < TOT; t0 += kCtRd * ct_threads<T, N, NB>()) {
         C2<T> x[kCtRd];
 #pragma unroll
         for (int i = 0; i < kCtRd; ++i) {
-            const int t = t0 + i * kCtThreads, y = t / NB, j = t - y * NB;
+            const int t = t0 + i * ct_threads<T, N, NB>(), y = t / NB, j = t - y * NB;
             const int r0 = 2 * j, r1 = r0 + 1;
             const long long gy = zoff + (long long)y * a.nx;
             const bool in = t < TOT && a.add_re;
@@ -362,7 +364,7 @@ __global__ void HQT_CT_BOUNDS k_y_d1r_c(YD1Args<T> a) {
         }
 #pragma unroll
         for (int i = 0; i < kCtRd; ++i) {
-            const int t = t0 + i * kCtThreads, y = t / NB, j = t - y * NB;
+            const int t = t0 + i * ct_threads<T, N, NB>(), y = t / NB, j = t - y * NB;
             if (t >= TOT) continue;
             const int r0 = 2 * j, r1 = r0 + 1;
             const long long gy = zoff + (long long)y * a.nx;
@@ -421,7 +423,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     pdl_wait();
     {
         const CtView<T, N> s = ctv<T, N>(A);
-        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
             const int bb = t % NB, y = t / NB;
             const int f = bb / TX, b = bb % TX;
             s[t] = (f < a.nf && b < valid) ? a.spec[f][zoff + (long long)y * a.nx + b]
@@ -432,7 +434,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     const int X = ct_fft<T, N, NB, -1>(A, B, R);
     {
         const CtView<T, N> s = ctv<T, N>(X);
-        for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+        for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
             const int bb = t % NB, ky = t / NB;
             const int kx = x0 + min(bb % TX, valid - 1);
             const int kxm = (a.nx - kx) % a.nx, kym = (N - ky) % N;
@@ -443,7 +445,7 @@ __global__ void HQT_CT_BOUNDS k_y_filt_c(YFiltArgs<T> a) {
     __syncthreads();
     const int r = ct_fft<T, N, NB, +1>(X, (X == A) ? B : A, R);
     const CtView<T, N> s = ctv<T, N>(r);
-    for (int t = threadIdx.x; t < N * NB; t += kCtThreads) {
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
         const int bb = t % NB, y = t / NB;
         const int f = bb / TX, b = bb % TX;
         if (f < a.nf && b < valid) a.spec[f][zoff + (long long)y * a.nx + b] = s[t];
