@@ -71,7 +71,8 @@ struct hqt_ctx {
     double *yax2[2] = {nullptr, nullptr}, *yay2[2] = {nullptr, nullptr};
     double *kax = nullptr, *kay = nullptr, *krho = nullptr;
     // derivatives
-    double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr;
+    double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr,
+            *dyypsi = nullptr;
     double *dxxay = nullptr, *divA = nullptr, *dxB = nullptr, *dyB = nullptr;
     double *dxat = nullptr, *dyat = nullptr, *dat = nullptr, *dxax = nullptr;
     // mixed precision: FP32 stage inputs ([0], [1]; [2] = copy of the state)
@@ -80,7 +81,8 @@ struct hqt_ctx {
     float2 *ypsi32[3] = {nullptr, nullptr, nullptr};
     float *yax32[3] = {nullptr, nullptr, nullptr}, *yay32[3] = {nullptr, nullptr, nullptr};
     float *at32 = nullptr;
-    float2 *dxpsi32 = nullptr, *lap32 = nullptr, *E32 = nullptr, *dypsi32 = nullptr;
+    float2 *dxpsi32 = nullptr, *dxx32 = nullptr, *dyy32 = nullptr, *E32 = nullptr,
+           *dypsi32 = nullptr;
     float *dxxay32 = nullptr, *divA32 = nullptr, *dxB32 = nullptr, *dyB32 = nullptr;
     float *dxat32 = nullptr, *dyat32 = nullptr;
     double *slice_mean = nullptr;                           // 5 per z-slice
@@ -294,10 +296,9 @@ int launch_y_rhs(hqt_ctx *c, const double2 *psi, const double *ax, const double 
     a.ax = ax;
     a.ay = ay;
     a.E = c->E;
-    a.dxxpsi = c->dxxpsi;
     a.dxxay = c->dxxay;
     a.dypsi = c->dypsi;
-    a.lap = c->dxxpsi;
+    a.dyypsi = c->dyypsi;
     a.divA = c->divA;
     a.dxB = c->dxB;
     a.dyB = c->dyB;
@@ -385,7 +386,7 @@ int launch_x_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *
     a.ax = ax;
     a.ay = ay;
     a.dxpsi = c->dxpsi32;
-    a.dxxpsi = c->lap32;
+    a.dxxpsi = c->dxx32;
     a.E = c->E32;
     a.dxxay = c->dxxay32;
     Prof pr(c, K_X_RHS);
@@ -418,10 +419,9 @@ int launch_y_rhs32(hqt_ctx *c, const float2 *psi, const float *ax, const float *
     a.ax = ax;
     a.ay = ay;
     a.E = c->E32;
-    a.dxxpsi = c->lap32;
     a.dxxay = c->dxxay32;
     a.dypsi = c->dypsi32;
-    a.lap = c->lap32;
+    a.dyypsi = c->dyy32;
     a.divA = c->divA32;
     a.dxB = c->dxB32;
     a.dyB = c->dyB32;
@@ -760,7 +760,8 @@ int enqueue_stages_mixed(hqt_ctx *c) {
         a.dyat = c->dyat32;
         a.dxpsi = c->dxpsi32;
         a.dypsi = c->dypsi32;
-        a.lap = c->lap32;
+        a.dxxpsi = c->dxx32;
+        a.dyypsi = c->dyy32;
         a.divA = c->divA32;
         a.dxB = c->dxB32;
         a.dyB = c->dyB32;
@@ -833,7 +834,8 @@ int enqueue_step(hqt_ctx *c) {
         a.dyat = c->dyat;
         a.dxpsi = c->dxpsi;
         a.dypsi = c->dypsi;
-        a.lap = c->dxxpsi;
+        a.dxxpsi = c->dxxpsi;
+        a.dyypsi = c->dyypsi;
         a.divA = c->divA;
         a.dxB = c->dxB;
         a.dyB = c->dyB;
@@ -1683,6 +1685,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
     A(&c->dxxpsi, sizeof(double2) * V);
     A(&c->E, sizeof(double2) * V);
     A(&c->dypsi, sizeof(double2) * V);
+    A(&c->dyypsi, sizeof(double2) * V);
     A(&c->dxxay, sizeof(double) * V);
     A(&c->divA, sizeof(double) * V);
     A(&c->dxB, sizeof(double) * V);
@@ -1700,7 +1703,8 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         }
         A(&c->at32, sizeof(float) * V);
         A(&c->dxpsi32, sizeof(float2) * V);
-        A(&c->lap32, sizeof(float2) * V);
+        A(&c->dxx32, sizeof(float2) * V);
+        A(&c->dyy32, sizeof(float2) * V);
         A(&c->E32, sizeof(float2) * V);
         A(&c->dypsi32, sizeof(float2) * V);
         A(&c->dxxay32, sizeof(float) * V);
@@ -2022,7 +2026,8 @@ int hqt_rhs_device(hqt_ctx *c, const void *dZ1, const void *dZ2, const void *dZ3
     a.dyat = c->dyat;
     a.dxpsi = c->dxpsi;
     a.dypsi = c->dypsi;
-    a.lap = c->dxxpsi;
+    a.dxxpsi = c->dxxpsi;
+    a.dyypsi = c->dyypsi;
     a.divA = c->divA;
     a.dxB = c->dxB;
     a.dyB = c->dyB;

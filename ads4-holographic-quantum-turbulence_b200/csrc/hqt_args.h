@@ -44,10 +44,9 @@ template <typename T> struct YRhsArgs {
     T s1, s2;
     const C2<T> *psi;
     const T *ax, *ay;
-    const C2<T> *E;       // d_x A_x + i d_x A_y
-    const C2<T> *dxxpsi;  // read, may alias lap
+    const C2<T> *E;  // d_x A_x + i d_x A_y
     const T *dxxay;
-    C2<T> *dypsi, *lap;
+    C2<T> *dypsi, *dyypsi;  // (the radial stage forms lap Psi = d_xx Psi + d_yy Psi)
     T *divA, *dxB, *dyB;
 };
 
@@ -136,7 +135,7 @@ template <typename T, typename TS, typename TD = T> struct ZStageArgs {
     const T *yax, *yay;
     const T *at, *dat;
     const TD *dxat, *dyat;
-    const C2<TD> *dxpsi, *dypsi, *lap;
+    const C2<TD> *dxpsi, *dypsi, *dxxpsi, *dyypsi;  // lap Psi = dxxpsi + dyypsi
     const TD *divA, *dxB, *dyB;
     // RK state and accumulators (type TS)
     const C2<TS> *zpsi;

@@ -188,9 +188,7 @@ __global__ void HQT_CT_BOUNDS k_y_rhs_c(YRhsArgs<T> a) {
     cp_commit();
     const int fr = (r1 == Y) ? C : Y;
     const int r2 = ct_fft<T, N, NB, +1>(X, fr, R);
-    cy_store_rd<T, N, NB, C2<T>>(
-        r2, valid, a.nx, zoff, [&](long long g) { return a.dxxpsi[g]; },
-        [&](long long g, C2<T> v, C2<T> x) { a.lap[g] = x + v; });
+    cy_store<T, N, NB>(r2, valid, a.nx, zoff, [&](long long g, C2<T> v) { a.dyypsi[g] = v; });
     __syncthreads();  // X and fr are free
     cy_load_async<T, N, NB>(fr, valid, a.nx, zoff, a.E);
     cp_commit();

@@ -8,8 +8,9 @@
 //   x pass (lines along x, contiguous):  d_x Psi, d_xx Psi,
 //            E = d_x(A_x + i A_y), d_xx A_y
 //   y pass (columns along y, tiles of TX adjacent columns per z-slice):
-//            d_y Psi, lap Psi = d_xx Psi + d_yy Psi, div A = d_x A_x + d_y A_y,
-//            d_x B and d_y B with B = d_x A_y - d_y A_x
+//            d_y Psi, d_yy Psi (the radial stage forms lap Psi = d_xx Psi +
+//            d_yy Psi), div A = d_x A_x + d_y A_y, d_x B and d_y B with
+//            B = d_x A_y - d_y A_x
 //
 // which is everything F1, F3, F4 and F2 need from the horizontal directions
 // (F3 uses 1/2 d_y(d_y A_x - d_x A_y) = -1/2 d_y B, F4 uses 1/2 d_x B).  Real
@@ -215,9 +216,7 @@ template <typename T> __global__ void HQT_FFT_BOUNDS k_y_rhs(YRhsArgs<T> a) {
     __syncthreads();
     int fr = (r1 == Y) ? A2 : Y;
     int r2 = fft_run<T>(X, fr, R, a.plan, nb, +1);
-    yl_store_rd<T, C2<T>>(
-        r2, n, nb, a.nx, zoff, [&](long long g) { return a.dxxpsi[g]; },
-        [&](long long g, int, C2<T> v, C2<T> x) { a.lap[g] = x + v; });
+    yl_store<T>(r2, n, nb, a.nx, zoff, [&](long long g, C2<T> v) { a.dyypsi[g] = v; });
     __syncthreads();
     // ---- C = A_x + i A_y and E = d_x C as one batch of 2*nb lines ----
     const int nb2 = 2 * nb;

@@ -180,10 +180,11 @@ __global__ void __launch_bounds__(32) k_x_rhs_pfa(const __grid_constant__ XRhsAr
 }
 
 // y pass of one RK stage (lines along y: kPfaLines adjacent x columns of one
-// z slice): d_y Psi, lap Psi = d_xx Psi + d_yy Psi, and from A_x, A_y and
-// E = d_x(A_x + i A_y) the fields div A = d_x A_x + d_y A_y, d_x B and d_y B
-// (B = d_x A_y - d_y A_x).  Addends (d_xx Psi, d_x A_x, d_xx A_y) are
-// fetched into a freed buffer while an inverse stage runs.
+// z slice): d_y Psi, d_yy Psi (the radial stage adds d_xx Psi), and from
+// A_x, A_y and E = d_x(A_x + i A_y) the fields div A = d_x A_x + d_y A_y,
+// d_x B and d_y B (B = d_x A_y - d_y A_x).  Inputs and addends (the gauge
+// lines, d_x A_x, d_xx A_y) are fetched into a freed buffer while a stage
+// runs.
 template <typename T, int P, int Q>
 __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsArgs<T> a) {
     using D = PfaDims<P, Q>;
@@ -221,31 +222,39 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
     __syncwarp();
     w.template stage_b_deriv<2>(L.b0, L.b1, a.s1, a.s2, cs);
     __syncwarp();
-    L.fetch(L.b0, [&](int ln, int n) { return &a.dxxpsi[gi(ln, n)].x; },
-            [&](int ln, int n) { return &a.dxxpsi[gi(ln, n)].y; });
-    cp_commit();
-    inverse(L.b1);
-    cp_wait<0>();
-    __syncwarp();
-    L.each([&](int ln, int n, int i) {
-        a.lap[gi(ln, n)] = mk2<T>(L.b0.re[i] + L.b1.re[i], L.b0.im[i] + L.b1.im[i]);
-    });
-    __syncwarp();
-    if constexpr (std::is_same<T, double>::value) {
-        // FP64: C = A_x + i A_y and E = d_x C after stage A, and the real
-        // fields separated from their pair spectra (measured faster in FP64
-        // than the two-field form below, which keeps fewer registers but
-        // loads the shared-memory pipe more)
+    // b0 is free: the first gauge line comes in while d_yy Psi is
+    // transformed and stored, the second (into b1) while the first is
+    // transformed.  FP64: C = A_x + i A_y and E = d_x C; FP32: the two-field
+    // form (W1 = E_x + i A_y, W2 = A_x + i E_y, below).
+    constexpr bool kF64 = std::is_same<T, double>::value;
+    if constexpr (kF64)
         L.fetch(L.b0, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
                 [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+    else
+        L.fetch(L.b0, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
+                [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
+    cp_commit();
+    inverse(L.b1);
+    L.each([&](int ln, int n, int i) { a.dyypsi[gi(ln, n)] = mk2<T>(L.b1.re[i], L.b1.im[i]); });
+    __syncwarp();
+    if constexpr (kF64)
         L.fetch(L.b1, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
                 [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
-        cp_commit();
-        cp_wait<0>();
-        __syncwarp();
-        w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
-        w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
-        __syncwarp();
+    else
+        L.fetch(L.b1, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
+                [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
+    cp_commit();
+    cp_wait<1>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
+    cp_wait<0>();
+    __syncwarp();
+    w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
+    __syncwarp();
+    if constexpr (kF64) {
+        // FP64: the real fields separated from their pair spectra (measured
+        // faster in FP64 than the two-field form below, which keeps fewer
+        // registers but loads the shared-memory pipe more)
         // column pairs (k2, Q - k2) of each line: spectra, combination, inverse
         constexpr int NPAIR = (Q + 1) / 2;
     #pragma unroll 1
@@ -345,16 +354,6 @@ __global__ void __launch_bounds__(32) k_y_rhs_pfa(const __grid_constant__ YRhsAr
         //     div A = E_x + Im(d_y W1),  d_x B = d_xx A_y - Re(d_y W1);
         //   W2 = A_x + i E_y:  d_y B = d_y E_y - d_yy A_x = Im(d_y W2) - Re(d_yy W2)
         //     = Re(IFFT((s1 k - s2 k^2) W2^)) (Im(z) = Re(-i z)), one real multiplier.
-        L.fetch(L.b0, [&](int ln, int n) { return &a.E[gi(ln, n)].x; },
-                [&](int ln, int n) { return &a.ay[gi(ln, n)]; });
-        L.fetch(L.b1, [&](int ln, int n) { return &a.ax[gi(ln, n)]; },
-                [&](int ln, int n) { return &a.E[gi(ln, n)].y; });
-        cp_commit();
-        cp_wait<0>();
-        __syncwarp();
-        w.template stage_a<-1>(L.b0, L_t::in_place(L.b0));
-        w.template stage_a<-1>(L.b1, L_t::in_place(L.b1));
-        __syncwarp();
         w.template stage_b_deriv<1>(L.b0, L.b0, a.s1, a.s2, cs);
         w.template stage_b<true, true>(L.b1, L.b1, cs, [&](int, int k1, int k2, T &re, T &im) {
             const T kk = PfaWarp<T, P, Q>::wavenumber(k1, k2);

@@ -31,7 +31,8 @@
 //   Gg  (d_x A_t, d_y A_t), (d_y B, d_x B), state, accumulator -> G
 //   F3, F4  g = d A_t + f Lz A, S = 1/2 Lz g -+ 1/2 d B
 //           + Im(conj(Psi) d Psi) - A |Psi|^2 (:74-75), F = Lzr(S), RK update
-//   G2  A_t, d_z A_t, lap Psi, div A, Psi state and accumulator -> G;
+//   G2  A_t, d_z A_t, d_xx Psi, d_yy Psi, div A, Psi state and accumulator
+//       -> G;
 //       dp = Lz Psi -> V
 //   S1  d2 = Lz dp, S1 (:72-73), boundary row kb = Lz(nz,:) div A -> V;
 //       then Gm of the next tile
@@ -107,8 +108,11 @@ template <typename TD, int NZP> struct ZfLayout {
     // G, gauge phase: (d_x A_t, d_y A_t), (d_y B, d_x B), state, accumulator
     static constexpr int gDT = 0, gBF = dc, gZA = 2 * dc, gKA = 2 * dc + c;
     static constexpr int gsz = 2 * dc + 2 * c;
-    // G, Psi phase: A_t, d_z A_t, lap Psi, div A, Psi state and accumulator
-    static constexpr int pAT = 0, pDAT = r, pLAP = 2 * r, pDIV = 2 * r + dc;
+    // G, Psi phase: A_t, d_z A_t, d_xx Psi, d_yy Psi, div A, Psi state and
+    // accumulator (lap Psi is formed here: the y pass then neither reads
+    // d_xx Psi nor waits for it before the gauge fields)
+    static constexpr int pAT = 0, pDAT = r, pLXX = 2 * r, pLYY = 2 * r + dc,
+                         pDIV = 2 * r + 2 * dc;
     static constexpr int pZP = ((pDIV + dr + 15) / 16) * 16, pKP = pZP + c;
     static constexpr int psz = pKP + c;
     static constexpr int gsz16 = ((gsz + 15) / 16) * 16;
@@ -240,7 +244,8 @@ __global__ void __launch_bounds__(kZThreads, 2)
     const ZTileF<double2> KA{reinterpret_cast<double2 *>(gr + Lay::gKA)};
     const ZTileF<T> AT{reinterpret_cast<T *>(gp + Lay::pAT)};
     const ZTileF<T> DAT{reinterpret_cast<T *>(gp + Lay::pDAT)};
-    const ZTileF<C2<TD>> LAP{reinterpret_cast<C2<TD> *>(gp + Lay::pLAP)};
+    const ZTileF<C2<TD>> LXX{reinterpret_cast<C2<TD> *>(gp + Lay::pLXX)};
+    const ZTileF<C2<TD>> LYY{reinterpret_cast<C2<TD> *>(gp + Lay::pLYY)};
     const ZTileF<TD> DIV{reinterpret_cast<TD *>(gp + Lay::pDIV)};
     const ZTileF<double2> ZP{reinterpret_cast<double2 *>(gp + Lay::pZP)};
     const ZTileF<double2> KP{reinterpret_cast<double2 *>(gp + Lay::pKP)};
@@ -268,7 +273,8 @@ __global__ void __launch_bounds__(kZThreads, 2)
     auto stage_psi = [&](long long site0) {
         zf_real<NZP, T>(AT, a.at, nz, P, site0, tid);
         zf_real<NZP, T>(DAT, a.dat, nz, P, site0, tid);
-        zf_real<NZP, C2<TD>>(LAP, a.lap, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(LXX, a.dxxpsi, nz, P, site0, tid);
+        zf_real<NZP, C2<TD>>(LYY, a.dyypsi, nz, P, site0, tid);
         zf_real<NZP, TD>(DIV, a.divA, nz, P, site0, tid);
         if (MODE >= 1) {
             zf_real<NZP, double2>(ZP, a.zpsi, nz, P, site0, tid);
@@ -420,7 +426,9 @@ __global__ void __launch_bounds__(kZThreads, 2)
                 const int ic = i < nz - 1 ? i : 0;
                 const double2 ps = PS(ic, cw + q), av = AXY(ic, cw + q), d1 = VC(ic, cw + q);
                 const T at = AT(ic, cw + q), dat = DAT(ic, cw + q);
-                const C2<TD> lp = LAP(ic, cw + q), dx = DXP(ic, cw + q), dy = DYP(ic, cw + q);
+                const C2<TD> lxx = LXX(ic, cw + q), lyy = LYY(ic, cw + q);
+                const C2<TD> dx = DXP(ic, cw + q), dy = DYP(ic, cw + q);
+                const T lpx = T(lxx.x) + T(lyy.x), lpy = T(lxx.y) + T(lyy.y);
                 const T dv = T(DIV(ic, cw + q));
                 const T z = zr[m], f = fzr[m], hh = T(0.5);
                 const T a2 = av.x * av.x + av.y * av.y;
@@ -428,10 +436,10 @@ __global__ void __launch_bounds__(kZThreads, 2)
                 const T w = av.x * T(dx.y) + av.y * T(dy.y);
                 const T r0 = -at * d1.y - hh * dat * ps.y + hh * f * d2[m][0] -
                              T(1.5) * z * z * d1.x - hh * z * ps.x - hh * a2 * ps.x +
-                             hh * T(lp.x) + hh * dv * ps.y + w;
+                             hh * lpx + hh * dv * ps.y + w;
                 const T r1 = at * d1.x + hh * dat * ps.x + hh * f * d2[m][1] -
                              T(1.5) * z * z * d1.y - hh * z * ps.y - hh * a2 * ps.y +
-                             hh * T(lp.y) - hh * dv * ps.x - u;
+                             hh * lpy - hh * dv * ps.x - u;
                 const bool in = i < nz - 1;
                 s1[m][0] = in ? r0 : 0.0;
                 s1[m][1] = in ? r1 : 0.0;
