@@ -47,6 +47,29 @@ __device__ __forceinline__ void cx_load_pair_async(int buf, int valid, long long
         }
     }
 }
+// a FieldIn (complex, or re with optional im) into the x-line layout of
+// cx_load by cp.async (zero past `valid` and for a missing im); the caller
+// commits and waits
+template <typename T, int N, int NB>
+__device__ __forceinline__ void cx_load_field_async(int buf, int valid, long long g0,
+                                                    const FieldIn<T> &f) {
+    const CtView<T, N> s = ctv<T, N>(buf);
+    for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
+        const int b = t / N, e = t - b * N;
+        C2<T> &d = s[e * NB + b];
+        if (b >= valid) {
+            d = mk2<T>(T(0), T(0));
+        } else if (f.c) {
+            cp_async<sizeof(C2<T>)>(&d, f.c + g0 + t);
+        } else {
+            cp_async<sizeof(T)>(&d.x, f.re + g0 + t);
+            if (f.im)
+                cp_async<sizeof(T)>(&d.y, f.im + g0 + t);
+            else
+                d.y = T(0);
+        }
+    }
+}
 // y lines: NB adjacent columns of one z slice; element (y, b) at y*NB + b
 template <typename T, int N, int NB, typename F>
 __device__ __forceinline__ void cy_load(int buf, int valid, int nx, long long zoff, F get) {
@@ -383,26 +406,35 @@ __global__ void HQT_CT_BOUNDS k_x_filt_fwd_c(XFiltFwdArgs<T> a) {
     ct_load_roots<T, N>(R, a.roots);
     pdl_wait();
     const int w = a.st ? a.st->winding : 0;
+    // field 0 (with the winding phase) is loaded directly; field f + 1 comes
+    // by cp.async into the buffer the transform of field f left free, while
+    // field f is stored
+    cx_load<T, N, NB>(A, valid, [&](int t) {
+        C2<T> v = load_field(a.in[0], g0 + t);
+        if (w != 0) {
+            // phase -2*pi*y*w/ny of line L0 + t/N (tevol_driven_cluster.m:139)
+            const int y = (L0 + t / N) % a.ny;
+            const long long q = ((long long)y * w) % a.ny;
+            double sn, cs;
+            sincospi(-2.0 * (double)q / (double)a.ny, &sn, &cs);
+            v = mk2<T>(v.x * (T)cs - v.y * (T)sn, v.x * (T)sn + v.y * (T)cs);
+        }
+        return v;
+    });
+    __syncthreads();
+    int src = A;
     for (int f = 0; f < a.nf; ++f) {
-        cx_load<T, N, NB>(A, valid, [&](int t) {
-            C2<T> v = load_field(a.in[f], g0 + t);
-            if (f == 0 && w != 0) {
-                // phase -2*pi*y*w/ny of line L0 + t/N (tevol_driven_cluster.m:139)
-                const int y = (L0 + t / N) % a.ny;
-                const long long q = ((long long)y * w) % a.ny;
-                double sn, cs;
-                sincospi(-2.0 * (double)q / (double)a.ny, &sn, &cs);
-                v = mk2<T>(v.x * (T)cs - v.y * (T)sn, v.x * (T)sn + v.y * (T)cs);
-            }
-            return v;
-        });
-        __syncthreads();
-        const int X = ct_fft<T, N, NB, -1>(A, B, R);
+        const int X = ct_fft<T, N, NB, -1>(src, src == A ? B : A, R);
+        const int F = (X == A) ? B : A;
+        if (f + 1 < a.nf) cx_load_field_async<T, N, NB>(F, valid, g0, a.in[f + 1]);
+        cp_commit();
         C2<T> *spec = a.spec[f];
         cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) {
             if (filt_col_live(t % N, a.dead0, a.dead1)) spec[g0 + t] = v;
         });
+        cp_wait<0>();
         __syncthreads();
+        src = F;
     }
 }
 
@@ -462,18 +494,38 @@ __global__ void HQT_CT_BOUNDS k_x_filt_inv_c(XFiltInvArgs<T> a) {
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
     int mybad = 0;
-    for (int f = 0; f < a.nf; ++f) {
+    // spectrum f by cp.async, the weight-zeroed columns as zero; spectrum
+    // f + 1 comes into the buffer the transform of field f left free while
+    // field f is stored
+    auto fetch = [&](int buf, int f) {
+        const CtView<T, N> s = ctv<T, N>(buf);
         const C2<T> *spec = a.spec[f];
-        cx_load<T, N, NB>(A, valid, [&](int t) {
-            return filt_col_live(t % N, a.dead0, a.dead1) ? spec[g0 + t] : mk2<T>(T(0), T(0));
-        });
-        __syncthreads();
-        const int X = ct_fft<T, N, NB, +1>(A, B, R);
+        for (int t = threadIdx.x; t < N * NB; t += ct_threads<T, N, NB>()) {
+            const int b = t / N, e = t - b * N;
+            C2<T> &d = s[e * NB + b];
+            if (b < valid && filt_col_live(e, a.dead0, a.dead1))
+                cp_async<sizeof(C2<T>)>(&d, spec + g0 + t);
+            else
+                d = mk2<T>(T(0), T(0));
+        }
+    };
+    fetch(A, 0);
+    cp_commit();
+    cp_wait<0>();
+    __syncthreads();
+    int src = A;
+    for (int f = 0; f < a.nf; ++f) {
+        const int X = ct_fft<T, N, NB, +1>(src, src == A ? B : A, R);
+        const int F = (X == A) ? B : A;
+        if (f + 1 < a.nf) fetch(F, f + 1);
+        cp_commit();
         cx_store<T, N, NB>(X, valid, [&](int t, C2<T> v) {
             if (!(isfinite(v.x) && isfinite(v.y))) mybad = 1;
             store_field(a.out[f], g0 + t, v);
         });
+        cp_wait<0>();
         __syncthreads();
+        src = F;
     }
     if (a.st) {
         if (mybad) bad = 1;

@@ -551,6 +551,8 @@ __global__ void __launch_bounds__(32) k_x_filt_fwd_pfa(const __grid_constant__ X
     const L_t L(min(kPfaLines, a.nlines - L0));
     auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
     const int wnd = a.st ? a.st->winding : 0;
+    // (Fetching field f + 1 into b0 while field f is stored measured 63.9 ->
+    // 65.7 us at 301x301x21; the x inverse below gains from it.)
 #pragma unroll 1
     for (int f = 0; f < a.nf; ++f) {
         L.fetch_field(L.b0, a.in[f], gi, [](int ln, int n) { return L_t::pos(ln, n); });
@@ -667,8 +669,10 @@ __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ X
     const L_t L(min(kPfaLines, a.nlines - L0));
     auto gi = [&](int ln, int n) { return g0 + (long long)ln * N + n; };
     bool bad = false;
-#pragma unroll 1
-    for (int f = 0; f < a.nf; ++f) {
+    // spectrum f into b0 (the weight-zeroed columns as zero); spectrum f + 1
+    // comes in (b0 is free after stage B) while field f is transformed and
+    // stored
+    auto fetch = [&](int f) {
         const double2 *spec = a.spec[f];
         for (int e = L.lane; e < L_t::LN; e += 32) {
             const int ln = e % kPfaLines, k = e / kPfaLines, i = L_t::spos(ln, k);
@@ -680,11 +684,17 @@ __global__ void __launch_bounds__(32) k_x_filt_inv_pfa(const __grid_constant__ X
                 L.b0.im[i] = T(0);
             }
         }
-        cp_commit();
+    };
+    fetch(0);
+    cp_commit();
+#pragma unroll 1
+    for (int f = 0; f < a.nf; ++f) {
         cp_wait<0>();
         __syncwarp();
         w.template stage_b<false, true>(L.b0, L.b1, cs, [](int, int, int, double &, double &) {});
         __syncwarp();
+        if (f + 1 < a.nf) fetch(f + 1);
+        cp_commit();
         w.template stage_a<+1>(L.b1, L_t::in_place(L.b1));
         __syncwarp();
         const bool f32 = a.slice_mean && (a.c32[f] || a.re32[f] || a.im32[f]);
