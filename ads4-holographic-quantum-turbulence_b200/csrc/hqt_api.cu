@@ -1148,7 +1148,8 @@ void tune_file_append(const std::string &key, const LineGeom &g) {
       << ' ' << g.NBx_2 << ' ' << g.TXy_rhs << ' ' << g.TXy_2 << ' ' << g.TXy_filt << '\n';
 }
 
-// A geometry from a cache could name an engine this build lacks for the length.
+// A geometry from a cache could name an engine the library lacks for the
+// length.
 bool geom_valid(const hqt_ctx *c, const LineGeom &g) {
     if ((g.px && !pfa_length(c->nx)) || (g.py && !pfa_length(c->ny))) return false;
     if ((g.cx && !ct_supported(c->nx)) || (g.cy && !ct_supported(c->ny))) return false;
@@ -1190,7 +1191,7 @@ int time_geom(hqt_ctx *c, const LineGeom &g, double *ms) {
 }
 
 // Choose the line-pass geometry by timing whole steps: every engine pairing
-// this build has for (nx, ny), and for the runtime-plan engine its
+// the library has for (nx, ny), and for the runtime-plan engine its
 // shared-memory heuristic and half of it.  Results are cached per process
 // (and in the file named by HQT_TUNE_CACHE) under the grid, precision and
 // step options.  The internal state is used as scratch and the step counter

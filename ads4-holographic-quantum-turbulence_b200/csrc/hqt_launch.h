@@ -93,7 +93,8 @@ cudaError_t z_misc(const ZColArgs<double> &a, const ZHost &h, int grid, int thre
 
 }  // namespace hqt
 
-// Compile-time column lengths of this build; a run uses the smallest >= nz.
+// Compile-time column lengths compiled into the library; a run uses the
+// smallest >= nz.
 #define HQT_NZP_LIST(X) X(8) X(12) X(16) X(17) X(21) X(25) X(33)
 // Line lengths with compile-time transforms; other lengths use hqt_fft.cuh.
 #define HQT_CN_LIST(X) X(33) X(64) X(128) X(192) X(256) X(301) X(512) X(1024)

@@ -39,7 +39,7 @@ extern "C" {
                                 (smoke-test id hqt:NonfiniteEvolution)     */
 #define HQT_ECUDA         3  /* CUDA runtime error                         */
 #define HQT_ENOMEM        4  /* device allocation failed                   */
-#define HQT_EUNSUPPORTED  5  /* size or mode this build does not handle    */
+#define HQT_EUNSUPPORTED  5  /* size or mode the library does not handle  */
 
 /* precision modes */
 #define HQT_FP64   0         /* plain FP64 drop-in                          */
