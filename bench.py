@@ -62,7 +62,7 @@ def ensemble_runs(n_runs: int = 32):
 
 # Algorithmic bytes per site of one launch of each kernel kind (FP64): the
 # arrays the kernel must read once and write once.
-ALG_BYTES = {"x_rhs": 88, "y_rhs": 128, "zstage": 248, "x_d1": 16, "y_d1": 20,
+ALG_BYTES = {"x_rhs": 88, "y_rhs": 112, "zstage": 264, "x_d1": 16, "y_d1": 20,
              "zcons": 40, "zcol_misc": 16, "filter_x_fwd": 96, "filter_y": 96,
              "filter_x_inv": 96}
 # compulsory traffic of a whole FP64 step per site: 4*(S_in + S_k) + 2*S_state
