@@ -67,6 +67,14 @@ ALG_BYTES = {"x_rhs": 88, "y_rhs": 112, "zstage": 264, "x_d1": 16, "y_d1": 20,
              "filter_x_inv": 96}
 # compulsory traffic of a whole FP64 step per site: 4*(S_in + S_k) + 2*S_state
 STEP_BYTES_FP64 = 4 * (40 + 32) + 2 * 40
+# FP64 tensor-core work of the prime-factor line passes (n = 301 = 7*43): one
+# 43-point stage A is 144 mma.sync.m8n8k4.f64 per two lines (2 passes x 6
+# reduction steps x 2 operand tiles x 3 row tiles x cos/sin), 512 flops each;
+# x_rhs runs 6 stage A per line pair, y_rhs 7.  The peak is the mma.sync f64
+# throughput measured on B200 at 1965 MHz (37.1 TFLOP/s for the m8n8k4,
+# m16n8k4 and m16n8k16 shapes alike).
+PFA_DMMA_PER_LINE = {"x_rhs": 6 * 144 / 2, "y_rhs": 7 * 144 / 2}
+FP64_TENSOR_TFLOPS = 37.1
 
 
 def peaks():
@@ -325,6 +333,14 @@ def run_ours(args, w, ws, rank, local):
                 "peak_source": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                 "share": top["ms"] / tot}
+    if nx == 301 and ny == 301 and top["kernel"] in PFA_DMMA_PER_LINE:
+        lines = (ny if top["kernel"] == "x_rhs" else nx) * nz
+        flops = lines * PFA_DMMA_PER_LINE[top["kernel"]] * 512
+        tf = flops / (avg_ms / 1e3) / 1e12
+        roofline["fp64_tensor"] = {
+            "achieved": tf, "peak": FP64_TENSOR_TFLOPS, "unit": "TFLOP/s",
+            "frac": tf / FP64_TENSOR_TFLOPS, "flops_per_launch": flops,
+            "peak_source": "mma.sync f64 throughput measured on B200 (probe)"}
     step_gbs = STEP_BYTES_FP64 * sites * args.steps / (ms / 1e3) / 1e9
     breakdown = {k["kernel"]: {"launches": k["launches"], "ms": round(k["ms"], 4),
                                "share": round(k["ms"] / tot, 4)} for k in rep["kernels"]}
