@@ -69,7 +69,8 @@ struct hqt_ctx {
     // stage inputs, double-buffered: stages 2 and 4 read Y[0], stage 3 reads Y[1]
     double2 *ypsi2[2] = {nullptr, nullptr}, *kpsi = nullptr;
     double *yax2[2] = {nullptr, nullptr}, *yay2[2] = {nullptr, nullptr};
-    double *kax = nullptr, *kay = nullptr, *krho = nullptr;
+    double2 *kA = nullptr;  // (A_x, A_y) accumulator, interleaved
+    double *krho = nullptr;
     // derivatives
     double2 *dxpsi = nullptr, *dxxpsi = nullptr, *E = nullptr, *dypsi = nullptr,
             *dyypsi = nullptr;
@@ -770,8 +771,7 @@ int enqueue_stages_mixed(hqt_ctx *c) {
         a.zay = ay;
         a.zrho = c->rho;
         a.kpsi = c->kpsi;
-        a.kax = c->kax;
-        a.kay = c->kay;
+        a.kA = c->kA;
         a.krho = c->krho;
         a.npsi = c->ypsi2[ni];
         a.nax = c->yax2[ni];
@@ -844,8 +844,7 @@ int enqueue_step(hqt_ctx *c) {
         a.zay = ay;
         a.zrho = c->rho;
         a.kpsi = c->kpsi;
-        a.kax = c->kax;
-        a.kay = c->kay;
+        a.kA = c->kA;
         a.krho = c->krho;
         a.npsi = c->ypsi2[ni];
         a.nax = c->yax2[ni];
@@ -1679,8 +1678,7 @@ int hqt_create(const hqt_params *params, int device, hqt_ctx **out) {
         A(&c->yay2[b], sizeof(double) * V);
     }
     A(&c->kpsi, sizeof(double2) * V);
-    A(&c->kax, sizeof(double) * V);
-    A(&c->kay, sizeof(double) * V);
+    A(&c->kA, sizeof(double2) * V);
     A(&c->krho, sizeof(double) * P2);
     A(&c->dxpsi, sizeof(double2) * V);
     A(&c->dxxpsi, sizeof(double2) * V);

@@ -141,7 +141,8 @@ template <typename T, typename TS, typename TD = T> struct ZStageArgs {
     const C2<TS> *zpsi;
     const TS *zax, *zay, *zrho;
     C2<TS> *kpsi;
-    TS *kax, *kay, *krho;
+    C2<TS> *kA;  // (A_x, A_y) accumulator, interleaved: staged by 16-byte copies
+    TS *krho;
     C2<T> *npsi;  // next stage input
     T *nax, *nay;
     C2<TD> *npsi_d;  // its copy in the derivative type (mixed precision; may be null)

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kZThreads, 2)
         zf_pair<NZP, TD>(BF, a.dyB, a.dxB, nz, P, site0, tid);
         if (MODE >= 1) {
             zf_pair<NZP, double>(ZA, a.zax, a.zay, nz, P, site0, tid);
-            if (kReadK) zf_pair<NZP, double>(KA, a.kax, a.kay, nz, P, site0, tid);
+            if (kReadK) zf_real<NZP, double2>(KA, a.kA, nz, P, site0, tid);
         }
     };
 
@@ -365,12 +365,10 @@ __global__ void __launch_bounds__(kZThreads, 2)
                     continue;
                 }
                 if (MODE == 1) {
-                    a.kax[gi] = kx;
-                    a.kay[gi] = ky;
+                    a.kA[gi] = make_double2(kx, ky);
                 } else {
                     const double2 K = KA(i, cw + q);
-                    a.kax[gi] = K.x + 2 * kx;
-                    a.kay[gi] = K.y + 2 * ky;
+                    a.kA[gi] = make_double2(K.x + 2 * kx, K.y + 2 * ky);
                 }
                 const TS nx = (MODE == 3) ? z.x + kx : z.x + kx / 2;
                 const TS ny = (MODE == 3) ? z.y + ky : z.y + ky / 2;
