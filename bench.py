@@ -77,6 +77,22 @@ PFA_DMMA_PER_LINE = {"x_rhs": 6 * 144 / 2, "y_rhs": 7 * 144 / 2}
 FP64_TENSOR_TFLOPS = 37.1
 
 
+def kernel_rows(kernels, tot, sites=None, peak=None):
+    """Per-kernel launches, time and share of the step; with ``sites`` and
+    ``peak``, also each FP64 kernel's algorithmic GB/s (ALG_BYTES per site x
+    sites x launches / time) and its fraction of the HBM peak."""
+    rows = {}
+    for k in kernels:
+        row = {"launches": k["launches"], "ms": round(k["ms"], 4),
+               "share": round(k["ms"] / tot, 4)}
+        if sites and peak and k["kernel"] in ALG_BYTES and k["ms"] > 0:
+            gbs = ALG_BYTES[k["kernel"]] * sites * k["launches"] / (k["ms"] / 1e3) / 1e9
+            row["alg_gbs"] = round(gbs, 1)
+            row["hbm_frac"] = round(gbs / peak, 4)
+        rows[k["kernel"]] = row
+    return rows
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -342,8 +358,7 @@ def run_ours(args, w, ws, rank, local):
             "frac": tf / FP64_TENSOR_TFLOPS, "flops_per_launch": flops,
             "peak_source": "mma.sync f64 throughput measured on B200 (probe)"}
     step_gbs = STEP_BYTES_FP64 * sites * args.steps / (ms / 1e3) / 1e9
-    breakdown = {k["kernel"]: {"launches": k["launches"], "ms": round(k["ms"], 4),
-                               "share": round(k["ms"] / tot, 4)} for k in rep["kernels"]}
+    breakdown = kernel_rows(rep["kernels"], tot, sites, peak)
 
     # end to end through the host-array call hqt_step on pinned buffers.  Each
     # call copies the whole state in (Z1..Z4 and rhoi's boundary plane) and
