@@ -1,22 +1,40 @@
-"""Host-side seeding: Newton stationary solve, spline regrid, initial fields."""
+"""Host-side seeding: Newton stationary solve, spline regrid, initial fields.
+
+The reference ships three stationary seeds (``data/reference/mu=6,nz=30,
+vy=7_20.mat``, ``mu=5,...,vy=3.8_20.mat``, ``mu=8,...,vy=13.5_20.mat``);
+``tests/golden/make_golden.py`` stores them as the ``seed_*.npz`` fixtures.
+Each must be a fixed point of the restated Newton solver and be reached by
+its continuation from an analytic guess."""
 import numpy as np
 import pytest
 
+from conftest import GOLDEN
+
 VY7 = -2 * np.pi * 7 / 20
+SHIPPED = [("seed_mu6_nz30_vy7", 6.0, 7.0), ("seed_mu5_nz30_vy3.8", 5.0, 3.8),
+           ("seed_mu8_nz30_vy13.5", 8.0, 13.5)]
 
 
-def test_shipped_seed_is_newton_fixed_point(hqt, shipped_seed):
+def load_seed(stem):
+    d = np.load(GOLDEN / f"{stem}.npz")
+    return {k: d[k] for k in d.files}
+
+
+@pytest.mark.parametrize("stem,mu,n", SHIPPED)
+def test_shipped_seed_is_newton_fixed_point(hqt, stem, mu, n):
     # the reference's own shipped profile satisfies the restated equations
-    s = shipped_seed
-    Z1, Z2, V, it, err = hqt.seed.NewtonRaphson_vy(30, s["Z1"], s["Z2"],
-                                                   s["Vy1"], VY7)
+    s = load_seed(stem)
+    assert float(s["mu"]) == mu
+    Z1, Z2, V, it, err = hqt.seed.NewtonRaphson_vy(30, s["Z1"], s["Z2"], s["Vy1"],
+                                                   -2 * np.pi * n / 20)
     assert it == 0 and err < 1e-6
     assert np.max(np.abs(Z1 - s["Z1"])) < 1e-6
 
 
-def test_continuation_reproduces_shipped_seed(hqt, shipped_seed):
-    prof = hqt.seed.stationary_profile(6.0, VY7)
-    s = shipped_seed
+@pytest.mark.parametrize("stem,mu,n", SHIPPED)
+def test_continuation_reproduces_shipped_seed(hqt, stem, mu, n):
+    prof = hqt.seed.stationary_profile(mu, -2 * np.pi * n / 20)
+    s = load_seed(stem)
     assert np.max(np.abs(prof.Z1 - s["Z1"])) < 1e-6
     assert np.max(np.abs(prof.Z2 - s["Z2"])) < 1e-6
     assert np.max(np.abs(prof.Vy1 - s["Vy1"])) < 1e-6
@@ -33,9 +51,11 @@ def test_smoke_test_newton_cases(hqt, shipped_seed):
         assert np.isfinite(err)
 
 
-def test_rhoi_is_minus_lz_z2(hqt, shipped_seed):
+@pytest.mark.parametrize("stem,mu,n", SHIPPED)
+def test_rhoi_is_minus_lz_z2(hqt, stem, mu, n):
     _, Lz = hqt.seed.radial_grid(30)
-    assert np.max(np.abs(-(Lz @ shipped_seed["Z2"]) - shipped_seed["rhoi"])) < 1e-9
+    s = load_seed(stem)
+    assert np.max(np.abs(-(Lz @ s["Z2"]) - s["rhoi"])) < 1e-9
 
 
 def test_chebdif_matches_oracle(hqt, oracle):
